@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""Throughput of the DSMC timestep on B200: atom-steps/s at 1e7 atoms.
+
+Workload: the full trapped step (1e7 Rb-87 atoms, linear quadrupole B' = 2.5 T/m, 50 uK,
+128^3 cells over +-5 thermal radii, dt = 1e-6 s, NTC collisions, Larmor precession,
+Majorana loss, energy knife 6 -> 4 kT over 1e5 steps), FP32 state with exact fixed-point
+diagnostics.  One bench "step" = one DSMC timestep of the whole cloud.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--atoms N]
+
+Under torchrun (N > 1) every rank simulates its own cloud (different seed): the clouds are
+independent, so the GPUs share no data and the scaling is weak.  ``--impl reference`` times
+the CPU restatement of the same step (the reference has no CPU code path; its CUDA kernels
+target sm_30) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s @1e7 atoms"
+UNIT = "atom-steps/s"
+WORKLOAD = "trapped-quadrupole-1e7-atoms-128cubed-cells-fp32"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--atoms", type=int, default=10_000_000)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def workload(atoms: int):
+    from cudadsmc_b200 import preset
+    run, c = preset(2)
+    c.n_atoms = atoms
+    c.capacity = atoms
+    return run, c
+
+
+def cpu_baseline(run, cloud, steps: int, threads: int | None = None) -> dict:
+    """The CPU restatement (OpenMP, float) timed on the host cores for a bounded sample."""
+    import oracle
+    if threads:
+        oracle.set_threads(threads)
+    nthreads = oracle.max_threads()
+    o = oracle.Oracle(run, cloud, fast=True)
+    o.init_cloud(run.seed)
+    o.step(1)  # warm-up
+    d0 = o.diagnostics()
+    t0 = time.perf_counter()
+    o.step(steps)
+    t1 = time.perf_counter()
+    d1 = o.diagnostics()
+    atom_steps = d1["atom_steps"] - d0["atom_steps"]
+    return {"value": atom_steps / (t1 - t0), "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{cloud.n_atoms:.0e} atoms, {steps} timed steps after init + 1 warm-up step "
+                      f"({t1 - t0:.1f} s), OpenMP float build of oracle/dsmc_oracle.cpp"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    run, c = workload(args.atoms)
+    res = cpu_baseline(run, c, steps=max(1, min(args.steps, args.cpu_steps)))
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": max(1, min(args.steps, args.cpu_steps)), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox cloud)",
+            "config": {"workload": WORKLOAD, "atoms": args.atoms, "cells": 128 ** 3, "host_threads": res["cores"]},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from cudadsmc_b200 import Simulation
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    run, c = workload(args.atoms)
+    sim = Simulation(run, c)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    sim.init_cloud(run.seed + 7919 * rank)
+
+    # ------------------------------------------------------------------ device-resident timing
+    sim.step(args.warmup)
+    sim.synchronize()
+    d0 = sim.diagnostics()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    d1 = sim.diagnostics()
+    atom_steps = d1["atom_steps"] - d0["atom_steps"]
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        a = torch.tensor([atom_steps], device="cuda", dtype=torch.float64)
+        dist.all_reduce(a)
+        atom_steps = int(a.item())
+    value = atom_steps / (ms * 1e-3)
+
+    # ------------------------------------------------------------------ per-kernel times (events)
+    sim.set_profiling(True)
+    sim.step(5)
+    kt = sim.kernel_times()
+    sim.set_profiling(False)
+    n_now = sim.diagnostics()["n_alive"]
+    commit_ms = kt["tile_pass_commit"][0] / kt["tile_pass_commit"][1]
+    plan_ms = kt["tile_pass_plan"][0] / kt["tile_pass_plan"][1]
+    bytes_atom_commit = 96  # read pos, vel, psi (48 B) + write them at the sorted slot (48 B)
+    bytes_atom_plan = 48
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    achieved = bytes_atom_commit * n_now / (commit_ms * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "tile_pass_commit_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = float(json.load(f)["dram_bytes_per_atom"]) * n_now
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "tile_pass_commit", "peak_source": peak_src,
+                "algorithmic_bytes_per_atom": bytes_atom_commit,
+                "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()},
+                "plan_pass_frac": bytes_atom_plan * n_now / (plan_ms * 1e-3) / 1e9 / peak}
+
+    # ------------------------------------------------------------------ end to end, host buffers
+    e2e = None
+    if not args.no_e2e:
+        st = sim.get_state()
+        pin = {k: torch.from_numpy(np.ascontiguousarray(st[k])).pin_memory() for k in ("pos", "vel", "psi")}
+        counts = st["cloud_counts"]
+        sim2 = Simulation(run, c)
+        sim2.set_stream(stream.cuda_stream)
+        sim2.set_state(pin["pos"].numpy(), pin["vel"].numpy(), pin["psi"].numpy(), counts)
+        sim2.step(args.warmup)
+        sim2.synchronize()
+        out = {k: torch.empty_like(v).pin_memory() for k, v in pin.items()}
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee0.record(stream)
+        sim2.set_state(pin["pos"].numpy(), pin["vel"].numpy(), pin["psi"].numpy(), counts)
+        a0 = sim2.diagnostics()["atom_steps"]
+        for _ in range(args.steps):
+            sim2.step(1)
+            dd = sim2.diagnostics()
+        st2 = sim2.get_state()
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee1.record(stream)
+        ee1.synchronize()
+        wall = time.perf_counter() - t0
+        e_ms = ee0.elapsed_time(ee1)
+        a_steps = dd["atom_steps"] - a0
+        if ws > 1:
+            t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+            a = torch.tensor([a_steps], device="cuda", dtype=torch.float64)
+            dist.all_reduce(a)
+            a_steps = int(a.item())
+        state_bytes = sum(v.numel() * v.element_size() for v in pin.values())
+        out_bytes = sum(st2[k].nbytes for k in ("pos", "vel", "psi"))
+        from cudadsmc_b200._abi import Diag
+        import ctypes
+        e2e = {"value": a_steps / (e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": out_bytes / args.steps + ctypes.sizeof(Diag),
+               "definition": "dsmc_set_state from pinned host buffers, K x (dsmc_step(1) + dsmc_diagnostics "
+                             "read back), dsmc_get_state to host; all inside the timed region",
+               "wall_s": wall}
+        sim2.close()
+
+    # ------------------------------------------------------------------ CPU baseline
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(run, c, steps=args.cpu_steps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Philox thermal cloud, no dataset)",
+                "config": {"workload": WORKLOAD, "atoms_per_gpu": args.atoms, "cells": 128 ** 3,
+                           "trap": "quadrupole B'=2.5 T/m", "T_uK": 50, "dt": 1e-6,
+                           "physics": "NTC collide + Larmor + Verlet + Majorana + knife 6->4 kT",
+                           "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
+                           "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"},
+                "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "n_alive_end": d1["n_alive"]}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

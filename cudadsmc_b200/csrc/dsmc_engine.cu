@@ -1,0 +1,698 @@
+// dsmc_engine.cu -- host side of the B200 DSMC engine: handle, device memory, launch
+// sequence of one timestep (captured into CUDA graphs), full sort, diagnostics and the C ABI
+// declared in include/dsmc.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dsmc.h"
+#include "dsmc_kernels.cuh"
+#include "dsmc_setup.h"
+
+using namespace dsmc;
+
+namespace {
+
+struct Fail {
+    dsmc_status st;
+    std::string msg;
+};
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? DSMC_ERR_ALLOC : DSMC_ERR_CUDA,           \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};                        \
+    } while (0)
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        free();
+        n = count;
+        if (count) CU(cudaMalloc((void**)&p, count * sizeof(T)));
+    }
+    void free() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { free(); }
+};
+
+const char* kKernelNames[] = {"tile_pass_plan", "scan_reduce", "scan_top",  "scan_down",
+                              "mover_place",    "mover_rank",  "tile_pass_commit", "finalize"};
+constexpr int kNumStepKernels = 8;
+
+}  // namespace
+
+struct dsmc_handle {
+    std::string last_error;
+    virtual ~dsmc_handle() {}
+    virtual void init(uint64_t seed) = 0;
+    virtual void step(int n) = 0;
+    virtual void sync() = 0;
+    virtual void diag(int cloud, dsmc_diag* out) = 0;
+    virtual void get_state(dsmc_state_buffers* out) = 0;
+    virtual void set_state(const dsmc_state_buffers* in) = 0;
+    virtual void get_cell_starts(int32_t* start, int64_t cap, int64_t* total) = 0;
+    virtual void get_sigvrmax(void* out, int64_t cap) = 0;
+    virtual void set_sigvrmax(const void* in, int64_t n) = 0;
+    virtual void set_stream(cudaStream_t s) = 0;
+    virtual void set_profiling(bool on) = 0;
+    virtual void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) = 0;
+};
+
+namespace {
+
+template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
+    typedef typename V4T<R>::type R4;
+    // configuration
+    dsmc_params run{};
+    std::vector<dsmc_cloud_params> cp;
+    std::vector<CloudPhys<R>> phys;
+    int nclouds = 0;
+    int total_cells = 0;
+    int capacity = 0;
+    int max_tiles = 0;
+    int tile_nominal = 0;
+    int nscan_blocks = 0;
+    std::vector<int> cloud_atoms_init;  // initial atoms per cloud
+    std::vector<int> cloud_cell_base;
+    // device memory
+    DevBuf<R4> pos[2], vel[2], psi[2];
+    DevBuf<int> start[2], tile_begin[2], tile_cloud[2];
+    DevBuf<int> Lc, Ic, mover_base, in_list, tile_movers, tile_ovf, tile_ovf_carry;
+    DevBuf<int4> mrec;
+    DevBuf<R> sigvrmax;
+    DevBuf<TilePartial> partials;
+    DevBuf<CloudPhys<R>> d_phys;
+    DevBuf<CloudDyn> cdyn;
+    DevBuf<CloudDiagDev> cdiag;
+    DevBuf<Ctl> ctl;
+    DevBuf<int> block_sums, block_off, scan_blk_cloud, scan_blk_cell0, cloud_first_blk;
+    // runtime
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int parity = 0;
+    bool initialised = false;
+    int64_t steps_taken = 0;
+    Args<R> args[2];
+    cudaGraphExec_t graph2 = nullptr;  // two steps: parity 0 then 1
+    bool use_graphs = true;
+    bool profiling = false;
+    double prof_ms[kNumStepKernels] = {0};
+    int64_t prof_n[kNumStepKernels] = {0};
+    cudaEvent_t ev[kNumStepKernels + 1] = {};
+    size_t smem_tile = 0;
+
+    Engine(const dsmc_params& r, const dsmc_cloud_params* clouds, int n) {
+        run = r;
+        nclouds = n;
+        cp.assign(clouds, clouds + n);
+        use_graphs = r.use_graphs != 0;
+        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP / 2;
+        if (tile_nominal > CAP / 2) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP / 2)};
+        if (tile_nominal < 32) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= 32"};
+        build_phys();
+        allocate();
+        CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        own_stream = true;
+        for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
+        smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int));
+        CU(cudaFuncSetAttribute(tile_pass<R, BLOCK, CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_tile));
+        CU(cudaFuncSetAttribute(tile_pass<R, BLOCK, CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_tile));
+        build_args();
+    }
+
+    ~Engine() override {
+        if (graph2) cudaGraphExecDestroy(graph2);
+        for (int i = 0; i <= kNumStepKernels; ++i)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    // ------------------------------------------------------------------ parameters
+    void build_phys() {
+        phys.resize(nclouds);
+        cloud_cell_base.resize(nclouds + 1);
+        cloud_atoms_init.resize(nclouds);
+        int64_t cells = 0, cap = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            const dsmc_cloud_params& c = cp[k];
+            const std::string bad = validate_cloud(run, c, k);
+            if (!bad.empty()) throw Fail{DSMC_ERR_INVALID, bad};
+            if (cells + cloud_cells(c) >= ((int64_t)1 << 31)) throw Fail{DSMC_ERR_INVALID, "more than 2^31 cells"};
+            make_cloud_phys<R>(run, c, k, (int)cells, phys[k]);
+            cloud_cell_base[k] = (int)cells;
+            cells += cloud_cells(c);
+            cap += c.capacity > 0 ? c.capacity : c.n_atoms;
+            cloud_atoms_init[k] = (int)c.n_atoms;
+        }
+        cloud_cell_base[nclouds] = (int)cells;
+        if (cap >= ((int64_t)1 << 31)) throw Fail{DSMC_ERR_INVALID, "more than 2^31 atoms"};
+        total_cells = (int)cells;
+        capacity = (int)std::max<int64_t>(cap, 1);
+        max_tiles = capacity / tile_nominal + nclouds + 2;
+    }
+
+    void allocate() {
+        for (int i = 0; i < 2; ++i) {
+            pos[i].alloc(capacity); vel[i].alloc(capacity); psi[i].alloc(capacity);
+            start[i].alloc(total_cells + 1);
+            tile_begin[i].alloc(max_tiles + 1);
+            tile_cloud[i].alloc(max_tiles);
+            CU(cudaMemset(start[i].p, 0, (total_cells + 1) * sizeof(int)));
+            CU(cudaMemset(tile_begin[i].p, 0, (max_tiles + 1) * sizeof(int)));
+            CU(cudaMemset(tile_cloud[i].p, 0, max_tiles * sizeof(int)));
+        }
+        Lc.alloc(total_cells); Ic.alloc(total_cells); mover_base.alloc(total_cells);
+        CU(cudaMemset(Lc.p, 0, total_cells * sizeof(int)));
+        CU(cudaMemset(Ic.p, 0, total_cells * sizeof(int)));
+        in_list.alloc(capacity);
+        mrec.alloc(capacity);
+        tile_movers.alloc(max_tiles); tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles);
+        sigvrmax.alloc(total_cells);
+        partials.alloc(max_tiles);
+        d_phys.alloc(nclouds);
+        CU(cudaMemcpy(d_phys.p, phys.data(), nclouds * sizeof(CloudPhys<R>), cudaMemcpyHostToDevice));
+        cdyn.alloc(nclouds); cdiag.alloc(nclouds); ctl.alloc(1);
+        CU(cudaMemset(cdyn.p, 0, nclouds * sizeof(CloudDyn)));
+        CU(cudaMemset(cdiag.p, 0, nclouds * sizeof(CloudDiagDev)));
+        CU(cudaMemset(ctl.p, 0, sizeof(Ctl)));
+        // scan blocks: each covers up to SCAN_CHUNK cells of a single cloud
+        std::vector<int> bc, b0, first(nclouds + 1);
+        for (int k = 0; k < nclouds; ++k) {
+            first[k] = (int)bc.size();
+            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += SCAN_CHUNK) {
+                bc.push_back(k);
+                b0.push_back(c);
+            }
+        }
+        first[nclouds] = (int)bc.size();
+        nscan_blocks = (int)bc.size();
+        scan_blk_cloud.alloc(nscan_blocks); scan_blk_cell0.alloc(nscan_blocks); cloud_first_blk.alloc(nclouds + 1);
+        block_sums.alloc(nscan_blocks); block_off.alloc(nscan_blocks);
+        CU(cudaMemcpy(scan_blk_cloud.p, bc.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(scan_blk_cell0.p, b0.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(cloud_first_blk.p, first.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    }
+
+    void build_args() {
+        for (int p = 0; p < 2; ++p) {
+            Args<R>& A = args[p];
+            memset(&A, 0, sizeof(A));
+            const int q = 1 - p;
+            A.pos_in = pos[p].p; A.vel_in = vel[p].p; A.psi_in = psi[p].p;
+            A.pos_out = pos[q].p; A.vel_out = vel[q].p; A.psi_out = psi[q].p;
+            A.old_start = start[p].p; A.new_start = start[q].p;
+            A.Lc = Lc.p; A.Ic = Ic.p; A.mover_base = mover_base.p;
+            A.sigvrmax = sigvrmax.p;
+            A.mrec = mrec.p; A.in_list = in_list.p;
+            A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p;
+            A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
+            A.tile_movers = tile_movers.p; A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
+            A.partials = partials.p;
+            A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
+            A.block_sums = block_sums.p; A.block_off = block_off.p;
+            A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
+            A.cloud_first_blk = cloud_first_blk.p;
+            A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
+            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal;
+            A.collide_every = run.collide_every; A.parity = p; A.init_mode = 0;
+            A.seed = run.seed;
+            A.capacity = capacity;
+        }
+    }
+
+    // ------------------------------------------------------------------ launches
+    void launch_step_kernel(int which, const Args<R>& A) {
+        switch (which) {
+        case 0:
+            tile_pass<R, BLOCK, CAP, false><<<max_tiles, BLOCK, smem_tile, stream>>>(A);
+            break;
+        case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
+        case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
+        case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
+        case 4: mover_place<R><<<max_tiles, 256, 0, stream>>>(A); break;
+        case 5: mover_rank<R><<<max_tiles, 256, 0, stream>>>(A); break;
+        case 6:
+            tile_pass<R, BLOCK, CAP, true><<<max_tiles, BLOCK, smem_tile, stream>>>(A);
+            break;
+        case 7: finalize<R, false><<<nclouds, 256, 0, stream>>>(A); break;
+        }
+    }
+
+    void enqueue_step(int p) {
+        for (int k = 0; k < kNumStepKernels; ++k) launch_step_kernel(k, args[p]);
+    }
+
+    void build_graph() {
+        if (graph2) return;
+        cudaGraph_t g;
+        CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(0);
+        enqueue_step(1);
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) throw Fail{DSMC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)};
+        e = cudaGraphInstantiate(&graph2, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) throw Fail{DSMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)};
+    }
+
+    void step(int n) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "dsmc_step before dsmc_init_cloud / dsmc_set_state"};
+        if (n < 0) throw Fail{DSMC_ERR_INVALID, "nsteps < 0"};
+        int done = 0;
+        if (profiling) {
+            for (; done < n; ++done) {
+                for (int k = 0; k < kNumStepKernels; ++k) {
+                    CU(cudaEventRecord(ev[k], stream));
+                    launch_step_kernel(k, args[parity]);
+                }
+                CU(cudaEventRecord(ev[kNumStepKernels], stream));
+                CU(cudaEventSynchronize(ev[kNumStepKernels]));
+                for (int k = 0; k < kNumStepKernels; ++k) {
+                    float ms = 0;
+                    CU(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+                    prof_ms[k] += ms;
+                    prof_n[k] += 1;
+                }
+                parity ^= 1;
+            }
+        } else {
+            if (use_graphs && n - done >= 2) build_graph();
+            if (use_graphs && parity == 1 && n - done >= 1) {
+                enqueue_step(1);
+                parity = 0;
+                ++done;
+            }
+            while (use_graphs && n - done >= 2) {
+                CU(cudaGraphLaunch(graph2, stream));
+                done += 2;
+            }
+            for (; done < n; ++done) {
+                enqueue_step(parity);
+                parity ^= 1;
+            }
+        }
+        CU(cudaGetLastError());
+        steps_taken += n;
+    }
+
+    void sync() override { CU(cudaStreamSynchronize(stream)); }
+
+    void set_stream(cudaStream_t s) override {
+        sync();
+        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        own_stream = false;
+        stream = s;
+    }
+
+    // ------------------------------------------------------------------ init + full sort
+    // Sorts ps/vs/ss (atoms grouped by cloud, counts[k] per cloud) into buffer set 0. The cell
+    // scan runs with parity 1 as "current" (zero atoms, zero old starts) so that its "next"
+    // outputs land in set 0; then measures the sorted state.
+    void sort_and_measure(const R4* ps, const R4* vs, const R4* ss, const std::vector<int>& counts) {
+        int n = 0;
+        std::vector<int> off(nclouds + 1, 0);
+        for (int k = 0; k < nclouds; ++k) { off[k] = n; n += counts[k]; }
+        off[nclouds] = n;
+        DevBuf<int> d_off, cell, ticket, oflag, orank, gb;
+        d_off.alloc(nclouds + 1);
+        CU(cudaMemcpyAsync(d_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        const int nn = std::max(n, 1);
+        cell.alloc(nn); ticket.alloc(nn); oflag.alloc(nn); orank.alloc(nn);
+        const int gblocks = (nn + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        gb.alloc(gblocks);
+        // reset bookkeeping: parity 1 is "current" with zero atoms, old starts all zero
+        CU(cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), stream));
+        CU(cudaMemsetAsync(start[1].p, 0, (total_cells + 1) * sizeof(int), stream));
+        CU(cudaMemsetAsync(Lc.p, 0, total_cells * sizeof(int), stream));
+        CU(cudaMemsetAsync(Ic.p, 0, total_cells * sizeof(int), stream));
+        Args<R> A = args[1];
+        A.init_mode = 1;
+        SortArgs<R> S;
+        S.pos_src = ps; S.vel_src = vs; S.psi_src = ss;
+        S.pos_dst = pos[0].p; S.vel_dst = vel[0].p; S.psi_dst = psi[0].p;
+        S.cloud_atom_off = d_off.p;
+        S.cell = cell.p; S.ticket = ticket.p; S.ovf_flag = oflag.p; S.ovf_rank = orank.p;
+        S.n = n; S.nclouds = nclouds;
+        const int ab = (n + 255) / 256;
+        if (n > 0) fs_cells<R><<<ab, 256, 0, stream>>>(S, A);
+        if (n > 0) {
+            gscan_reduce<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p);
+            gscan_top<<<1, 1024, 0, stream>>>(gb.p, gblocks, nullptr);
+            gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p, orank.p);
+        }
+        scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
+        scan_top<R><<<1, 1024, 0, stream>>>(A);
+        scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
+        if (n > 0) {
+            fs_place<R><<<ab, 256, 0, stream>>>(S, A);
+            fs_scatter<R><<<ab, 256, 0, stream>>>(S, A);
+        }
+        CU(cudaGetLastError());
+        parity = 0;
+        // step counter and diagnostics of the sorted state
+        measure_tiles<R, 256><<<max_tiles, 256, 0, stream>>>(args[0]);
+        finalize<R, true><<<nclouds, 256, 0, stream>>>(args[0]);
+        CU(cudaGetLastError());
+        CU(cudaStreamSynchronize(stream));
+        initialised = true;
+        steps_taken = 0;
+        check_err();
+    }
+
+    void init(uint64_t seed) override {
+        run.seed = seed;
+        for (int p = 0; p < 2; ++p) args[p].seed = seed;
+        int n = 0;
+        std::vector<int> off(nclouds + 1, 0), modes(nclouds);
+        for (int k = 0; k < nclouds; ++k) {
+            off[k] = n;
+            n += cloud_atoms_init[k];
+            modes[k] = cp[k].init_mode;
+        }
+        off[nclouds] = n;
+        DevBuf<int> d_off, d_modes;
+        d_off.alloc(nclouds + 1);
+        d_modes.alloc(nclouds);
+        CU(cudaMemcpyAsync(d_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_modes.p, modes.data(), nclouds * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), stream));
+        if (n > 0)
+            init_atoms<R><<<(n + 255) / 256, 256, 0, stream>>>(args[0], d_off.p, n, d_modes.p, pos[1].p, vel[1].p,
+                                                                psi[1].p, (unsigned long long)seed);
+        // (sigma v_r)max per cell
+        std::vector<R> sv(nclouds);
+        for (int k = 0; k < nclouds; ++k) sv[k] = (R)default_sigvrmax(run, cp[k]);
+        DevBuf<R> d_sv;
+        DevBuf<int> d_cb;
+        d_sv.alloc(nclouds);
+        d_cb.alloc(nclouds + 1);
+        CU(cudaMemcpyAsync(d_sv.p, sv.data(), nclouds * sizeof(R), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_cb.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        fill_sigvrmax<R><<<(total_cells + 255) / 256, 256, 0, stream>>>(sigvrmax.p, d_cb.p, d_sv.p, nclouds, total_cells);
+        CU(cudaGetLastError());
+        sort_and_measure(pos[1].p, vel[1].p, psi[1].p, cloud_atoms_init);
+    }
+
+    void check_err() {
+        Ctl h;
+        CU(cudaMemcpyAsync(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        if (h.err) {
+            std::string m = "device error bits 0x" + std::to_string(h.err) + ":";
+            dsmc_status st = DSMC_ERR_CUDA;
+            if (h.err & EB_CELL_FULL) { m += " a cell holds more atoms than a tile can stage;"; st = DSMC_ERR_CELL_FULL; }
+            if (h.err & EB_NAN) { m += " non-finite velocity;"; st = DSMC_ERR_NAN; }
+            if (h.err & EB_INIT_REJECT) { m += " initial rejection sampling gave up;"; st = DSMC_ERR_INVALID; }
+            if (h.err & EB_TILE_OVERFLOW) { m += " tile table overflow;"; st = DSMC_ERR_CAPACITY; }
+            if (h.err & EB_INCONSISTENT) { m += " inconsistent cell bookkeeping (after an earlier error);"; }
+            throw Fail{st, m};
+        }
+    }
+
+    // ------------------------------------------------------------------ diagnostics / state
+    void diag(int cloud, dsmc_diag* out) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "diagnostics before init"};
+        if (cloud < -1 || cloud >= nclouds) throw Fail{DSMC_ERR_INVALID, "cloud index out of range"};
+        std::vector<CloudDiagDev> g(nclouds);
+        CU(cudaMemcpyAsync(g.data(), cdiag.p, nclouds * sizeof(CloudDiagDev), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        CU(cudaGetLastError());
+        int k0 = cloud < 0 ? 0 : cloud, k1 = cloud < 0 ? nclouds : cloud + 1;
+        CloudDiagDev s;
+        memset(&s, 0, sizeof(s));
+        double e_kin = 0, e_pot = 0, e_evap = 0;
+        double msum = 0;
+        int err = 0;
+        for (int k = k0; k < k1; ++k) {
+            const CloudDiagDev& d = g[k];
+            const CloudPhys<R>& P = phys[k];
+            s.step = d.step;
+            s.n_alive += d.n_alive;
+            s.sum_v2 += d.sum_v2;
+            s.sum_B += d.sum_B;
+            s.cum_evap += d.cum_evap; s.cum_maj += d.cum_maj; s.cum_knife += d.cum_knife;
+            s.cum_coll += d.cum_coll; s.cum_cand += d.cum_cand;
+            s.cum_atom_steps += d.cum_atom_steps;
+            e_kin += 0.5 * P.mass * fx_to_double(d.sum_v2);
+            e_pot += P.moment * fx_to_double(d.sum_B);
+            e_evap += 0.5 * P.mass * fx_to_double(d.cum_evap_v2) + P.moment * fx_to_double(d.cum_evap_B);
+            msum += P.mass * fx_to_double(d.sum_v2);
+            err |= (int)d.err;
+        }
+        memset(out, 0, sizeof(*out));
+        out->step = s.step;
+        out->time = (double)s.step * run.dt;
+        out->n_alive = s.n_alive;
+        out->e_kin = e_kin;
+        out->e_pot = e_pot;
+        out->sum_v2 = fx_to_double(s.sum_v2);
+        out->sum_absB = fx_to_double(s.sum_B);
+        out->temperature = s.n_alive > 0 ? msum / (3.0 * phys[k0].kB * (double)s.n_alive) : 0.0;
+        out->n_evaporated = s.cum_evap;
+        out->n_majorana = s.cum_maj;
+        out->n_knife = s.cum_knife;
+        out->e_evaporated = e_evap;
+        out->collisions = s.cum_coll;
+        out->candidates = s.cum_cand;
+        out->atom_steps = s.cum_atom_steps;
+        Ctl h;
+        CU(cudaMemcpy(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        out->error = h.err | err;
+    }
+
+    void get_state(dsmc_state_buffers* o) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "get_state before init"};
+        sync();
+        Ctl h;
+        CU(cudaMemcpy(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        const int n = h.n[parity];
+        if (o->n < n) throw Fail{DSMC_ERR_INVALID, "state buffers too small: need " + std::to_string(n)};
+        std::vector<CloudDyn> d(nclouds);
+        CU(cudaMemcpy(d.data(), cdyn.p, nclouds * sizeof(CloudDyn), cudaMemcpyDeviceToHost));
+        if (o->pos) CU(cudaMemcpyAsync(o->pos, pos[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        if (o->vel) CU(cudaMemcpyAsync(o->vel, vel[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        if (o->psi) CU(cudaMemcpyAsync(o->psi, psi[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        o->n = n;
+        if (o->cloud_counts)
+            for (int k = 0; k < nclouds; ++k) o->cloud_counts[k] = d[k].n[parity];
+    }
+
+    void set_state(const dsmc_state_buffers* in) override {
+        if (!in || !in->pos || !in->vel || !in->psi || !in->cloud_counts)
+            throw Fail{DSMC_ERR_INVALID, "set_state needs pos, vel, psi and cloud_counts"};
+        std::vector<int> counts(nclouds);
+        int64_t tot = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            if (in->cloud_counts[k] < 0) throw Fail{DSMC_ERR_INVALID, "negative cloud count"};
+            counts[k] = (int)in->cloud_counts[k];
+            tot += in->cloud_counts[k];
+        }
+        if (tot != in->n) throw Fail{DSMC_ERR_INVALID, "cloud_counts do not add up to n"};
+        if (tot > capacity) throw Fail{DSMC_ERR_CAPACITY, "more atoms than the handle's capacity"};
+        CU(cudaMemcpyAsync(pos[1].p, in->pos, (size_t)tot * sizeof(R4), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(vel[1].p, in->vel, (size_t)tot * sizeof(R4), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(psi[1].p, in->psi, (size_t)tot * sizeof(R4), cudaMemcpyHostToDevice, stream));
+        if (!initialised) {
+            // sigvrmax defaults as at init
+            std::vector<R> sv(total_cells);
+            for (int k = 0; k < nclouds; ++k) {
+                const R v = (R)default_sigvrmax(run, cp[k]);
+                for (int cc = cloud_cell_base[k]; cc < cloud_cell_base[k + 1]; ++cc) sv[cc] = v;
+            }
+            CU(cudaMemcpyAsync(sigvrmax.p, sv.data(), total_cells * sizeof(R), cudaMemcpyHostToDevice, stream));
+            CU(cudaStreamSynchronize(stream));
+        }
+        sort_and_measure(pos[1].p, vel[1].p, psi[1].p, counts);
+    }
+
+    void get_cell_starts(int32_t* st, int64_t cap, int64_t* total) override {
+        if (total) *total = total_cells;
+        if (!st) return;
+        if (cap < total_cells + 1) throw Fail{DSMC_ERR_INVALID, "cell start buffer too small"};
+        sync();
+        CU(cudaMemcpy(st, start[parity].p, (total_cells + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+
+    void get_sigvrmax(void* out, int64_t cap) override {
+        if (cap < total_cells) throw Fail{DSMC_ERR_INVALID, "sigvrmax buffer too small"};
+        sync();
+        CU(cudaMemcpy(out, sigvrmax.p, total_cells * sizeof(R), cudaMemcpyDeviceToHost));
+    }
+    void set_sigvrmax(const void* in, int64_t n) override {
+        if (n != total_cells) throw Fail{DSMC_ERR_INVALID, "sigvrmax length must equal the number of cells"};
+        sync();
+        CU(cudaMemcpy(sigvrmax.p, in, total_cells * sizeof(R), cudaMemcpyHostToDevice));
+    }
+
+    void set_profiling(bool on) override {
+        profiling = on;
+        for (int k = 0; k < kNumStepKernels; ++k) { prof_ms[k] = 0; prof_n[k] = 0; }
+    }
+    void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) override {
+        const int n = std::min(cap, kNumStepKernels);
+        for (int k = 0; k < n; ++k) {
+            if (names) names[k] = kKernelNames[k];
+            if (ms) ms[k] = prof_ms[k];
+            if (launches) launches[k] = prof_n[k];
+        }
+        if (count) *count = kNumStepKernels;
+    }
+};
+
+template <class F> dsmc_status guard(dsmc_handle* h, F&& f) {
+    try {
+        f();
+        if (h) h->last_error.clear();
+        return DSMC_OK;
+    } catch (const Fail& e) {
+        if (h) h->last_error = e.msg;
+        return e.st;
+    } catch (const std::exception& e) {
+        if (h) h->last_error = e.what();
+        return DSMC_ERR_ALLOC;
+    }
+}
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+// ====================================================================================== C ABI
+DSMC_API int32_t dsmc_abi_version(void) { return DSMC_ABI_VERSION; }
+
+DSMC_API const char* dsmc_status_string(dsmc_status s) {
+    switch (s) {
+    case DSMC_OK: return "ok";
+    case DSMC_ERR_INVALID: return "invalid argument";
+    case DSMC_ERR_CUDA: return "CUDA error";
+    case DSMC_ERR_ALLOC: return "allocation failed";
+    case DSMC_ERR_CAPACITY: return "capacity exceeded";
+    case DSMC_ERR_CELL_FULL: return "cell too full for one tile";
+    case DSMC_ERR_NAN: return "non-finite state";
+    case DSMC_ERR_STATE: return "call out of order";
+    case DSMC_ERR_UNSUPPORTED: return "unsupported";
+    case DSMC_ERR_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+DSMC_API const char* dsmc_last_error(const dsmc_handle* h) {
+    return h ? h->last_error.c_str() : g_create_error.c_str();
+}
+
+DSMC_API dsmc_status dsmc_preset(int32_t which, dsmc_params* run, dsmc_cloud_params* c) {
+    if (!run || !c) return DSMC_ERR_INVALID;
+    return fill_preset(which, run, c);
+}
+
+DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params* clouds, int32_t nclouds,
+                                 dsmc_handle** out) {
+    g_create_error.clear();
+    if (!run || !clouds || nclouds < 1 || !out) {
+        g_create_error = "dsmc_create: null argument or nclouds < 1";
+        return DSMC_ERR_INVALID;
+    }
+    *out = nullptr;
+    try {
+        int dev_count = 0;
+        cudaError_t e = cudaGetDeviceCount(&dev_count);
+        if (e != cudaSuccess || dev_count < 1) {
+            g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+            return DSMC_ERR_CUDA;
+        }
+        if (run->precision == DSMC_FP32)
+            *out = new Engine<float, 256, 2048>(*run, clouds, nclouds);
+        else if (run->precision == DSMC_FP64)
+            *out = new Engine<double, 256, 1024>(*run, clouds, nclouds);
+        else {
+            g_create_error = "precision must be DSMC_FP32 or DSMC_FP64";
+            return DSMC_ERR_INVALID;
+        }
+        return DSMC_OK;
+    } catch (const Fail& f) {
+        g_create_error = f.msg;
+        return f.st;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return DSMC_ERR_ALLOC;
+    }
+}
+
+DSMC_API dsmc_status dsmc_destroy(dsmc_handle* h) {
+    delete h;
+    return DSMC_OK;
+}
+
+#define NEED_H                                                                                     \
+    if (!h) return DSMC_ERR_INVALID
+
+DSMC_API dsmc_status dsmc_set_stream(dsmc_handle* h, void* s) {
+    NEED_H;
+    return guard(h, [&] { h->set_stream((cudaStream_t)s); });
+}
+DSMC_API dsmc_status dsmc_init_cloud(dsmc_handle* h, uint64_t seed) {
+    NEED_H;
+    return guard(h, [&] { h->init(seed); });
+}
+DSMC_API dsmc_status dsmc_step(dsmc_handle* h, int32_t n) {
+    NEED_H;
+    return guard(h, [&] { h->step(n); });
+}
+DSMC_API dsmc_status dsmc_synchronize(dsmc_handle* h) {
+    NEED_H;
+    return guard(h, [&] { h->sync(); });
+}
+DSMC_API dsmc_status dsmc_diagnostics(dsmc_handle* h, int32_t cloud, dsmc_diag* out) {
+    NEED_H;
+    if (!out) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->diag(cloud, out); });
+}
+DSMC_API dsmc_status dsmc_get_state(dsmc_handle* h, dsmc_state_buffers* out) {
+    NEED_H;
+    if (!out) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->get_state(out); });
+}
+DSMC_API dsmc_status dsmc_set_state(dsmc_handle* h, const dsmc_state_buffers* in) {
+    NEED_H;
+    return guard(h, [&] { h->set_state(in); });
+}
+DSMC_API dsmc_status dsmc_get_cell_starts(dsmc_handle* h, int32_t* st, int64_t cap, int64_t* total) {
+    NEED_H;
+    return guard(h, [&] { h->get_cell_starts(st, cap, total); });
+}
+DSMC_API dsmc_status dsmc_get_sigvrmax(dsmc_handle* h, void* out, int64_t cap) {
+    NEED_H;
+    if (!out) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->get_sigvrmax(out, cap); });
+}
+DSMC_API dsmc_status dsmc_set_sigvrmax(dsmc_handle* h, const void* in, int64_t n) {
+    NEED_H;
+    if (!in) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->set_sigvrmax(in, n); });
+}
+DSMC_API dsmc_status dsmc_set_profiling(dsmc_handle* h, int32_t on) {
+    NEED_H;
+    return guard(h, [&] { h->set_profiling(on != 0); });
+}
+DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, double* ms, int64_t* launches,
+                                       int32_t cap, int32_t* count) {
+    NEED_H;
+    return guard(h, [&] { h->kernel_times(names, ms, launches, cap, count); });
+}
+DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h) { return h ? kNumStepKernels : 0; }

@@ -1,0 +1,859 @@
+// dsmc_kernels.cuh -- sm_100a kernels of one DSMC timestep.
+//
+// Data layout in HBM (per precision R = float | double, R4 = float4 | double4):
+//   pos[i] = (x, y, z, atom id bits)   vel[i] = (vx, vy, vz, flag bits)   psi[i] = (u_re, u_im, d_re, d_im)
+//   three structure-of-arrays streams of 16 B (FP32) per atom, double-buffered; atoms are kept
+//   sorted by global cell (clouds one after another, each cloud's grid cells then its overflow
+//   cell), so every cell is a contiguous range and start[c] gives its first atom.
+//
+// One step = 8 launches, all sized statically so the sequence can be captured in a CUDA graph:
+//   tile_pass<PLAN>   per tile: collide its cells, move every atom, classify stayer/mover/lost,
+//                     count leavers L[c] and incoming movers I[c], record movers
+//   scan_reduce/top/down   new per-cell counts n_c - L_c + I_c -> new start[], next tiling,
+//                     mover base per cell, overflow carries
+//   mover_place / mover_rank   deterministic rank of incoming movers by their old index
+//   tile_pass<COMMIT> recompute the identical step, write every surviving atom at its sorted
+//                     destination, per-tile exact diagnostics
+//   finalize          per-cloud diagnostics, knife temperature, step counter
+// The sort is stable by (new cell, moved?, old index): in each new cell the atoms that stayed
+// keep their previous order and are followed by the atoms that entered it, by old index.
+// Tiles are contiguous, cloud-pure atom ranges of ~T atoms whose boundaries snap to cell starts
+// (the overflow cell, which never collides, is split at nominal boundaries).
+#ifndef DSMC_KERNELS_CUH
+#define DSMC_KERNELS_CUH
+
+#include <cuda_runtime.h>
+#include "dsmc_physics.h"
+
+namespace dsmc {
+
+template <class R> struct V4T;
+template <> struct V4T<float> { typedef float4 type; };
+template <> struct V4T<double> { typedef double4 type; };
+
+enum : int {
+    EB_CELL_FULL = 1,
+    EB_NAN = 2,
+    EB_CAPACITY = 4,
+    EB_INIT_REJECT = 8,
+    EB_TILE_OVERFLOW = 16,
+    EB_INCONSISTENT = 32
+};
+
+struct __align__(16) TilePartial {
+    i128 sum_v2, sum_B, evap_v2, evap_B;
+    long long n_alive, n_maj, n_knife, coll, cand, pad0, pad1, pad2;
+};
+
+struct CloudDyn {
+    int n[2];         // atoms, by parity
+    int start[2];     // first atom index, by parity
+    int tile_off[2];  // first tile, by parity
+    int ntiles[2];
+    double T_knife;   // temperature used by the knife of the coming step
+    double pad;
+};
+
+struct __align__(16) CloudDiagDev {
+    i128 sum_v2, sum_B, cum_evap_v2, cum_evap_B;
+    long long step, n_alive, cum_evap, cum_maj, cum_knife, cum_coll, cum_cand, err, cum_atom_steps, pad;
+};
+
+struct Ctl {
+    int n[2];
+    int ntiles[2];
+    int step[2];
+    int err;
+    int pad;
+};
+
+template <class R> struct Args {
+    typedef typename V4T<R>::type R4;
+    const R4* pos_in;
+    const R4* vel_in;
+    const R4* psi_in;
+    R4* pos_out;
+    R4* vel_out;
+    R4* psi_out;
+    const int* old_start;
+    int* new_start;
+    int* Lc;
+    int* Ic;
+    int* mover_base;
+    R* sigvrmax;
+    int4* mrec;
+    int* in_list;
+    const int* tile_begin;
+    const int* tile_cloud;
+    int* tile_begin_next;
+    int* tile_cloud_next;
+    int* tile_movers;
+    int* tile_ovf;
+    int* tile_ovf_carry;
+    TilePartial* partials;
+    const CloudPhys<R>* clouds;
+    CloudDyn* cdyn;
+    CloudDiagDev* cdiag;
+    Ctl* ctl;
+    int* block_sums;
+    int* block_off;
+    const int* scan_blk_cloud;
+    const int* scan_blk_cell0;
+    const int* cloud_first_blk;  // nclouds + 1
+    int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
+    int capacity;
+    unsigned long long seed;
+};
+
+// ---------------------------------------------------------------------------------------------
+// block-wide helpers
+// ---------------------------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t* wsum, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = BLOCK / 32;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < NW ? wsum[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < NW) wsum[lane] = w;
+    }
+    __syncthreads();
+    uint32_t off = warp ? wsum[warp - 1] : 0u;
+    total = wsum[NW - 1];
+    __syncthreads();
+    return off + x - v;
+}
+
+__device__ __forceinline__ i128 shfl_down_i128(i128 v, int o) {
+    unsigned long long lo = (unsigned long long)v;
+    long long hi = (long long)(v >> 64);
+    lo = __shfl_down_sync(0xffffffffu, lo, o);
+    hi = __shfl_down_sync(0xffffffffu, hi, o);
+    return (i128)(((unsigned __int128)(unsigned long long)hi << 64) | (unsigned __int128)lo);
+}
+__device__ __forceinline__ i128 warp_sum_i128(i128 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += shfl_down_i128(v, o);
+    return v;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// reduce 4 i128 + 5 int64 over the block into p (thread 0 holds the result)
+template <int BLOCK>
+__device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial* sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = BLOCK / 32;
+    t.sum_v2 = warp_sum_i128(t.sum_v2);
+    t.sum_B = warp_sum_i128(t.sum_B);
+    t.evap_v2 = warp_sum_i128(t.evap_v2);
+    t.evap_B = warp_sum_i128(t.evap_B);
+    t.n_alive = warp_sum_ll(t.n_alive);
+    t.n_maj = warp_sum_ll(t.n_maj);
+    t.n_knife = warp_sum_ll(t.n_knife);
+    t.coll = warp_sum_ll(t.coll);
+    t.cand = warp_sum_ll(t.cand);
+    if (lane == 0) sm[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < NW; ++w) {
+            t.sum_v2 += sm[w].sum_v2;
+            t.sum_B += sm[w].sum_B;
+            t.evap_v2 += sm[w].evap_v2;
+            t.evap_B += sm[w].evap_B;
+            t.n_alive += sm[w].n_alive;
+            t.n_maj += sm[w].n_maj;
+            t.n_knife += sm[w].n_knife;
+            t.coll += sm[w].coll;
+            t.cand += sm[w].cand;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void zero_partial(TilePartial& t) {
+    t.sum_v2 = 0; t.sum_B = 0; t.evap_v2 = 0; t.evap_B = 0;
+    t.n_alive = 0; t.n_maj = 0; t.n_knife = 0; t.coll = 0; t.cand = 0;
+    t.pad0 = 0; t.pad1 = 0; t.pad2 = 0;
+}
+
+template <class R>
+__device__ __forceinline__ void load_cloud(CloudPhys<R>& dst, const CloudPhys<R>* src) {
+    static_assert(sizeof(CloudPhys<R>) % 4 == 0, "cloud params must be word sized");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(CloudPhys<R>) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+template <class R>
+__device__ __forceinline__ R knife_cut_for(const CloudPhys<R>& P, double T, int step) {
+    if (!(P.flags & F_KNIFE)) return R(0);
+    double eta = knife_eta(P.knife_nknots, P.knife_step, P.knife_eta, (double)step);
+    return (R)knife_cut_v2(eta, P.kB, T, P.mass);
+}
+
+// ---------------------------------------------------------------------------------------------
+// tile_pass: the fused collide + move + classify kernel, run twice per step.
+//   COMMIT = false (plan):   leaver / mover counts, mover records, overflow stayers per tile
+//   COMMIT = true  (commit): the same arithmetic again, then scatter + diagnostics
+// Shared memory per tile: pos, vel (R4 each), old cell (int), packed prefix (uint32) x CAP atoms.
+// ---------------------------------------------------------------------------------------------
+template <class R, int BLOCK, int CAP, bool COMMIT>
+__global__ void __launch_bounds__(BLOCK) tile_pass(Args<R> A) {
+    typedef typename V4T<R>::type R4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R4* s_pos = reinterpret_cast<R4*>(smem_raw);
+    R4* s_vel = s_pos + CAP;
+    int* s_cell = reinterpret_cast<int*>(s_vel + CAP);
+    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_cell + CAP);
+    __shared__ CloudPhys<R> P;
+    __shared__ uint32_t wsum[32];
+    __shared__ TilePartial red[BLOCK / 32];
+
+    const int p = A.parity;
+    const int b = blockIdx.x;
+    if (b >= A.ctl->ntiles[p]) return;
+    const int tb = A.tile_begin[b];
+    const int te = A.tile_begin[b + 1];
+    const int L = te - tb;
+    const int cloud = A.tile_cloud[b];
+    if (L > CAP || L < 0) {
+        // cannot stage this tile: flag it and leave a consistent, empty contribution so that
+        // every later kernel only touches indices it computed itself
+        if (threadIdx.x == 0) {
+            atomicOr(&A.ctl->err, EB_CELL_FULL);
+            if (!COMMIT) {
+                A.tile_movers[b] = 0;
+                A.tile_ovf[b] = 0;
+            } else {
+                TilePartial z;
+                zero_partial(z);
+                A.partials[b] = z;
+            }
+        }
+        return;
+    }
+    load_cloud(P, A.clouds + cloud);
+    const int step = A.ctl->step[p];
+    __syncthreads();
+    const bool box = (P.trap == TRAP_BOX);
+    const R cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
+
+    // phase 1: stage the tile's positions and velocities, old cells
+    for (int t = threadIdx.x; t < L; t += BLOCK) {
+        R4 q = A.pos_in[tb + t];
+        R4 v = A.vel_in[tb + t];
+        s_pos[t] = q;
+        s_vel[t] = v;
+        s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
+    }
+    __syncthreads();
+
+    // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles)
+    long long my_coll = 0, my_cand = 0;
+    if ((P.flags & F_COLLIDE) && (step % A.collide_every) == 0) {
+        for (int t = threadIdx.x; t < L; t += BLOCK) {
+            const int c = s_cell[t];
+            if (c == P.ovf_cell) continue;
+            if (t > 0 && s_cell[t - 1] == c) continue;
+            const int n = A.old_start[c + 1] - A.old_start[c];
+            if (A.old_start[c] != tb + t || n > L - t) {  // cell not wholly inside this tile
+                atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                continue;
+            }
+            if (n < 2) continue;
+            R svm = A.sigvrmax[c];
+            CollideResult<R> cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                      (uint32_t)step, A.seed);
+            if (COMMIT) {
+                A.sigvrmax[c] = svm;
+                my_coll += cr.accepted;
+                my_cand += cr.candidates;
+            }
+        }
+        __syncthreads();
+    }
+
+    // phase 3: move + classify, in chunks of BLOCK atoms with a running packed prefix
+    TilePartial acc;
+    zero_partial(acc);
+    acc.coll = my_coll;
+    acc.cand = my_cand;
+    uint32_t carry = 0;
+    const int lane = threadIdx.x & 31;
+    for (int base = 0; base < L; base += BLOCK) {
+        const int t = base + threadIdx.x;
+        const bool valid = t < L;
+        Atom<R> a;
+        AtomOut<R> o;
+        bool stayer = false, mover = false;
+        int c_old = 0;
+        R4 q, v, s;
+        if (valid) {
+            q = s_pos[t];
+            v = s_vel[t];
+            s = A.psi_in[tb + t];
+            a.x = q.x; a.y = q.y; a.z = q.z;
+            a.vx = v.x; a.vy = v.y; a.vz = v.z;
+            a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
+            a.flags = lane_to_u32(v.w);
+            advance_atom(P, cut, a, o);
+            c_old = s_cell[t];
+            const bool alive = (o.fate == FATE_ALIVE);
+            stayer = alive && (o.cell == c_old);
+            mover = alive && !stayer;
+            if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
+        }
+        uint32_t tot;
+        uint32_t ex = block_excl_scan_u32<BLOCK>(((uint32_t)stayer << 16) | (uint32_t)mover, wsum, tot);
+        ex += carry;
+        carry += tot;
+        if (valid) s_pre[t] = ex;
+        __syncthreads();
+        if (!COMMIT) {
+            const bool leaver = valid && !stayer;
+            const unsigned lm = __ballot_sync(0xffffffffu, leaver);
+            if (leaver) {
+                const unsigned peers = __match_any_sync(lm, c_old);
+                if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
+            }
+            const unsigned mm = __ballot_sync(0xffffffffu, mover);
+            if (mover) {
+                const unsigned peers = __match_any_sync(mm, o.cell);
+                const int leader = __ffs(peers) - 1;
+                int base_ticket = 0;
+                if (lane == leader) base_ticket = atomicAdd(&A.Ic[o.cell], __popc(peers));
+                base_ticket = __shfl_sync(peers, base_ticket, leader);
+                const int ticket = base_ticket + __popc(peers & ((1u << lane) - 1u));
+                A.mrec[tb + (int)(ex & 0xFFFFu)] = make_int4(o.cell, tb + t, ticket, 0);
+            }
+        } else if (valid) {
+            int dest = -1;
+            if (stayer) {
+                const int seg = A.old_start[c_old];
+                const int sl = seg > tb ? seg - tb : 0;
+                if (sl <= t) {
+                    int rank = (int)(ex >> 16) - (int)(s_pre[sl] >> 16);
+                    if (seg < tb)
+                        rank += A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
+                    dest = A.new_start[c_old] + rank;
+                    if (dest < A.new_start[c_old] || dest >= A.new_start[c_old + 1]) dest = -2;
+                } else {
+                    dest = -2;
+                }
+            } else if (mover) {
+                dest = A.mrec[tb + (int)(ex & 0xFFFFu)].w;
+                if (dest < 0 || dest >= A.capacity) dest = -2;
+            }
+            if (dest == -2) {
+                atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            } else if (dest >= 0) {
+                R4 qo, vo, so;
+                qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
+                vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = v.w;
+                so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
+                A.pos_out[dest] = qo;
+                A.vel_out[dest] = vo;
+                A.psi_out[dest] = so;
+                acc.n_alive += 1;
+                acc.sum_v2 += fx_from((double)o.v2);
+                acc.sum_B += fx_from((double)o.absB);
+            } else if (!stayer && !mover) {
+                acc.evap_v2 += fx_from((double)o.v2);
+                acc.evap_B += fx_from((double)o.absB);
+                if (o.fate == FATE_MAJORANA) acc.n_maj += 1;
+                else acc.n_knife += 1;
+            }
+        }
+    }
+
+    if (!COMMIT) {
+        if (threadIdx.x == 0) {
+            A.tile_movers[b] = (int)(carry & 0xFFFFu);
+            int ovf = 0;
+            if (L > 0 && s_cell[L - 1] == P.ovf_cell) {
+                const int seg = A.old_start[P.ovf_cell];
+                const int sl = seg > tb ? seg - tb : 0;
+                ovf = (int)(carry >> 16) - (int)(s_pre[sl] >> 16);
+            }
+            A.tile_ovf[b] = ovf;
+        }
+    } else {
+        block_reduce_partial<BLOCK>(acc, red);
+        if (threadIdx.x == 0) A.partials[b] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-cell scans. Each scan block covers <= SCAN_ITEMS*SCAN_BLOCK cells of one cloud.
+// count of cell c after the step: (old_start[c+1] - old_start[c]) - L[c] + I[c]
+// ---------------------------------------------------------------------------------------------
+constexpr int SCAN_BLOCK = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_CHUNK = SCAN_BLOCK * SCAN_ITEMS;
+
+template <class R>
+__device__ __forceinline__ int cloud_cell_end(const Args<R>& A, int cloud) {
+    return A.clouds[cloud].ovf_cell + 1;
+}
+
+template <class R>
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
+    __shared__ uint32_t wsum[32];
+    const int blk = blockIdx.x;
+    const int cloud = A.scan_blk_cloud[blk];
+    const int c0 = A.scan_blk_cell0[blk];
+    const int cend = cloud_cell_end(A, cloud);
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
+        if (c < cend) s += (uint32_t)((A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c]);
+    }
+    uint32_t tot;
+    block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
+    if (threadIdx.x == 0) A.block_sums[blk] = (int)tot;
+}
+
+// single block: block offsets, per-cloud totals and tilings for the next step, overflow carries
+template <class R>
+__global__ void __launch_bounds__(1024) scan_top(Args<R> A) {
+    __shared__ uint32_t wsum[32];
+    __shared__ int s_carry;
+    const int p = A.parity, q = 1 - p;
+    // 1. exclusive scan of block sums
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < A.nscan_blocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < A.nscan_blocks ? (uint32_t)A.block_sums[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan_u32<1024>(v, wsum, tot);
+        if (i < A.nscan_blocks) A.block_off[i] = (int)ex + s_carry;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += (int)tot;
+        __syncthreads();
+    }
+    const int total = s_carry;
+    // 2. per-cloud counts, starts, tile offsets (clouds in chunks of 1024)
+    __shared__ int s_tcarry;
+    if (threadIdx.x == 0) s_tcarry = 0;
+    __syncthreads();
+    for (int base = 0; base < A.nclouds; base += 1024) {
+        const int k = base + threadIdx.x;
+        int n = 0, st = 0, nt = 0;
+        if (k < A.nclouds) {
+            const int fb = A.cloud_first_blk[k], lb = A.cloud_first_blk[k + 1] - 1;
+            st = A.block_off[fb];
+            n = A.block_off[lb] + A.block_sums[lb] - st;
+            nt = (n + A.tile_nominal - 1) / A.tile_nominal;
+        }
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan_u32<1024>((uint32_t)nt, wsum, tot);
+        if (k < A.nclouds) {
+            CloudDyn& d = A.cdyn[k];
+            d.n[q] = n;
+            d.start[q] = st;
+            d.ntiles[q] = nt;
+            d.tile_off[q] = (int)ex + s_tcarry;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_tcarry += (int)tot;
+        __syncthreads();
+    }
+    const int ntiles_next = s_tcarry;
+    if (threadIdx.x == 0) {
+        A.ctl->n[q] = total;
+        A.ctl->ntiles[q] = ntiles_next > A.max_tiles ? A.max_tiles : ntiles_next;
+        if (ntiles_next > A.max_tiles) atomicOr(&A.ctl->err, EB_TILE_OVERFLOW);
+        A.new_start[A.total_cells] = total;
+        A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
+    }
+    // 3. cloud of every next tile: binary search of the per-cloud first tiles
+    for (int t = threadIdx.x; t < ntiles_next && t < A.max_tiles; t += 1024) {
+        int lo = 0, hi = A.nclouds;  // largest k with tile_off[k] <= t and ntiles[k] > 0
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (A.cdyn[mid].tile_off[q] <= t) lo = mid; else hi = mid;
+        }
+        while (lo + 1 < A.nclouds && A.cdyn[lo + 1].tile_off[q] <= t) ++lo;
+        A.tile_cloud_next[t] = lo;
+    }
+    // 4. overflow-stayer prefix over the current tiles: tile_ovf_carry[b] = sum of tile_ovf over
+    //    tiles before b; the carry of a tile is this prefix minus the prefix at its cloud's first tile.
+    if (!A.init_mode) {
+        constexpr int IT = 16;
+        const int nt = A.ctl->ntiles[p];
+        if (threadIdx.x == 0) s_carry = 0;
+        __syncthreads();
+        for (int base = 0; base < nt; base += 1024 * IT) {
+            const int i0 = base + threadIdx.x * IT;
+            int v[IT];
+            uint32_t s = 0;
+#pragma unroll
+            for (int k = 0; k < IT; ++k) {
+                v[k] = (i0 + k < nt) ? A.tile_ovf[i0 + k] : 0;
+                s += (uint32_t)v[k];
+            }
+            uint32_t tot;
+            uint32_t ex = block_excl_scan_u32<1024>(s, wsum, tot) + (uint32_t)s_carry;
+#pragma unroll
+            for (int k = 0; k < IT; ++k) {
+                if (i0 + k < nt) A.tile_ovf_carry[i0 + k] = (int)ex;
+                ex += (uint32_t)v[k];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry += (int)tot;
+            __syncthreads();
+        }
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
+    __shared__ uint32_t wsum[32];
+    const int q = 1 - A.parity;
+    const int blk = blockIdx.x;
+    const int cloud = A.scan_blk_cloud[blk];
+    const int c0 = A.scan_blk_cell0[blk];
+    const int cend = cloud_cell_end(A, cloud);
+    const int ovf = cend - 1;
+    int cnt[SCAN_ITEMS], oldc[SCAN_ITEMS], lv[SCAN_ITEMS], in[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
+        if (c < cend) {
+            oldc[k] = A.old_start[c + 1] - A.old_start[c];
+            lv[k] = A.Lc[c];
+            in[k] = A.Ic[c];
+            cnt[k] = oldc[k] - lv[k] + in[k];
+        } else {
+            oldc[k] = 0; lv[k] = 0; in[k] = 0; cnt[k] = 0;
+        }
+        s += (uint32_t)cnt[k];
+    }
+    uint32_t tot;
+    uint32_t ex = block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot) + (uint32_t)A.block_off[blk];
+    const CloudDyn& d = A.cdyn[cloud];
+    const int S = d.start[q];
+    const int toff = d.tile_off[q];
+    const int T = A.tile_nominal;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
+        if (c < cend) {
+            const int st = (int)ex;
+            A.new_start[c] = st;
+            if (in[k] > 0) A.mover_base[c] = st + oldc[k] - lv[k];
+            if (lv[k]) A.Lc[c] = 0;
+            if (in[k]) A.Ic[c] = 0;
+            if (cnt[k] > 0) {
+                const int e = st + cnt[k];
+                // nominal tile starts S + j*T falling in [st, e)
+                int j = (st - S + T - 1) / T;
+                for (; S + j * T < e; ++j) {
+                    const int pnom = S + j * T;
+                    int tbeg;
+                    if (pnom == st) tbeg = st;
+                    else tbeg = (c == ovf) ? pnom : e;
+                    const int ti = toff + j;
+                    if (ti < A.max_tiles) A.tile_begin_next[ti] = tbeg;
+                }
+            }
+            ex += (uint32_t)cnt[k];
+        }
+    }
+}
+
+// incoming movers: each writes its old index into its cell's incoming slots (ticket order)
+template <class R>
+__global__ void __launch_bounds__(256) mover_place(Args<R> A) {
+    const int b = blockIdx.x;
+    if (b >= A.ctl->ntiles[A.parity]) return;
+    const int tb = A.tile_begin[b];
+    const int m = A.tile_movers[b];
+    for (int i = threadIdx.x; i < m; i += 256) {
+        const int4 r = A.mrec[tb + i];
+        const int slot = A.mover_base[r.x] + r.z;
+        if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
+        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+    }
+}
+
+// rank = number of incoming movers of the same cell with a smaller old index
+template <class R>
+__global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
+    const int b = blockIdx.x;
+    if (b >= A.ctl->ntiles[A.parity]) return;
+    const int tb = A.tile_begin[b];
+    const int m = A.tile_movers[b];
+    for (int i = threadIdx.x; i < m; i += 256) {
+        int4 r = A.mrec[tb + i];
+        const int lo = A.mover_base[r.x];
+        const int hi = A.new_start[r.x + 1];
+        if (lo < 0 || hi > A.capacity || lo > hi) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            r.w = -1;
+            A.mrec[tb + i] = r;
+            continue;
+        }
+        int rank = 0;
+        for (int k = lo; k < hi; ++k) rank += (A.in_list[k] < r.y) ? 1 : 0;
+        r.w = lo + rank;
+        A.mrec[tb + i] = r;
+    }
+}
+
+// per-cloud diagnostics from the tile partials; block k handles cloud k
+template <class R, bool INIT>
+__global__ void __launch_bounds__(256) finalize(Args<R> A) {
+    __shared__ TilePartial red[8];
+    const int p = A.parity;
+    const int k = blockIdx.x;
+    CloudDyn& d = A.cdyn[k];
+    const int t0 = d.tile_off[p], nt = d.ntiles[p];
+    TilePartial acc;
+    zero_partial(acc);
+    for (int j = threadIdx.x; j < nt; j += 256) {
+        const TilePartial& t = A.partials[t0 + j];
+        acc.sum_v2 += t.sum_v2;
+        acc.sum_B += t.sum_B;
+        acc.evap_v2 += t.evap_v2;
+        acc.evap_B += t.evap_B;
+        acc.n_alive += t.n_alive;
+        acc.n_maj += t.n_maj;
+        acc.n_knife += t.n_knife;
+        acc.coll += t.coll;
+        acc.cand += t.cand;
+    }
+    block_reduce_partial<256>(acc, red);
+    if (threadIdx.x == 0) {
+        const CloudPhys<R>& P = A.clouds[k];
+        CloudDiagDev& g = A.cdiag[k];
+        const int step_now = A.ctl->step[p];
+        if (INIT) {
+            g.step = step_now;
+            g.cum_evap = 0; g.cum_maj = 0; g.cum_knife = 0; g.cum_coll = 0; g.cum_cand = 0;
+            g.cum_evap_v2 = 0; g.cum_evap_B = 0; g.cum_atom_steps = 0;
+        } else {
+            g.step = step_now + 1;
+            g.cum_evap += acc.n_maj + acc.n_knife;
+            g.cum_maj += acc.n_maj;
+            g.cum_knife += acc.n_knife;
+            g.cum_coll += acc.coll;
+            g.cum_cand += acc.cand;
+            g.cum_evap_v2 += acc.evap_v2;
+            g.cum_evap_B += acc.evap_B;
+            g.cum_atom_steps += acc.n_alive + acc.n_maj + acc.n_knife;
+        }
+        g.n_alive = acc.n_alive;
+        g.sum_v2 = acc.sum_v2;
+        g.sum_B = acc.sum_B;
+        g.err = A.ctl->err;
+        d.T_knife = knife_temperature(P.mass, P.kB, P.T0, (P.flags & F_KNIFE_FIXED_T) != 0, acc.sum_v2,
+                                      acc.n_alive);
+        if (k == 0 && !INIT) A.ctl->step[1 - p] = step_now + 1;
+    }
+}
+
+// diagnostics of the current (sorted) state without moving it: tile partials for finalize<INIT>
+template <class R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
+    typedef typename V4T<R>::type R4;
+    __shared__ TilePartial red[BLOCK / 32];
+    __shared__ CloudPhys<R> P;
+    const int p = A.parity;
+    const int b = blockIdx.x;
+    if (b >= A.ctl->ntiles[p]) return;
+    const int tb = A.tile_begin[b], te = A.tile_begin[b + 1];
+    load_cloud(P, A.clouds + A.tile_cloud[b]);
+    __syncthreads();
+    TilePartial acc;
+    zero_partial(acc);
+    for (int i = tb + threadIdx.x; i < te; i += BLOCK) {
+        const R4 q = A.pos_in[i];
+        const R4 v = A.vel_in[i];
+        Field<R> f;
+        trap_field(P, q.x, q.y, q.z, f);
+        const R v2 = v.x * v.x + v.y * v.y + v.z * v.z;
+        acc.n_alive += 1;
+        acc.sum_v2 += fx_from((double)v2);
+        acc.sum_B += fx_from((double)f.absB);
+    }
+    block_reduce_partial<BLOCK>(acc, red);
+    if (threadIdx.x == 0) A.partials[b] = acc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// full sort (initialisation and set_state): arbitrary order -> stable by (cell, index)
+// ---------------------------------------------------------------------------------------------
+template <class R> struct SortArgs {
+    typedef typename V4T<R>::type R4;
+    const R4* pos_src;
+    const R4* vel_src;
+    const R4* psi_src;
+    R4* pos_dst;
+    R4* vel_dst;
+    R4* psi_dst;
+    const int* cloud_atom_off;  // nclouds + 1, atoms of the source grouped by cloud
+    int* cell;
+    int* ticket;
+    int* ovf_flag;
+    int* ovf_rank;
+    int n, nclouds;
+};
+
+template <class R>
+__device__ __forceinline__ int find_cloud(const int* off, int nclouds, int i) {
+    int lo = 0, hi = nclouds;  // off[lo] <= i < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) fs_cells(SortArgs<R> S, Args<R> A) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= S.n) return;
+    const int k = find_cloud<R>(S.cloud_atom_off, S.nclouds, i);
+    const CloudPhys<R>& P = A.clouds[k];
+    const auto q = S.pos_src[i];
+    const int c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);
+    S.cell[i] = c;
+    S.ovf_flag[i] = (c == P.ovf_cell) ? 1 : 0;
+    S.ticket[i] = atomicAdd(&A.Ic[c], 1);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) fs_place(SortArgs<R> S, Args<R> A) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= S.n) return;
+    if (S.ovf_flag[i]) return;
+    const int c = S.cell[i];
+    A.in_list[A.mover_base[c] + S.ticket[i]] = i;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) fs_scatter(SortArgs<R> S, Args<R> A) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= S.n) return;
+    const int c = S.cell[i];
+    int dest;
+    if (S.ovf_flag[i]) {
+        const int k = find_cloud<R>(S.cloud_atom_off, S.nclouds, i);
+        dest = A.new_start[c] + (S.ovf_rank[i] - S.ovf_rank[S.cloud_atom_off[k]]);
+    } else {
+        const int lo = A.new_start[c], hi = A.new_start[c + 1];
+        int rank = 0;
+        for (int j = lo; j < hi; ++j) rank += (A.in_list[j] < i) ? 1 : 0;
+        dest = lo + rank;
+    }
+    S.pos_dst[dest] = S.pos_src[i];
+    S.vel_dst[dest] = S.vel_src[i];
+    S.psi_dst[dest] = S.psi_src[i];
+}
+
+// generic exclusive scan of n ints (3 kernels, no inter-block waiting)
+__global__ void __launch_bounds__(SCAN_BLOCK) gscan_reduce(const int* in, int n, int* bsum) {
+    __shared__ uint32_t wsum[32];
+    const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k)
+        if (base + k < n) s += (uint32_t)in[base + k];
+    uint32_t tot;
+    block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = (int)tot;
+}
+__global__ void __launch_bounds__(1024) gscan_top(int* bsum, int nb, int* total) {
+    __shared__ uint32_t wsum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += 1024) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < nb ? (uint32_t)bsum[i] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan_u32<1024>(v, wsum, tot);
+        if (i < nb) bsum[i] = (int)ex + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += (int)tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+__global__ void __launch_bounds__(SCAN_BLOCK) gscan_down(const int* in, int n, const int* boff, int* out) {
+    __shared__ uint32_t wsum[32];
+    const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += (uint32_t)v[k];
+    }
+    uint32_t tot;
+    uint32_t ex = block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot) + (uint32_t)boff[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) out[base + k] = (int)ex;
+        ex += (uint32_t)v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// initial cloud and small fills
+// ---------------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(256) init_atoms(Args<R> A, const int* cloud_atom_off, int n,
+                                                  const int* init_mode, typename V4T<R>::type* pos,
+                                                  typename V4T<R>::type* vel, typename V4T<R>::type* psi,
+                                                  unsigned long long seed) {
+    typedef typename V4T<R>::type R4;
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const int k = find_cloud<R>(cloud_atom_off, A.nclouds, i);
+    const CloudPhys<R>& P = A.clouds[k];
+    const uint32_t local = (uint32_t)(i - cloud_atom_off[k]);
+    Atom<R> a;
+    const bool ok = init_atom(P, init_mode[k], local, (uint64_t)seed, a);
+    if (!ok) atomicOr(&A.ctl->err, EB_INIT_REJECT);
+    R4 q, v, s;
+    q.x = a.x; q.y = a.y; q.z = a.z; q.w = lane_from_u32(local, R(0));
+    v.x = a.vx; v.y = a.vy; v.z = a.vz; v.w = lane_from_u32(a.flags, R(0));
+    s.x = a.ur; s.y = a.ui; s.z = a.dr; s.w = a.di;
+    pos[i] = q;
+    vel[i] = v;
+    psi[i] = s;
+}
+
+template <class R>
+__global__ void fill_sigvrmax(R* sv, const int* cell_cloud_base, const R* init_val, int nclouds, int total) {
+    const int c = blockIdx.x * 256 + threadIdx.x;
+    if (c >= total) return;
+    int k = 0;
+    while (k + 1 < nclouds && cell_cloud_base[k + 1] <= c) ++k;
+    sv[c] = init_val[k];
+}
+
+}  // namespace dsmc
+
+#endif  // DSMC_KERNELS_CUH

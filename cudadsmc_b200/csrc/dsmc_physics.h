@@ -1,0 +1,696 @@
+// dsmc_physics.h -- per-atom and per-cell arithmetic of the DSMC timestep.
+//
+// Included by the sm_100a kernels (nvcc, compiled with --fmad=false) and by the CPU
+// oracle (g++, -ffp-contract=off).  Every value is produced by IEEE-754 operations that
+// are correctly rounded on both sides (+ - * /, sqrt, fma, floor/rint, integer ops), so the
+// GPU and the CPU restatement give bit-identical results for the same inputs in float and
+// in double.  Elementary functions (sin/cos/log/exp) are written here from their series
+// (Cody-Waite argument reduction, Taylor / atanh series) instead of calling libm or the
+// CUDA math library, whose implementations differ between host and device.
+//
+// Physics follows CUDADSMC (paths inside that project):
+//   trap field and Jacobian           src/moveAtoms.cu:135-157 (Ioffe-Pritchard),
+//                                     energyComparison.py:53 (quadrupole |B| = B' sqrt(x^2/4+y^2/4+z^2))
+//   acceleration a = -(mu/m) grad|B|  src/moveAtoms.cu:93-116
+//   velocity Verlet                   src/moveAtoms.cu:51-65
+//   Larmor rotation exp(-i theta s.B^) src/wavefunction.cu:39-73
+//   normalisation                     src/wavefunction.cu:279-299
+//   Majorana test <s.B^> < 0          src/evaporation.cu:86-95
+//   cell index                        src/collisions.cu:187-219
+//   NTC collisions                    src/collisions.cu:291-437, 529-546
+//   random numbers: Philox4x32-10, Salmon, Moraes, Dror, Shaw, "Parallel random numbers:
+//   as easy as 1, 2, 3", SC'11 (replaces the cuRAND XORWOW states of src/setUp.cu:63-75).
+#ifndef DSMC_PHYSICS_H
+#define DSMC_PHYSICS_H
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define DSMC_HD __host__ __device__ __forceinline__
+#else
+#include <math.h>
+#include <string.h>
+#define DSMC_HD inline
+#endif
+
+namespace dsmc {
+
+typedef __int128 i128;
+
+// ---------------------------------------------------------------------------------------
+// Correctly rounded primitives (identical on host and device)
+// ---------------------------------------------------------------------------------------
+DSMC_HD float xfma(float a, float b, float c) { return fmaf(a, b, c); }
+DSMC_HD double xfma(double a, double b, double c) { return fma(a, b, c); }
+DSMC_HD float xsqrt(float x) { return sqrtf(x); }
+DSMC_HD double xsqrt(double x) { return sqrt(x); }
+DSMC_HD float xfloor(float x) { return floorf(x); }
+DSMC_HD double xfloor(double x) { return floor(x); }
+DSMC_HD float xceil(float x) { return ceilf(x); }
+DSMC_HD double xceil(double x) { return ceil(x); }
+DSMC_HD float xrint(float x) { return rintf(x); }
+DSMC_HD double xrint(double x) { return rint(x); }
+
+DSMC_HD uint32_t f2u(float f) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(f);
+#else
+    uint32_t u; memcpy(&u, &f, 4); return u;
+#endif
+}
+DSMC_HD float u2f(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(u);
+#else
+    float f; memcpy(&f, &u, 4); return f;
+#endif
+}
+DSMC_HD uint64_t d2u(double f) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(f);
+#else
+    uint64_t u; memcpy(&u, &f, 8); return u;
+#endif
+}
+DSMC_HD double u2d(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)u);
+#else
+    double f; memcpy(&f, &u, 8); return f;
+#endif
+}
+
+// 4th-lane integer payloads (atom id in pos.w, flag bits in vel.w)
+DSMC_HD float lane_from_u32(uint32_t u, float) { return u2f(u); }
+DSMC_HD double lane_from_u32(uint32_t u, double) { return u2d((uint64_t)u); }
+DSMC_HD uint32_t lane_to_u32(float f) { return f2u(f); }
+DSMC_HD uint32_t lane_to_u32(double f) { return (uint32_t)d2u(f); }
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11): 10 rounds of the 4x32 S-P network with the
+// multipliers M0 = 0xD2511F53, M1 = 0xCD9E8D57 and key schedule constants (Weyl
+// sequence) W0 = 0x9E3779B9, W1 = 0xBB67AE85 given in the paper.
+// ---------------------------------------------------------------------------------------
+struct u32x4 { uint32_t x, y, z, w; };
+
+DSMC_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        u32x4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Stream purposes (third counter word, high byte); the low 24 bits carry the cloud id.
+enum : uint32_t {
+    PURPOSE_INIT_POS = 1u,
+    PURPOSE_INIT_VEL = 2u,
+    PURPOSE_COLLIDE = 3u,
+    PURPOSE_FLIP = 4u
+};
+
+DSMC_HD u32x4 draw(uint32_t id, uint32_t step, uint32_t purpose, uint32_t cloud, uint32_t sub,
+                   uint64_t seed) {
+    u32x4 c;
+    c.x = id;
+    c.y = step;
+    c.z = (purpose << 24) | (cloud & 0xFFFFFFu);
+    c.w = sub;
+    return philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// uniform in the open interval (0,1): float from 24 bits, double from 53 bits (two words)
+DSMC_HD float u01f(uint32_t a) { return ((float)(a >> 8) + 0.5f) * 0x1p-24f; }
+DSMC_HD double u01d(uint32_t a, uint32_t b) {
+    uint64_t m = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);
+    return ((double)m + 0.5) * 0x1p-53;
+}
+template <class R> DSMC_HD R u01(uint32_t a, uint32_t b);
+template <> DSMC_HD float u01<float>(uint32_t a, uint32_t) { return u01f(a); }
+template <> DSMC_HD double u01<double>(uint32_t a, uint32_t b) { return u01d(a, b); }
+
+// unbiased-enough index in [0, n): high word of a 32x32 product (bias < n / 2^32)
+DSMC_HD uint32_t index_below(uint32_t r, uint32_t n) {
+    return (uint32_t)(((uint64_t)r * (uint64_t)n) >> 32);
+}
+
+// ---------------------------------------------------------------------------------------
+// Elementary functions from their series.
+// sin/cos: x = k pi/2 + r with pi/2 split in three parts (the leading parts have trailing
+// zero bits, so k*part is exact), |r| <= pi/4, Taylor series evaluated with fma (Horner).
+// log: x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh((m-1)/(m+1)) series.
+// exp: x = k ln2 + r, |r| <= ln2/2, Taylor series, scaled by 2^k.
+// The split constants were derived from Machin's formula for pi and the atanh(1/3)
+// series for ln 2 in exact rational arithmetic.
+// ---------------------------------------------------------------------------------------
+DSMC_HD void xsincos(float x, float* s, float* c) {
+    const float two_over_pi = 0x1.45f306p-1f;
+    const float p1 = 0x1.922p+0f, p2 = -0x1.2aep-18f, p3 = -0x1.de973ep-31f;
+    float k = xrint(x * two_over_pi);
+    float r = xfma(-k, p1, x);
+    r = xfma(-k, p2, r);
+    r = xfma(-k, p3, r);
+    float r2 = r * r;
+    // sin r = r + r^3 (-1/3! + r^2 (1/5! + r^2 (-1/7! + r^2/9!)))
+    float ps = xfma(r2, 2.75573192e-6f, -1.98412698e-4f);
+    ps = xfma(r2, ps, 8.33333333e-3f);
+    ps = xfma(r2, ps, -1.66666667e-1f);
+    float sr = xfma(r * r2, ps, r);
+    // cos r = 1 + r^2 (-1/2 + r^2 (1/4! + r^2 (-1/6! + r^2 (1/8! - r^2/10!))))
+    float pc = xfma(r2, -2.75573192e-7f, 2.48015873e-5f);
+    pc = xfma(r2, pc, -1.38888889e-3f);
+    pc = xfma(r2, pc, 4.16666667e-2f);
+    pc = xfma(r2, pc, -0.5f);
+    float cr = xfma(r2, pc, 1.0f);
+    int q = ((int)k) & 3;
+    float ss = (q & 1) ? cr : sr;
+    float cc = (q & 1) ? sr : cr;
+    if (q == 1 || q == 2) cc = -cc;
+    if (q >= 2) ss = -ss;
+    *s = ss;
+    *c = cc;
+}
+
+DSMC_HD void xsincos(double x, double* s, double* c) {
+    const double two_over_pi = 0x1.45f306dc9c883p-1;
+    const double p1 = 0x1.921fb58p+0, p2 = -0x1.dde974p-27, p3 = 0x1.1a62633145c07p-54;
+    double k = xrint(x * two_over_pi);
+    double r = xfma(-k, p1, x);
+    r = xfma(-k, p2, r);
+    r = xfma(-k, p3, r);
+    double r2 = r * r;
+    // Taylor coefficients 1/n!, alternating signs
+    double ps = xfma(r2, 2.8114572543455206e-15, -7.6471637318198164e-13);   // 1/17!, -1/15!
+    ps = xfma(r2, ps, 1.6059043836821613e-10);                                // 1/13!
+    ps = xfma(r2, ps, -2.5052108385441720e-8);                                // -1/11!
+    ps = xfma(r2, ps, 2.7557319223985893e-6);                                 // 1/9!
+    ps = xfma(r2, ps, -1.9841269841269841e-4);                                // -1/7!
+    ps = xfma(r2, ps, 8.3333333333333333e-3);                                 // 1/5!
+    ps = xfma(r2, ps, -1.6666666666666667e-1);                                // -1/3!
+    double sr = xfma(r * r2, ps, r);
+    double pc = xfma(r2, 1.5619206968586225e-16, -4.7794773323873853e-14);   // 1/18!, -1/16!
+    pc = xfma(r2, pc, 1.1470745597729725e-11);                                // 1/14!
+    pc = xfma(r2, pc, -2.0876756987868099e-9);                                // -1/12!
+    pc = xfma(r2, pc, 2.7557319223985891e-7);                                 // 1/10!
+    pc = xfma(r2, pc, -2.4801587301587302e-5);                                // -1/8!
+    pc = xfma(r2, pc, 1.3888888888888889e-3);                                 // 1/6!
+    pc = xfma(r2, pc, -4.1666666666666667e-2);                                // -1/4!
+    pc = xfma(r2, pc, 0.5);                                                   // 1/2!
+    double cr = xfma(-r2, pc, 1.0);
+    int q = ((int)(long long)k) & 3;
+    double ss = (q & 1) ? cr : sr;
+    double cc = (q & 1) ? sr : cr;
+    if (q == 1 || q == 2) cc = -cc;
+    if (q >= 2) ss = -ss;
+    *s = ss;
+    *c = cc;
+}
+
+// natural log for normal positive x
+DSMC_HD float xlog(float x) {
+    uint32_t u = f2u(x);
+    int e = (int)(u >> 23) - 127;
+    float m = u2f((u & 0x7FFFFFu) | 0x3F800000u);
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    // atanh series: 2 s (1 + s^2/3 + s^4/5 + s^6/7 + s^8/9)
+    float p = xfma(s2, 0.111111111f, 0.142857143f);
+    p = xfma(s2, p, 0.2f);
+    p = xfma(s2, p, 0.333333333f);
+    float lm = xfma(2.0f * s * s2, p, 2.0f * s);
+    const float ln2_hi = 0x1.62ep-1f, ln2_lo = 0x1.0bfbe8p-15f;
+    float fe = (float)e;
+    return xfma(fe, ln2_hi, xfma(fe, ln2_lo, lm));
+}
+
+DSMC_HD double xlog(double x) {
+    uint64_t u = d2u(x);
+    int e = (int)(u >> 52) - 1023;
+    double m = u2d((u & 0xFFFFFFFFFFFFFull) | 0x3FF0000000000000ull);
+    if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    double p = xfma(s2, 1.0 / 21.0, 1.0 / 19.0);
+    p = xfma(s2, p, 1.0 / 17.0);
+    p = xfma(s2, p, 1.0 / 15.0);
+    p = xfma(s2, p, 1.0 / 13.0);
+    p = xfma(s2, p, 1.0 / 11.0);
+    p = xfma(s2, p, 1.0 / 9.0);
+    p = xfma(s2, p, 1.0 / 7.0);
+    p = xfma(s2, p, 1.0 / 5.0);
+    p = xfma(s2, p, 1.0 / 3.0);
+    double lm = xfma(2.0 * s * s2, p, 2.0 * s);
+    const double ln2_hi = 0x1.62e42ffp-1, ln2_lo = -0x1.718432a1b0e26p-35;
+    double fe = (double)e;
+    return xfma(fe, ln2_hi, xfma(fe, ln2_lo, lm));
+}
+
+DSMC_HD float xexp(float x) {
+    if (x < -87.0f) return 0.0f;
+    if (x > 88.0f) x = 88.0f;
+    float k = xrint(x * 0x1.715476p+0f);
+    float r = xfma(-k, 0x1.62ep-1f, x);
+    r = xfma(-k, 0x1.0bfbe8p-15f, r);
+    float p = xfma(r, 1.98412698e-4f, 1.38888889e-3f);  // 1/7!, 1/6!
+    p = xfma(r, p, 8.33333333e-3f);
+    p = xfma(r, p, 4.16666667e-2f);
+    p = xfma(r, p, 1.66666667e-1f);
+    p = xfma(r, p, 0.5f);
+    p = xfma(r, p, 1.0f);
+    p = xfma(r, p, 1.0f);
+    return p * u2f((uint32_t)((int)k + 127) << 23);
+}
+
+DSMC_HD double xexp(double x) {
+    if (x < -708.0) return 0.0;
+    if (x > 709.0) x = 709.0;
+    double k = xrint(x * 0x1.71547652b82fep+0);
+    double r = xfma(-k, 0x1.62e42ffp-1, x);
+    r = xfma(-k, -0x1.718432a1b0e26p-35, r);
+    double p = xfma(r, 1.6059043836821613e-10, 2.0876756987868099e-9);  // 1/13!, 1/12!
+    p = xfma(r, p, 2.5052108385441720e-8);
+    p = xfma(r, p, 2.7557319223985891e-7);
+    p = xfma(r, p, 2.7557319223985893e-6);
+    p = xfma(r, p, 2.4801587301587302e-5);
+    p = xfma(r, p, 1.9841269841269841e-4);
+    p = xfma(r, p, 1.3888888888888889e-3);
+    p = xfma(r, p, 8.3333333333333333e-3);
+    p = xfma(r, p, 4.1666666666666667e-2);
+    p = xfma(r, p, 1.6666666666666667e-1);
+    p = xfma(r, p, 0.5);
+    p = xfma(r, p, 1.0);
+    p = xfma(r, p, 1.0);
+    return p * u2d((uint64_t)((long long)k + 1023) << 52);
+}
+
+// ---------------------------------------------------------------------------------------
+// Exact fixed-point accumulation for diagnostics: a non-negative double d (< 2^62) maps to
+// round-toward-zero(d * 2^64) as a 128-bit integer.  Sums of these are exact and therefore
+// independent of summation order (GPU tiles, CPU loop, batched or single clouds).
+// ---------------------------------------------------------------------------------------
+DSMC_HD i128 fx_from(double d) {
+    double h = xfloor(d);
+    int64_t hi = (int64_t)h;
+    double fr = (d - h) * 0x1p64;
+    uint64_t lo = (uint64_t)fr;
+    return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
+}
+DSMC_HD double fx_to_double(i128 q) {
+    int64_t hi = (int64_t)(q >> 64);
+    uint64_t lo = (uint64_t)q;
+    return (double)hi + (double)lo * 0x1p-64;
+}
+
+// knife temperature after a step: T = m sum(v^2) / (3 kB n) from the exact fixed-point sum
+DSMC_HD double knife_temperature(double mass, double kB, double T0, bool fixed_T, i128 sum_v2, long long n) {
+    if (fixed_T || n <= 0) return T0;
+    return mass * fx_to_double(sum_v2) / (3.0 * kB * (double)n);
+}
+
+// ---------------------------------------------------------------------------------------
+// Parameters of one cloud as the kernels see them (derived on the host from
+// dsmc_cloud_params + dsmc_params, identically for the GPU engine and the oracle).
+// ---------------------------------------------------------------------------------------
+enum { TRAP_QUADRUPOLE = 0, TRAP_IOFFE_PRITCHARD = 1, TRAP_BOX = 2 };
+enum {
+    F_COLLIDE = 1, F_LARMOR = 2, F_MAJORANA = 4, F_KNIFE = 8, F_NORMALISE = 16, F_KNIFE_FIXED_T = 32
+};
+
+template <class R> struct CloudPhys {
+    int32_t trap, flags;
+    int32_t nx, ny, nz;
+    int32_t cell_base;   // global id of grid cell (0,0,0)
+    int32_t ovf_cell;    // global id of the overflow cell = cell_base + nx*ny*nz
+    int32_t cloud_id;
+    R gmin_x, gmin_y, gmin_z;
+    R inv_dx, inv_dy, inv_dz;
+    R box_x, box_y, box_z;       // grid box edge lengths (periodic wrap)
+    R inv_box_x, inv_box_y, inv_box_z;
+    R Bp, Bpp, B0, B_floor;       // gradient, curvature, bias, trap-bottom |B|
+    R dt, half_dt;
+    R accel_scale;                // mu / m
+    R theta_per_B;                // mu dt / hbar
+    R kappa;                      // 2 mu / m: energy per (m/2) in units of v^2 per tesla
+    R sigma;                      // cross-section
+    R cand_pref;                  // alpha * dt_collide / V_cell
+    R v_init;                     // sqrt(kB T0 / m)
+    R r0_init;                    // kB T0 / mu  (quadrupole thermal length)
+    R inv_kT_over_mu;             // mu / (kB T0) for rejection sampling
+    int32_t knife_nknots;
+    int32_t pad0;
+    double knife_step[9];
+    double knife_eta[9];
+    double mass, moment, kB, T0;  // for diagnostics and the knife cut
+};
+
+// piecewise-linear knife eta(step), constant outside the knots
+DSMC_HD double knife_eta(const int32_t nk, const double* ks, const double* ke, double step) {
+    if (nk <= 0) return 1e300;
+    if (step <= ks[0]) return ke[0];
+    for (int i = 1; i < nk; ++i) {
+        if (step <= ks[i]) {
+            double f = (step - ks[i - 1]) / (ks[i] - ks[i - 1]);
+            return ke[i - 1] + f * (ke[i] - ke[i - 1]);
+        }
+    }
+    return ke[nk - 1];
+}
+
+// knife cut in units of v^2 (E / (m/2)): 2 eta kB T / m
+DSMC_HD double knife_cut_v2(double eta, double kB, double T, double mass) {
+    return 2.0 * eta * kB * T / mass;
+}
+
+// ---------------------------------------------------------------------------------------
+// Trap field: B, |B|, B^ and grad|B| at a point.
+// ---------------------------------------------------------------------------------------
+template <class R> struct Field {
+    R bx, by, bz;     // unit vector B^
+    R absB;           // |B|
+    R gx, gy, gz;     // grad |B|
+};
+
+template <class R>
+DSMC_HD void trap_field(const CloudPhys<R>& P, R x, R y, R z, Field<R>& f) {
+    R Bx, By, Bz;
+    R jxx, jxy, jxz, jyx, jyy, jyz, jzx, jzy, jzz;  // dB_i / dx_j stored as j{i}{j}
+    if (P.trap == TRAP_QUADRUPOLE) {
+        const R h = R(0.5) * P.Bp;
+        Bx = h * x;
+        By = h * y;
+        Bz = P.B0 - P.Bp * z;
+        jxx = h; jxy = R(0); jxz = R(0);
+        jyx = R(0); jyy = h; jyz = R(0);
+        jzx = R(0); jzy = R(0); jzz = -P.Bp;
+    } else if (P.trap == TRAP_IOFFE_PRITCHARD) {
+        // CUDADSMC/src/moveAtoms.cu:135-157
+        const R hc = R(0.5) * P.Bpp;
+        Bx = P.Bp * x - hc * (x * z);
+        By = -(P.Bp * y) - hc * (y * z);
+        Bz = P.B0 + hc * (z * z - R(0.5) * (x * x + y * y));
+        jxx = P.Bp - hc * z; jxy = R(0); jxz = -(hc * x);
+        jyx = R(0); jyy = -P.Bp - hc * z; jyz = -(hc * y);
+        jzx = -(hc * x); jzy = -(hc * y); jzz = P.Bpp * z;
+    } else {
+        f.bx = R(0); f.by = R(0); f.bz = R(1);
+        f.absB = R(0);
+        f.gx = R(0); f.gy = R(0); f.gz = R(0);
+        return;
+    }
+    R b2 = Bx * Bx + By * By + Bz * Bz;
+    R ab = xsqrt(b2);
+    if (ab > R(0)) {
+        R inv = R(1) / ab;
+        f.bx = Bx * inv; f.by = By * inv; f.bz = Bz * inv;
+    } else {
+        f.bx = R(0); f.by = R(0); f.bz = R(1);
+    }
+    f.absB = ab;
+    // d|B|/dx_j = B^ . dB/dx_j  (columns of the Jacobian, moveAtoms.cu:97-107)
+    f.gx = f.bx * jxx + f.by * jyx + f.bz * jzx;
+    f.gy = f.bx * jxy + f.by * jyy + f.bz * jzy;
+    f.gz = f.bx * jxz + f.by * jyz + f.bz * jzz;
+}
+
+// ---------------------------------------------------------------------------------------
+// Cell index (collisions.cu:194-219): floor((x - xmin) / dx) per axis, linear id
+// z*nx*ny + y*nx + x, atoms outside the grid go to the cloud's overflow cell.
+// Evaluated as (x - xmin) * (1/dx) without contraction, identically on host and device.
+// ---------------------------------------------------------------------------------------
+template <class R>
+DSMC_HD int32_t cell_of(const CloudPhys<R>& P, R x, R y, R z, bool periodic) {
+    R fx = (x - P.gmin_x) * P.inv_dx;
+    R fy = (y - P.gmin_y) * P.inv_dy;
+    R fz = (z - P.gmin_z) * P.inv_dz;
+    if (periodic) {
+        int ix = (fx >= R(0)) ? (int)fx : 0;
+        int iy = (fy >= R(0)) ? (int)fy : 0;
+        int iz = (fz >= R(0)) ? (int)fz : 0;
+        if (!(fx == fx) || !(fy == fy) || !(fz == fz)) return P.ovf_cell;
+        ix = ix < P.nx ? ix : P.nx - 1;
+        iy = iy < P.ny ? iy : P.ny - 1;
+        iz = iz < P.nz ? iz : P.nz - 1;
+        return P.cell_base + (iz * P.ny + iy) * P.nx + ix;
+    }
+    if (!(fx >= R(0) && fx < (R)P.nx && fy >= R(0) && fy < (R)P.ny && fz >= R(0) &&
+          fz < (R)P.nz))
+        return P.ovf_cell;
+    int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    return P.cell_base + (iz * P.ny + iy) * P.nx + ix;
+}
+
+// ---------------------------------------------------------------------------------------
+// One timestep of one atom: Larmor rotation about B^(x) (evolveWavefunction runs before
+// moveAtoms, main.cu:465-476), renormalisation, velocity Verlet kick-drift-kick with the
+// acceleration recomputed from the position (no stored a), periodic wrap for the box,
+// then the evaporation tests at the new position (evaporationTag, evaporation.cu:68-106)
+// and the new cell.
+// ---------------------------------------------------------------------------------------
+template <class R> struct Atom {
+    R x, y, z, vx, vy, vz;
+    R ur, ui, dr, di;  // psi_up, psi_dn
+    uint32_t flags;    // bit 0: anti-trapped
+};
+
+enum { FATE_ALIVE = 0, FATE_MAJORANA = 1, FATE_KNIFE = 2 };
+
+template <class R> struct AtomOut {
+    int32_t cell;
+    int32_t fate;
+    R v2;     // |v|^2 after the step
+    R absB;   // |B| after the step
+};
+
+template <class R>
+DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R>& o) {
+    const bool box = (P.trap == TRAP_BOX);
+    Field<R> f0;
+    trap_field(P, a.x, a.y, a.z, f0);
+
+    if ((P.flags & F_LARMOR) && !box) {
+        // psi <- [cos t - i sin t (s.B^)] psi, t = mu |B| dt / hbar   (wavefunction.cu:39-73)
+        R th = P.theta_per_B * f0.absB;
+        R s, c;
+        xsincos(th, &s, &c);
+        R nur = a.ur * c + (f0.bx * a.di - f0.by * a.dr + f0.bz * a.ui) * s;
+        R nui = a.ui * c + (-(f0.bx * a.dr) - f0.by * a.di - f0.bz * a.ur) * s;
+        R ndr = a.dr * c + (f0.bx * a.ui + f0.by * a.ur - f0.bz * a.di) * s;
+        R ndi = a.di * c + (-(f0.bx * a.ur) + f0.by * a.ui + f0.bz * a.dr) * s;
+        a.ur = nur; a.ui = nui; a.dr = ndr; a.di = ndi;
+        if (P.flags & F_NORMALISE) {
+            R n2 = a.ur * a.ur + a.ui * a.ui + a.dr * a.dr + a.di * a.di;
+            R inv = R(1) / xsqrt(n2);
+            a.ur = a.ur * inv; a.ui = a.ui * inv; a.dr = a.dr * inv; a.di = a.di * inv;
+        }
+    }
+
+    // velocity Verlet (moveAtoms.cu:51-65); anti-trapped atoms feel +grad|B|
+    const R sgn = (a.flags & 1u) ? R(1) : R(-1);
+    const R as = sgn * P.accel_scale;
+    const R hdt = P.half_dt;
+    a.vx = a.vx + hdt * (as * f0.gx);
+    a.vy = a.vy + hdt * (as * f0.gy);
+    a.vz = a.vz + hdt * (as * f0.gz);
+    a.x = a.x + P.dt * a.vx;
+    a.y = a.y + P.dt * a.vy;
+    a.z = a.z + P.dt * a.vz;
+    if (box) {
+        a.x = a.x - P.box_x * xfloor((a.x - P.gmin_x) * P.inv_box_x);
+        a.y = a.y - P.box_y * xfloor((a.y - P.gmin_y) * P.inv_box_y);
+        a.z = a.z - P.box_z * xfloor((a.z - P.gmin_z) * P.inv_box_z);
+    }
+    Field<R> f1;
+    trap_field(P, a.x, a.y, a.z, f1);
+    a.vx = a.vx + hdt * (as * f1.gx);
+    a.vy = a.vy + hdt * (as * f1.gy);
+    a.vz = a.vz + hdt * (as * f1.gz);
+
+    o.v2 = a.vx * a.vx + a.vy * a.vy + a.vz * a.vz;
+    o.absB = f1.absB;
+    o.fate = FATE_ALIVE;
+    if ((P.flags & F_MAJORANA) && !box) {
+        // <s.B^> = 2 Bx Re(u* d) + 2 By Im(u* d) + Bz (|u|^2 - |d|^2)   (evaporation.cu:88-90)
+        R re = a.ur * a.dr + a.ui * a.di;
+        R im = a.ur * a.di - a.ui * a.dr;
+        R sz = (a.ur * a.ur + a.ui * a.ui) - (a.dr * a.dr + a.di * a.di);
+        R proj = R(2) * (f1.bx * re) + R(2) * (f1.by * im) + f1.bz * sz;
+        if (proj < R(0)) o.fate = FATE_MAJORANA;
+    }
+    if ((P.flags & F_KNIFE) && o.fate == FATE_ALIVE) {
+        R e = o.v2 + P.kappa * (f1.absB - P.B_floor);
+        if (e > cut_v2) o.fate = FATE_KNIFE;
+    }
+    o.cell = cell_of(P, a.x, a.y, a.z, box);
+}
+
+// ---------------------------------------------------------------------------------------
+// No-time-counter collisions in one cell (collisions.cu:306-437 with the intended
+// semantics): Mc = n(n-1)/2 candidate pairs, Ncand = ceil(Mc alpha dt_c (sigma v_r)max / V),
+// each candidate is a uniformly chosen distinct pair (i, j) accepted with probability
+// sigma v_r alpha dt_c Mc / (V Ncand); accepted pairs scatter isotropically about their
+// centre of mass (collisions.cu:425-437, 537-546).  vel points at n consecutive atoms
+// (4 reals each).  Random numbers: two Philox blocks per candidate keyed by
+// (cell, step, cloud, candidate).
+// ---------------------------------------------------------------------------------------
+template <class R> struct CollideResult {
+    int32_t accepted;
+    int32_t candidates;
+};
+
+template <class R, class V4>
+DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPhys<R>& P,
+                                      uint32_t local_cell, uint32_t step, uint64_t seed) {
+    CollideResult<R> res;
+    res.accepted = 0;
+    res.candidates = 0;
+    if (n < 2) return res;
+    const R Mc = R(0.5) * ((R)n * (R)(n - 1));
+    const R x = Mc * P.cand_pref * sigvrmax;
+    const R ncf = xceil(x);
+    if (!(ncf >= R(1))) return res;
+    const int ncand = ncf < R(1 << 24) ? (int)ncf : (1 << 24);
+    const R pacc = (P.cand_pref * Mc) / ncf;
+    const R two_pi = R(6.283185307179586476925286766559);
+    for (int k = 0; k < ncand; ++k) {
+        u32x4 w = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k, seed);
+        u32x4 w2 = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k + 1u, seed);
+        uint32_t i = index_below(w.x, (uint32_t)n);
+        uint32_t j = index_below(w.y, (uint32_t)(n - 1));
+        j += (j >= i) ? 1u : 0u;
+        V4 vi = vel[i];
+        V4 vj = vel[j];
+        R dx = vi.x - vj.x, dy = vi.y - vj.y, dz = vi.z - vj.z;
+        R vr = xsqrt(dx * dx + dy * dy + dz * dz);
+        R svr = P.sigma * vr;
+        if (svr > sigvrmax) sigvrmax = svr;
+        R pa = svr * pacc;
+        R u = u01<R>(w.z, w2.z);
+        if (u < pa) {
+            R ct = R(2) * u01<R>(w.w, w2.w) - R(1);
+            R st2 = R(1) - ct * ct;
+            R st = xsqrt(st2 > R(0) ? st2 : R(0));
+            R phi = two_pi * u01<R>(w2.x, w2.y);
+            R sp, cp;
+            xsincos(phi, &sp, &cp);
+            R hv = R(0.5) * vr;
+            R nx = st * cp, ny = st * sp, nz = ct;
+            R cx = R(0.5) * (vi.x + vj.x), cy = R(0.5) * (vi.y + vj.y), cz = R(0.5) * (vi.z + vj.z);
+            vi.x = cx + hv * nx; vi.y = cy + hv * ny; vi.z = cz + hv * nz;
+            vj.x = cx - hv * nx; vj.y = cy - hv * ny; vj.z = cz - hv * nz;
+            vel[i] = vi;
+            vel[j] = vj;
+            res.accepted += 1;
+        }
+    }
+    res.candidates = ncand;
+    return res;
+}
+
+// ---------------------------------------------------------------------------------------
+// Initial state of one atom (generateInitialDist, setUp.cu:129-165, with an exact sampler):
+//   quadrupole: scaled radius rho = sqrt(x^2/4+y^2/4+z^2) has density ~ rho^2 exp(-rho/r0),
+//     i.e. Gamma(3, r0): rho = -r0 log(u1 u2 u3); direction isotropic in (x/2, y/2, z);
+//   Ioffe-Pritchard: bounded rejection sampling, uniform proposal over the grid box,
+//     acceptance exp(-mu (|B| - B_floor) / kT);
+//   box: uniform over the grid box.
+// Velocities: Maxwellian N(0, kT/m) per axis by Box-Muller.  Spinor aligned with B^
+// (the +1 eigenvector of s.B^, without the rsqrt(1 + B^x) singularity of setUp.cu:240).
+// Returns false if rejection sampling gave up (the atom is then placed at the trap centre).
+// ---------------------------------------------------------------------------------------
+template <class R>
+DSMC_HD bool init_atom(const CloudPhys<R>& P, int init_mode, uint32_t local_id, uint64_t seed,
+                       Atom<R>& a) {
+    const R two_pi = R(6.283185307179586476925286766559);
+    bool ok = true;
+    if (init_mode == 1 || P.trap == TRAP_BOX) {
+        u32x4 w = draw(local_id, 0u, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 0u, seed);
+        u32x4 w2 = draw(local_id, 0u, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 1u, seed);
+        a.x = P.gmin_x + P.box_x * u01<R>(w.x, w2.x);
+        a.y = P.gmin_y + P.box_y * u01<R>(w.y, w2.y);
+        a.z = P.gmin_z + P.box_z * u01<R>(w.z, w2.z);
+    } else if (P.trap == TRAP_QUADRUPOLE) {
+        u32x4 w = draw(local_id, 0u, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 0u, seed);
+        u32x4 w2 = draw(local_id, 0u, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 1u, seed);
+        R u1 = u01<R>(w.x, w2.x), u2 = u01<R>(w.y, w2.y), u3 = u01<R>(w.z, w2.z);
+        R rho = -P.r0_init * (xlog(u1) + xlog(u2) + xlog(u3));
+        R ct = R(2) * u01<R>(w.w, w2.w) - R(1);
+        u32x4 w3 = draw(local_id, 0u, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 2u, seed);
+        R phi = two_pi * u01<R>(w3.x, w3.y);
+        R st2 = R(1) - ct * ct;
+        R st = xsqrt(st2 > R(0) ? st2 : R(0));
+        R sp, cp;
+        xsincos(phi, &sp, &cp);
+        // scaled coordinates (x/2, y/2, z) are isotropic; the bias shifts the zero along z
+        a.x = R(2) * (rho * (st * cp));
+        a.y = R(2) * (rho * (st * sp));
+        a.z = rho * ct + (P.Bp != R(0) ? P.B0 / P.Bp : R(0));
+    } else {
+        ok = false;
+        a.x = R(0); a.y = R(0); a.z = R(0);
+        for (uint32_t t = 0; t < 4096u; ++t) {
+            u32x4 w = draw(local_id, t, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 0u, seed);
+            u32x4 w2 = draw(local_id, t, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 1u, seed);
+            R x = P.gmin_x + P.box_x * u01<R>(w.x, w2.x);
+            R y = P.gmin_y + P.box_y * u01<R>(w.y, w2.y);
+            R z = P.gmin_z + P.box_z * u01<R>(w.z, w2.z);
+            Field<R> f;
+            trap_field(P, x, y, z, f);
+            R pr = xexp(-(P.inv_kT_over_mu * (f.absB - P.B_floor)));
+            if (u01<R>(w.w, w2.w) < pr) {
+                a.x = x; a.y = y; a.z = z;
+                ok = true;
+                break;
+            }
+        }
+    }
+    // Maxwellian velocities by Box-Muller
+    u32x4 v = draw(local_id, 0u, PURPOSE_INIT_VEL, (uint32_t)P.cloud_id, 0u, seed);
+    u32x4 v2 = draw(local_id, 0u, PURPOSE_INIT_VEL, (uint32_t)P.cloud_id, 1u, seed);
+    R g[4];
+    {
+        R r1 = xsqrt(R(-2) * xlog(u01<R>(v.x, v2.x)));
+        R s1, c1;
+        xsincos(two_pi * u01<R>(v.y, v2.y), &s1, &c1);
+        R r2 = xsqrt(R(-2) * xlog(u01<R>(v.z, v2.z)));
+        R s2, c2;
+        xsincos(two_pi * u01<R>(v.w, v2.w), &s2, &c2);
+        g[0] = r1 * c1; g[1] = r1 * s1; g[2] = r2 * c2; g[3] = r2 * s2;
+    }
+    a.vx = P.v_init * g[0];
+    a.vy = P.v_init * g[1];
+    a.vz = P.v_init * g[2];
+    // aligned spinor
+    Field<R> f;
+    trap_field(P, a.x, a.y, a.z, f);
+    if (f.bz >= R(0)) {
+        R h = xsqrt(R(0.5) * (R(1) + f.bz));
+        R inv = R(1) / (R(2) * h);
+        a.ur = h; a.ui = R(0);
+        a.dr = f.bx * inv; a.di = f.by * inv;
+    } else {
+        R h = xsqrt(R(0.5) * (R(1) - f.bz));
+        R inv = R(1) / (R(2) * h);
+        a.ur = f.bx * inv; a.ui = -(f.by * inv);
+        a.dr = h; a.di = R(0);
+    }
+    a.flags = 0u;
+    return ok;
+}
+
+}  // namespace dsmc
+
+#endif  // DSMC_PHYSICS_H

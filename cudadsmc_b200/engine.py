@@ -1,0 +1,210 @@
+"""Python binding of the sm_100a DSMC engine (libdsmc_b200.so, C ABI in include/dsmc.h).
+
+``Simulation`` follows the call structure of CUDADSMC's ``main()`` (CUDADSMC/src/main.cu):
+create the handle (allocation, main.cu:83-140), ``init_cloud`` (h_initRNG +
+h_generateInitialDist + initSigvrmax, setUp.cu:32-292), ``step`` (one pass of the loop body,
+main.cu:416-523) and ``diagnostics`` / ``get_state`` (the snapshot copies, main.cu:526-577).
+There is no CPU fallback: if the library is missing or no GPU is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import CloudParams, Diag, RunParams, StateBuffers
+
+_LIB = None
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdsmc_b200.so")
+
+# every symbol include/dsmc.h declares
+EXPORTED_SYMBOLS = (
+    "dsmc_abi_version", "dsmc_status_string", "dsmc_last_error", "dsmc_preset", "dsmc_create",
+    "dsmc_destroy", "dsmc_set_stream", "dsmc_init_cloud", "dsmc_step", "dsmc_synchronize",
+    "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
+    "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
+    "dsmc_launches_per_step",
+)
+
+
+class DSMCError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Loads libdsmc_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} is missing: build it with `python -m cudadsmc_b200.build`")
+    lib = C.CDLL(p)
+    vp, i32, i64, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64
+    sig = {
+        "dsmc_abi_version": (i32, []),
+        "dsmc_status_string": (C.c_char_p, [i32]),
+        "dsmc_last_error": (C.c_char_p, [vp]),
+        "dsmc_preset": (i32, [i32, C.POINTER(RunParams), C.POINTER(CloudParams)]),
+        "dsmc_create": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), i32, C.POINTER(vp)]),
+        "dsmc_destroy": (i32, [vp]),
+        "dsmc_set_stream": (i32, [vp, vp]),
+        "dsmc_init_cloud": (i32, [vp, u64]),
+        "dsmc_step": (i32, [vp, i32]),
+        "dsmc_synchronize": (i32, [vp]),
+        "dsmc_diagnostics": (i32, [vp, i32, C.POINTER(Diag)]),
+        "dsmc_get_state": (i32, [vp, C.POINTER(StateBuffers)]),
+        "dsmc_set_state": (i32, [vp, C.POINTER(StateBuffers)]),
+        "dsmc_get_cell_starts": (i32, [vp, C.POINTER(C.c_int32), i64, C.POINTER(i64)]),
+        "dsmc_get_sigvrmax": (i32, [vp, vp, i64]),
+        "dsmc_set_sigvrmax": (i32, [vp, vp, i64]),
+        "dsmc_set_profiling": (i32, [vp, i32]),
+        "dsmc_kernel_times": (i32, [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(i64), i32,
+                                    C.POINTER(i32)]),
+        "dsmc_launches_per_step": (i32, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def preset(which: int) -> tuple[RunParams, CloudParams]:
+    """Named workloads of the engine (see dsmc_preset in include/dsmc.h)."""
+    lib = load_library()
+    run, cloud = RunParams(), CloudParams()
+    st = lib.dsmc_preset(which, C.byref(run), C.byref(cloud))
+    if st != 0:
+        raise DSMCError(st, f"unknown preset {which}")
+    return run, cloud
+
+
+def real_dtype(run: RunParams):
+    return np.float32 if run.precision == _abi.FP32 else np.float64
+
+
+class Simulation:
+    """One engine handle: one or more clouds advanced together on the current GPU."""
+
+    def __init__(self, run: RunParams, clouds: CloudParams | Sequence[CloudParams]):
+        self.lib = load_library()
+        if isinstance(clouds, CloudParams):
+            clouds = [clouds]
+        self.run = run.copy()
+        self.clouds = [c.copy() for c in clouds]
+        arr = (CloudParams * len(self.clouds))(*self.clouds)
+        h = C.c_void_p()
+        st = self.lib.dsmc_create(C.byref(self.run), arr, len(self.clouds), C.byref(h))
+        if st != 0:
+            raise DSMCError(st, self.lib.dsmc_last_error(None).decode())
+        self._h = h
+        self.dtype = real_dtype(run)
+
+    # -- lifecycle ---------------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.dsmc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise DSMCError(st, self.lib.dsmc_last_error(self._h).decode())
+
+    # -- reference loop --------------------------------------------------------------------------
+    def init_cloud(self, seed: int | None = None) -> None:
+        self._check(self.lib.dsmc_init_cloud(self._h, int(self.run.seed if seed is None else seed)))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.lib.dsmc_step(self._h, int(nsteps)))
+
+    def synchronize(self) -> None:
+        self._check(self.lib.dsmc_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self.lib.dsmc_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def diagnostics(self, cloud: int = -1) -> dict:
+        d = Diag()
+        self._check(self.lib.dsmc_diagnostics(self._h, int(cloud), C.byref(d)))
+        return d.as_dict()
+
+    # -- state -------------------------------------------------------------------------------------
+    def n_alive(self) -> int:
+        return int(self.diagnostics()["n_alive"])
+
+    def get_state(self) -> dict:
+        """Sorted state: pos/vel/psi as (n, 4) arrays, atom ids, cloud counts."""
+        cap = int(sum(max(c.capacity, c.n_atoms) for c in self.clouds))
+        pos = np.empty((cap, 4), self.dtype)
+        vel = np.empty((cap, 4), self.dtype)
+        psi = np.empty((cap, 4), self.dtype)
+        counts = np.zeros(len(self.clouds), np.int64)
+        b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, cap,
+                         counts.ctypes.data_as(C.POINTER(C.c_int64)))
+        self._check(self.lib.dsmc_get_state(self._h, C.byref(b)))
+        n = int(b.n)
+        return {"pos": pos[:n], "vel": vel[:n], "psi": psi[:n], "cloud_counts": counts}
+
+    def set_state(self, pos: np.ndarray, vel: np.ndarray, psi: np.ndarray, cloud_counts) -> None:
+        pos = np.ascontiguousarray(pos, self.dtype)
+        vel = np.ascontiguousarray(vel, self.dtype)
+        psi = np.ascontiguousarray(psi, self.dtype)
+        counts = np.ascontiguousarray(np.asarray(cloud_counts, np.int64))
+        n = pos.shape[0]
+        b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, n,
+                         counts.ctypes.data_as(C.POINTER(C.c_int64)))
+        self._check(self.lib.dsmc_set_state(self._h, C.byref(b)))
+
+    def cell_starts(self) -> np.ndarray:
+        total = C.c_int64()
+        self._check(self.lib.dsmc_get_cell_starts(self._h, None, 0, C.byref(total)))
+        out = np.empty(total.value + 1, np.int32)
+        self._check(self.lib.dsmc_get_cell_starts(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                  out.size, C.byref(total)))
+        return out
+
+    def sigvrmax(self) -> np.ndarray:
+        total = C.c_int64()
+        self._check(self.lib.dsmc_get_cell_starts(self._h, None, 0, C.byref(total)))
+        out = np.empty(total.value, self.dtype)
+        self._check(self.lib.dsmc_get_sigvrmax(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_sigvrmax(self, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, self.dtype)
+        self._check(self.lib.dsmc_set_sigvrmax(self._h, v.ctypes.data, v.size))
+
+    # -- profiling ---------------------------------------------------------------------------------
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.lib.dsmc_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        names = (C.c_char_p * 32)()
+        ms = (C.c_double * 32)()
+        launches = (C.c_int64 * 32)()
+        cnt = C.c_int32()
+        self._check(self.lib.dsmc_kernel_times(self._h, names, ms, launches, 32, C.byref(cnt)))
+        return {names[i].decode(): (ms[i], launches[i]) for i in range(cnt.value)}
+
+    def launches_per_step(self) -> int:
+        return int(self.lib.dsmc_launches_per_step(self._h))

@@ -1,0 +1,202 @@
+/*
+ * dsmc.h -- C ABI of the B200 DSMC engine (libdsmc_b200.so).
+ *
+ * One handle simulates one or more independent atom clouds ("clouds") with the
+ * Direct Simulation Monte Carlo timestep of inJeans/CUDADSMC:
+ *   collide (Bird no-time-counter, s-wave) -> Larmor spin precession ->
+ *   velocity-Verlet motion in the trap -> Majorana / energy-knife evaporation ->
+ *   cell index -> stable sort by cell -> diagnostics.
+ *
+ * Conventions (all entry points):
+ *   - every call returns dsmc_status (0 = DSMC_OK); dsmc_last_error() gives text;
+ *   - the handle owns all device memory; callers pass host pointers only, except
+ *     dsmc_set_stream (a cudaStream_t passed as void*) and the *_device calls;
+ *   - all GPU work is enqueued on the handle's stream; calls on one handle are
+ *     not thread-safe, separate handles are independent.
+ *
+ * Reference interfaces replaced (paths inside the CUDADSMC project):
+ *   dsmc_create            <- cudaCalloc block + params, CUDADSMC/src/main.cu:83-140,165-174
+ *   dsmc_init_cloud        <- h_initRNG + h_generateInitialDist + initSigvrmax,
+ *                             CUDADSMC/src/setUp.cu:32,79,287; first index/sort main.cu:191-198
+ *   dsmc_step              <- one pass of the main loop body, CUDADSMC/src/main.cu:416-523:
+ *                             indexAtoms (collisions.cu:21), sortArrays (collisions.cu:275),
+ *                             cellStartandEndKernel/findNumberOfAtomsInCell/exclusive_scan
+ *                             (collisions.cu:228,254; main.cu:440), collide (collisions.cu:291),
+ *                             evolveWavefunction (wavefunction.cu:11), moveAtoms (moveAtoms.cu:23),
+ *                             evaporationTag + remove_if (evaporation.cu:68; main.cu:493),
+ *                             normalise (wavefunction.cu:279)
+ *   dsmc_diagnostics       <- calculateTemp (evaporation.cu:108) + atomNumber/collisionCount
+ *                             snapshot fields (main.cu:526-577)
+ *   dsmc_get_state/set_state <- the D2H snapshot copies, CUDADSMC/src/main.cu:526-536
+ */
+#ifndef DSMC_B200_H
+#define DSMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define DSMC_EXTERN extern "C"
+#else
+#define DSMC_EXTERN extern
+#endif
+#define DSMC_API DSMC_EXTERN __attribute__((visibility("default")))
+
+#define DSMC_ABI_VERSION 1
+
+typedef enum dsmc_status {
+    DSMC_OK = 0,
+    DSMC_ERR_INVALID = 1,     /* bad argument or parameter */
+    DSMC_ERR_CUDA = 2,        /* CUDA runtime error (no device, launch failure...) */
+    DSMC_ERR_ALLOC = 3,       /* device or host allocation failed */
+    DSMC_ERR_CAPACITY = 4,    /* atom capacity exceeded */
+    DSMC_ERR_CELL_FULL = 5,   /* a grid cell holds more atoms than one tile can stage */
+    DSMC_ERR_NAN = 6,         /* non-finite position or velocity met */
+    DSMC_ERR_STATE = 7,       /* call out of order (e.g. step before init) */
+    DSMC_ERR_UNSUPPORTED = 8, /* feature not available in this build / mode */
+    DSMC_ERR_TIMEOUT = 9      /* a bounded device-side wait gave up */
+} dsmc_status;
+
+enum { DSMC_FP32 = 0, DSMC_FP64 = 1 };
+
+/* Trap models. QUADRUPOLE: B = B'(x/2, y/2, -z) + B0 z^ (the linear trap of the
+ * benchmark configs; B0 is an optional uniform bias).  IOFFE_PRITCHARD: the field of
+ * CUDADSMC/src/moveAtoms.cu:135-142, B = B0 z^ + B'(x,-y,0) + B''/2(-xz,-yz,z^2-(x^2+y^2)/2).
+ * BOX: no field, periodic boundaries on the grid box (homogeneous-gas checks). */
+enum { DSMC_TRAP_QUADRUPOLE = 0, DSMC_TRAP_IOFFE_PRITCHARD = 1, DSMC_TRAP_BOX = 2 };
+
+/* Per-cloud behaviour flags. */
+enum {
+    DSMC_F_COLLIDE = 1 << 0,      /* NTC collisions */
+    DSMC_F_LARMOR = 1 << 1,       /* spinor precession about the local field */
+    DSMC_F_MAJORANA = 1 << 2,     /* remove atoms with <sigma.B^> < 0 (evaporation.cu:90-95) */
+    DSMC_F_KNIFE = 1 << 3,        /* remove atoms with E > eta(step) kB T */
+    DSMC_F_NORMALISE = 1 << 4,    /* renormalise the spinor after every rotation */
+    DSMC_F_KNIFE_FIXED_T = 1 << 5 /* knife uses the initial T instead of the running T */
+};
+
+/* Initial distributions. */
+enum {
+    DSMC_INIT_THERMAL = 0, /* Boltzmann density of the trap (exact Gamma(3) sampler for the
+                              quadrupole, bounded rejection sampling otherwise) */
+    DSMC_INIT_UNIFORM = 1  /* uniform over the grid box (BOX trap) */
+};
+
+#define DSMC_MAX_KNOTS 9
+
+typedef struct dsmc_cloud_params {
+    int64_t n_atoms;      /* initial number of test particles */
+    int64_t capacity;     /* maximum atoms (0 -> n_atoms) */
+    int32_t trap;         /* DSMC_TRAP_* */
+    int32_t flags;        /* DSMC_F_* */
+    int32_t cells[3];     /* grid cells per axis (overflow cell added internally) */
+    int32_t init_mode;    /* DSMC_INIT_* */
+    double grid_min[3];   /* grid box lower corner (m) */
+    double grid_max[3];   /* grid box upper corner (m) */
+    double mass;          /* atom mass (kg) */
+    double moment;        /* magnetic moment mu (J/T): U = mu |B|, theta = mu |B| dt / hbar */
+    double B0;            /* bias field along z (T) */
+    double dBdz;          /* field gradient B' (T/m) */
+    double d2Bdz2;        /* field curvature B'' (T/m^2), Ioffe-Pritchard only */
+    double temperature;   /* initial temperature (K) */
+    double alpha;         /* real atoms per test particle */
+    double sigma;         /* collision cross-section (m^2) */
+    double sigvrmax_init; /* initial (sigma v_r)_max per cell (m^3/s); 0 -> sigma sqrt(16 kB T/(pi m)) */
+    int32_t knife_nknots; /* piecewise-linear knife ramp eta(step), up to DSMC_MAX_KNOTS knots */
+    int32_t stream_id;    /* Philox stream of this cloud (24 bits): a cloud run alone and the same
+                             cloud inside a batch give identical results when their stream ids match */
+    double knife_step[DSMC_MAX_KNOTS];
+    double knife_eta[DSMC_MAX_KNOTS];
+} dsmc_cloud_params;
+
+typedef struct dsmc_params {
+    int32_t precision;     /* DSMC_FP32 or DSMC_FP64 */
+    int32_t collide_every; /* motion steps per collision step (reference: loopsPerCollision) */
+    double dt;             /* timestep (s) */
+    double hbar;           /* 0 -> 1.05457148e-34 (CUDADSMC/include/deviceSystemParameters.cuh:18) */
+    double kB;             /* 0 -> 1.3806503e-23 */
+    uint64_t seed;         /* Philox key for init (overridden by dsmc_init_cloud) and collisions */
+    int32_t tile_atoms;    /* nominal atoms per tile (0 -> engine default) */
+    int32_t use_graphs;    /* 1 -> replay captured CUDA graphs in dsmc_step (default), 0 -> plain launches */
+} dsmc_params;
+
+typedef struct dsmc_diag {
+    int64_t step;          /* steps taken since init */
+    double time;           /* simulated time (s) */
+    int64_t n_alive;       /* atoms in the cloud */
+    double e_kin;          /* total kinetic energy of the test particles (J) */
+    double e_pot;          /* total potential energy mu |B| (J) */
+    double temperature;    /* m <v^2> / (3 kB) (K) */
+    double sum_v2;         /* sum of v^2 (m^2/s^2), exact fixed-point sum */
+    double sum_absB;       /* sum of |B| (T), exact fixed-point sum */
+    int64_t n_evaporated;  /* cumulative atoms removed (Majorana + knife) */
+    int64_t n_majorana;    /* cumulative Majorana losses */
+    int64_t n_knife;       /* cumulative knife losses */
+    double e_evaporated;   /* cumulative energy carried away (J) */
+    int64_t collisions;    /* cumulative accepted collisions */
+    int64_t candidates;    /* cumulative NTC candidate pairs */
+    int64_t atom_steps;    /* cumulative sum over steps of the atoms each step processed */
+    int32_t error;         /* device error bits seen so far (0 = none) */
+    int32_t reserved0;
+} dsmc_diag;
+
+/* Host-side view of the atom state, structure-of-arrays with 4 reals per atom
+ * (float for DSMC_FP32, double for DSMC_FP64):
+ *   pos[4i..4i+3] = x, y, z, atom id (integer bits in the 4th lane)
+ *   vel[4i..4i+3] = vx, vy, vz, flag bits (bit 0: anti-trapped spin state)
+ *   psi[4i..4i+3] = Re psi_up, Im psi_up, Re psi_dn, Im psi_dn
+ * Atoms are grouped by cloud; cloud_counts[k] atoms of cloud k, in cloud order. */
+typedef struct dsmc_state_buffers {
+    void* pos;
+    void* vel;
+    void* psi;
+    int64_t n;              /* in: capacity of the buffers (get) / atoms given (set); out: atoms */
+    int64_t* cloud_counts;  /* nclouds entries */
+} dsmc_state_buffers;
+
+typedef struct dsmc_handle dsmc_handle;
+
+DSMC_API int32_t dsmc_abi_version(void);
+DSMC_API const char* dsmc_status_string(dsmc_status s);
+DSMC_API const char* dsmc_last_error(const dsmc_handle* h);
+
+/* Fills run and cloud parameters with one of the named workloads
+ *   0: small trapped cloud, FP64 (1e4 atoms, 50^3 cells, B'=2.5 T/m, 20 uK)
+ *   1: homogeneous periodic box (1e6 atoms, 100^3 cells, 10 uK, alpha = 1e4)
+ *   2: full trapped step (1e7 atoms, 128^3 cells, 50 uK, Larmor + Majorana + knife 6->4)
+ *   4: adjoint workload (1e6 atoms, 0.1 mT bias, 30 uK, 8-knot knife)
+ * n_atoms and cells may be overridden afterwards. */
+DSMC_API dsmc_status dsmc_preset(int32_t which, dsmc_params* run, dsmc_cloud_params* cloud);
+
+DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params* clouds,
+                                 int32_t nclouds, dsmc_handle** out);
+DSMC_API dsmc_status dsmc_destroy(dsmc_handle* h);
+DSMC_API dsmc_status dsmc_set_stream(dsmc_handle* h, void* cuda_stream);
+
+DSMC_API dsmc_status dsmc_init_cloud(dsmc_handle* h, uint64_t seed);
+DSMC_API dsmc_status dsmc_step(dsmc_handle* h, int32_t nsteps);
+DSMC_API dsmc_status dsmc_synchronize(dsmc_handle* h);
+
+/* cloud >= 0: that cloud; cloud == -1: sums over all clouds (temperature from the sums). */
+DSMC_API dsmc_status dsmc_diagnostics(dsmc_handle* h, int32_t cloud, dsmc_diag* out);
+
+DSMC_API dsmc_status dsmc_get_state(dsmc_handle* h, dsmc_state_buffers* out);
+DSMC_API dsmc_status dsmc_set_state(dsmc_handle* h, const dsmc_state_buffers* in);
+
+/* Cell bookkeeping of the current sorted order: start[c] for every global cell
+ * (grid cells of each cloud then its overflow cell), plus start[total] = n_alive.
+ * ncells_total receives the number of global cells. */
+DSMC_API dsmc_status dsmc_get_cell_starts(dsmc_handle* h, int32_t* start, int64_t capacity,
+                                          int64_t* ncells_total);
+/* Per-cell (sigma v_r)_max, one real per global cell (float or double). */
+DSMC_API dsmc_status dsmc_get_sigvrmax(dsmc_handle* h, void* out, int64_t capacity);
+DSMC_API dsmc_status dsmc_set_sigvrmax(dsmc_handle* h, const void* in, int64_t n);
+
+/* Per-kernel device time (ms) accumulated while profiling is on; names[i] are static strings.
+ * Profiling launches every kernel separately, bracketed by CUDA events on the handle's stream. */
+DSMC_API dsmc_status dsmc_set_profiling(dsmc_handle* h, int32_t on);
+DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, double* ms,
+                                       int64_t* launches, int32_t capacity, int32_t* count);
+/* Number of kernel launches one dsmc_step(h, 1) issues. */
+DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h);
+
+#endif /* DSMC_B200_H */

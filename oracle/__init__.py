@@ -1,0 +1,185 @@
+"""CPU oracle of the DSMC timestep -- TEST INFRASTRUCTURE ONLY.
+
+Python binding of oracle/build/liboracle.so (dsmc_oracle.cpp, a serial C++ restatement of
+CUDADSMC's timestep that shares the IEEE-exact per-atom arithmetic of the engine).  Only the
+tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it; the engine never
+does.  ``Oracle`` mirrors ``cudadsmc_b200.Simulation`` method for method.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+from cudadsmc_b200._abi import CloudParams, Diag, RunParams, StateBuffers, FP32
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
+_LIB = None
+
+
+def load() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            from cudadsmc_b200 import build as _b
+            _b.build_oracle()
+        lib = C.CDLL(LIB_PATH)
+        vp, i32, i64, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64
+        sig = {
+            "oracle_create": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), i32, i32, C.POINTER(vp)]),
+            "oracle_last_error": (C.c_char_p, [vp]),
+            "oracle_destroy": (None, [vp]),
+            "oracle_init": (i32, [vp, u64]),
+            "oracle_step": (i32, [vp, i32]),
+            "oracle_diag": (i32, [vp, i32, C.POINTER(Diag)]),
+            "oracle_get_state": (i32, [vp, C.POINTER(StateBuffers)]),
+            "oracle_set_state": (i32, [vp, C.POINTER(StateBuffers)]),
+            "oracle_get_cell_starts": (i32, [vp, C.POINTER(C.c_int32), i64, C.POINTER(i64)]),
+            "oracle_get_sigvrmax": (i32, [vp, vp, i64]),
+            "oracle_set_sigvrmax": (i32, [vp, vp, i64]),
+            "oracle_max_threads": (i32, []),
+            "oracle_set_threads": (None, [i32]),
+            "oracle_preset": (i32, [i32, C.POINTER(RunParams), C.POINTER(CloudParams)]),
+            "oracle_philox": (None, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+            "oracle_math_f": (None, [i32, C.POINTER(C.c_float), C.POINTER(C.c_float), i64]),
+            "oracle_math_d": (None, [i32, C.POINTER(C.c_double), C.POINTER(C.c_double), i64]),
+            "oracle_field_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), i64]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def preset(which: int) -> tuple[RunParams, CloudParams]:
+    run, cloud = RunParams(), CloudParams()
+    if load().oracle_preset(which, C.byref(run), C.byref(cloud)) != 0:
+        raise ValueError(f"unknown preset {which}")
+    return run, cloud
+
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    c = (C.c_uint32 * 4)(*[int(x) & 0xFFFFFFFF for x in ctr])
+    k = (C.c_uint32 * 2)(*[int(x) & 0xFFFFFFFF for x in key])
+    o = (C.c_uint32 * 4)()
+    load().oracle_philox(c, k, o)
+    return np.array(list(o), np.uint32)
+
+
+def math(which: str, x: np.ndarray) -> np.ndarray:
+    code = {"sin": 0, "cos": 1, "log": 2, "exp": 3}[which]
+    x = np.ascontiguousarray(x)
+    y = np.empty_like(x)
+    if x.dtype == np.float32:
+        load().oracle_math_f(code, x.ctypes.data_as(C.POINTER(C.c_float)), y.ctypes.data_as(C.POINTER(C.c_float)), x.size)
+    else:
+        x = x.astype(np.float64)
+        y = np.empty_like(x)
+        load().oracle_math_d(code, x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)), x.size)
+    return y
+
+
+def field(run: RunParams, cloud: CloudParams, xyz: np.ndarray) -> np.ndarray:
+    xyz = np.ascontiguousarray(xyz, np.float64)
+    out = np.empty((xyz.shape[0], 7), np.float64)
+    load().oracle_field_d(C.byref(run), C.byref(cloud), xyz.ctypes.data_as(C.POINTER(C.c_double)),
+                          out.ctypes.data_as(C.POINTER(C.c_double)), xyz.shape[0])
+    return out
+
+
+def max_threads() -> int:
+    return int(load().oracle_max_threads())
+
+
+def set_threads(n: int) -> None:
+    load().oracle_set_threads(int(n))
+
+
+class Oracle:
+    """CPU restatement with the Simulation interface. fast=True selects the OpenMP path."""
+
+    def __init__(self, run: RunParams, clouds: CloudParams | Sequence[CloudParams], fast: bool = False):
+        self.lib = load()
+        if isinstance(clouds, CloudParams):
+            clouds = [clouds]
+        self.run = run.copy()
+        self.clouds = [c.copy() for c in clouds]
+        arr = (CloudParams * len(self.clouds))(*self.clouds)
+        h = C.c_void_p()
+        if self.lib.oracle_create(C.byref(self.run), arr, len(self.clouds), 1 if fast else 0, C.byref(h)) != 0:
+            raise ValueError(self.lib.oracle_last_error(None).decode())
+        self._h = h
+        self.dtype = np.float32 if run.precision == FP32 else np.float64
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise RuntimeError(self.lib.oracle_last_error(self._h).decode())
+
+    def init_cloud(self, seed: int | None = None):
+        self._check(self.lib.oracle_init(self._h, int(self.run.seed if seed is None else seed)))
+
+    def step(self, n: int = 1):
+        self._check(self.lib.oracle_step(self._h, int(n)))
+
+    def diagnostics(self, cloud: int = -1) -> dict:
+        d = Diag()
+        self._check(self.lib.oracle_diag(self._h, int(cloud), C.byref(d)))
+        return d.as_dict()
+
+    def get_state(self) -> dict:
+        cap = int(sum(max(c.capacity, c.n_atoms) for c in self.clouds))
+        cap = max(cap, 1)
+        pos = np.empty((cap, 4), self.dtype)
+        vel = np.empty((cap, 4), self.dtype)
+        psi = np.empty((cap, 4), self.dtype)
+        counts = np.zeros(len(self.clouds), np.int64)
+        b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, cap,
+                         counts.ctypes.data_as(C.POINTER(C.c_int64)))
+        self._check(self.lib.oracle_get_state(self._h, C.byref(b)))
+        n = int(b.n)
+        return {"pos": pos[:n], "vel": vel[:n], "psi": psi[:n], "cloud_counts": counts}
+
+    def set_state(self, pos, vel, psi, cloud_counts):
+        pos = np.ascontiguousarray(pos, self.dtype)
+        vel = np.ascontiguousarray(vel, self.dtype)
+        psi = np.ascontiguousarray(psi, self.dtype)
+        counts = np.ascontiguousarray(np.asarray(cloud_counts, np.int64))
+        b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, pos.shape[0],
+                         counts.ctypes.data_as(C.POINTER(C.c_int64)))
+        self._check(self.lib.oracle_set_state(self._h, C.byref(b)))
+
+    def cell_starts(self) -> np.ndarray:
+        total = C.c_int64()
+        self._check(self.lib.oracle_get_cell_starts(self._h, None, 0, C.byref(total)))
+        out = np.empty(total.value + 1, np.int32)
+        self._check(self.lib.oracle_get_cell_starts(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size,
+                                                    C.byref(total)))
+        return out
+
+    def sigvrmax(self) -> np.ndarray:
+        total = C.c_int64()
+        self._check(self.lib.oracle_get_cell_starts(self._h, None, 0, C.byref(total)))
+        out = np.empty(total.value, self.dtype)
+        self._check(self.lib.oracle_get_sigvrmax(self._h, out.ctypes.data, out.size))
+        return out
+
+    def set_sigvrmax(self, values):
+        v = np.ascontiguousarray(values, self.dtype)
+        self._check(self.lib.oracle_set_sigvrmax(self._h, v.ctypes.data, v.size))

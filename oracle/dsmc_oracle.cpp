@@ -1,0 +1,501 @@
+// dsmc_oracle.cpp -- CPU restatement of the CUDADSMC timestep.  TEST INFRASTRUCTURE ONLY:
+// used by tests/, __graft_entry__.smoke() and bench.py's CPU baseline as the checker and the
+// timed host-core baseline; the product (cudadsmc_b200) never links or calls it.
+//
+// What it restates (paths inside the CUDADSMC project):
+//   main loop order            src/main.cu:410-524 (index/sort, collide, spin, move, evaporate)
+//   initial cloud              src/setUp.cu:129-252 (exact Gamma(3) sampler for the linear trap)
+//   (sigma v_r)max init        src/setUp.cu:287-292
+//   cell index                 src/collisions.cu:163-226
+//   sort by cell               src/collisions.cu:275-287 (thrust::sort_by_key, stable)
+//   NTC collisions             src/collisions.cu:291-437, 529-546
+//   Larmor + normalise         src/wavefunction.cu:11-73, 279-299
+//   Verlet motion              src/moveAtoms.cu:23-157
+//   evaporation tag + compact  src/evaporation.cu:68-106, src/main.cu:493-498
+//   temperature                src/evaporation.cu:108-128
+// with the intended semantics where the reference has defects: the sort pairs each atom with
+// its own cell (collisions.cu:181 vs 282-284), candidate pairs are uniform over all distinct
+// pairs (collisions.cu:407 never picks the last atom), dt is the run's dt everywhere
+// (collisions.cu:314, wavefunction.cu:45,63 hard-code 1e-7).
+//
+// The per-atom and per-cell arithmetic is the shared header dsmc_physics.h (IEEE-exact
+// operations only), so results are bit-identical to the GPU for the same inputs.  The
+// serial path (fast = 0) defines the sorted order directly as a stable sort of the survivors
+// by (new cell, moved); the OpenMP path (fast = 1) builds the same order in parallel and is
+// the timed CPU baseline.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "dsmc.h"
+#include "dsmc_physics.h"
+#include "dsmc_setup.h"
+
+using namespace dsmc;
+
+namespace {
+
+template <class R> struct Q4 { R x, y, z, w; };
+
+struct CloudAcc {
+    long long step = 0, n_alive = 0;
+    i128 sum_v2 = 0, sum_B = 0, cum_evap_v2 = 0, cum_evap_B = 0;
+    long long cum_evap = 0, cum_maj = 0, cum_knife = 0, cum_coll = 0, cum_cand = 0, cum_atom_steps = 0;
+    double T_knife = 0;
+};
+
+struct OracleBase {
+    std::string err;
+    virtual ~OracleBase() {}
+    virtual void init(uint64_t seed) = 0;
+    virtual void step(int n) = 0;
+    virtual void diag(int cloud, dsmc_diag* out) = 0;
+    virtual void get_state(dsmc_state_buffers* o) = 0;
+    virtual void set_state(const dsmc_state_buffers* in) = 0;
+    virtual void cell_starts(int32_t* st, int64_t cap, int64_t* total) = 0;
+    virtual void get_sigvrmax(void* out, int64_t cap) = 0;
+    virtual void set_sigvrmax(const void* in, int64_t n) = 0;
+};
+
+struct OFail { std::string msg; };
+
+template <class R> struct Oracle final : OracleBase {
+    typedef Q4<R> V;
+    dsmc_params run;
+    std::vector<dsmc_cloud_params> cp;
+    std::vector<CloudPhys<R>> phys;
+    int nclouds = 0, total_cells = 0;
+    bool fast = false;
+    std::vector<int> cell_base;           // nclouds + 1
+    std::vector<int> natoms;              // atoms per cloud (current)
+    std::vector<V> pos, vel, psi;         // current state, sorted
+    std::vector<int> start;               // total_cells + 1
+    std::vector<R> sigvrmax;
+    std::vector<CloudAcc> acc;
+    int step_no = 0;
+    bool ready = false;
+
+    Oracle(const dsmc_params& r, const dsmc_cloud_params* c, int n, bool f) : run(r), cp(c, c + n), nclouds(n), fast(f) {
+        phys.resize(n);
+        cell_base.resize(n + 1);
+        int cells = 0;
+        for (int k = 0; k < n; ++k) {
+            std::string bad = validate_cloud(run, cp[k], k);
+            if (!bad.empty()) throw OFail{bad};
+            make_cloud_phys<R>(run, cp[k], k, cells, phys[k]);
+            cell_base[k] = cells;
+            cells += (int)cloud_cells(cp[k]);
+        }
+        cell_base[n] = cells;
+        total_cells = cells;
+        start.assign(total_cells + 1, 0);
+        sigvrmax.resize(total_cells);
+        for (int k = 0; k < n; ++k)
+            for (int c = cell_base[k]; c < cell_base[k + 1]; ++c) sigvrmax[c] = (R)default_sigvrmax(run, cp[k]);
+        acc.resize(n);
+        natoms.assign(n, 0);
+    }
+
+    int cloud_begin(int k) const {
+        int s = 0;
+        for (int j = 0; j < k; ++j) s += natoms[j];
+        return s;
+    }
+
+    // --------------------------------------------------------------- full sort + measure
+    void sort_by_cell_and_measure(std::vector<V>& P, std::vector<V>& Vv, std::vector<V>& S) {
+        const int n = (int)P.size();
+        std::vector<int> cell(n), order(n);
+        int i0 = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            const CloudPhys<R>& C = phys[k];
+            for (int i = i0; i < i0 + natoms[k]; ++i)
+                cell[i] = cell_of(C, P[i].x, P[i].y, P[i].z, C.trap == TRAP_BOX);
+            i0 += natoms[k];
+        }
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
+        pos.resize(n); vel.resize(n); psi.resize(n);
+        for (int j = 0; j < n; ++j) {
+            pos[j] = P[order[j]]; vel[j] = Vv[order[j]]; psi[j] = S[order[j]];
+        }
+        std::fill(start.begin(), start.end(), 0);
+        for (int j = 0; j < n; ++j) start[cell[order[j]] + 1]++;
+        for (int c = 0; c < total_cells; ++c) start[c + 1] += start[c];
+        step_no = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            CloudAcc& a = acc[k];
+            a = CloudAcc();
+            const CloudPhys<R>& C = phys[k];
+            const int b = cloud_begin(k);
+            for (int i = b; i < b + natoms[k]; ++i) {
+                Field<R> f;
+                trap_field(C, pos[i].x, pos[i].y, pos[i].z, f);
+                const R v2 = vel[i].x * vel[i].x + vel[i].y * vel[i].y + vel[i].z * vel[i].z;
+                a.sum_v2 += fx_from((double)v2);
+                a.sum_B += fx_from((double)f.absB);
+            }
+            a.n_alive = natoms[k];
+            a.T_knife = knife_temperature(C.mass, C.kB, C.T0, (C.flags & F_KNIFE_FIXED_T) != 0, a.sum_v2, a.n_alive);
+        }
+        ready = true;
+    }
+
+    void init(uint64_t seed) override {
+        run.seed = seed;
+        int n = 0;
+        for (int k = 0; k < nclouds; ++k) { natoms[k] = (int)cp[k].n_atoms; n += natoms[k]; }
+        std::vector<V> P(n), Vv(n), S(n);
+        int i0 = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            const CloudPhys<R>& C = phys[k];
+#pragma omp parallel for schedule(static) if (fast)
+            for (int j = 0; j < natoms[k]; ++j) {
+                Atom<R> a;
+                init_atom(C, cp[k].init_mode, (uint32_t)j, seed, a);
+                const int i = i0 + j;
+                P[i] = V{a.x, a.y, a.z, lane_from_u32((uint32_t)j, R(0))};
+                Vv[i] = V{a.vx, a.vy, a.vz, lane_from_u32(a.flags, R(0))};
+                S[i] = V{a.ur, a.ui, a.dr, a.di};
+            }
+            i0 += natoms[k];
+        }
+        sort_by_cell_and_measure(P, Vv, S);
+    }
+
+    void set_state(const dsmc_state_buffers* in) override {
+        int n = 0;
+        for (int k = 0; k < nclouds; ++k) { natoms[k] = (int)in->cloud_counts[k]; n += natoms[k]; }
+        if (n != in->n) throw OFail{"cloud_counts do not add up to n"};
+        std::vector<V> P(n), Vv(n), S(n);
+        memcpy(P.data(), in->pos, n * sizeof(V));
+        memcpy(Vv.data(), in->vel, n * sizeof(V));
+        memcpy(S.data(), in->psi, n * sizeof(V));
+        sort_by_cell_and_measure(P, Vv, S);
+    }
+
+    // --------------------------------------------------------------- one timestep
+    void step(int nsteps) override {
+        if (!ready) throw OFail{"step before init"};
+        for (int s = 0; s < nsteps; ++s) step_once();
+    }
+
+    void step_once() {
+        const int n = (int)pos.size();
+        const uint32_t st = (uint32_t)step_no;
+        std::vector<long long> coll(nclouds, 0), cand(nclouds, 0);
+        // 1. collisions, cell by cell (the cells of the current sorted order)
+        if (step_no % run.collide_every == 0) {
+            for (int k = 0; k < nclouds; ++k) {
+                const CloudPhys<R>& C = phys[k];
+                if (!(C.flags & F_COLLIDE)) continue;
+                long long ca = 0, cc = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : ca, cc) if (fast)
+                for (int c = C.cell_base; c < C.ovf_cell; ++c) {
+                    const int m = start[c + 1] - start[c];
+                    if (m < 2) continue;
+                    R svm = sigvrmax[c];
+                    CollideResult<R> r =
+                        collide_cell<R, V>(&vel[start[c]], m, svm, C, (uint32_t)(c - C.cell_base), st, run.seed);
+                    sigvrmax[c] = svm;
+                    ca += r.accepted;
+                    cc += r.candidates;
+                }
+                coll[k] = ca;
+                cand[k] = cc;
+            }
+        }
+        // 2. spin + motion + evaporation tests, atom by atom
+        std::vector<int> newcell(n), fate(n);
+        std::vector<unsigned char> moved(n);
+        std::vector<R> v2(n), absB(n);
+        int i0 = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            const CloudPhys<R>& C = phys[k];
+            R cut = R(0);
+            if (C.flags & F_KNIFE) {
+                double eta = knife_eta(C.knife_nknots, C.knife_step, C.knife_eta, (double)step_no);
+                cut = (R)knife_cut_v2(eta, C.kB, acc[k].T_knife, C.mass);
+            }
+            const bool box = C.trap == TRAP_BOX;
+#pragma omp parallel for schedule(static) if (fast)
+            for (int i = i0; i < i0 + natoms[k]; ++i) {
+                const int oc = cell_of(C, pos[i].x, pos[i].y, pos[i].z, box);
+                Atom<R> a;
+                a.x = pos[i].x; a.y = pos[i].y; a.z = pos[i].z;
+                a.vx = vel[i].x; a.vy = vel[i].y; a.vz = vel[i].z;
+                a.ur = psi[i].x; a.ui = psi[i].y; a.dr = psi[i].z; a.di = psi[i].w;
+                a.flags = lane_to_u32(vel[i].w);
+                AtomOut<R> o;
+                advance_atom(C, cut, a, o);
+                pos[i].x = a.x; pos[i].y = a.y; pos[i].z = a.z;
+                vel[i].x = a.vx; vel[i].y = a.vy; vel[i].z = a.vz;
+                psi[i].x = a.ur; psi[i].y = a.ui; psi[i].z = a.dr; psi[i].w = a.di;
+                newcell[i] = o.cell;
+                fate[i] = o.fate;
+                moved[i] = (o.cell != oc) ? 1 : 0;
+                v2[i] = o.v2;
+                absB[i] = o.absB;
+            }
+            i0 += natoms[k];
+        }
+        // 3. survivors sorted stably by (new cell, moved); the lost are tallied
+        std::vector<int> order;
+        if (!fast) {
+            order.reserve(n);
+            for (int i = 0; i < n; ++i)
+                if (fate[i] == FATE_ALIVE) order.push_back(i);
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                if (newcell[a] != newcell[b]) return newcell[a] < newcell[b];
+                return moved[a] < moved[b];
+            });
+        } else {
+            order = fast_order(newcell, fate, moved);
+        }
+        std::vector<V> P2(order.size()), V2(order.size()), S2(order.size());
+#pragma omp parallel for schedule(static) if (fast)
+        for (int j = 0; j < (int)order.size(); ++j) {
+            P2[j] = pos[order[j]]; V2[j] = vel[order[j]]; S2[j] = psi[order[j]];
+        }
+        // diagnostics
+        i0 = 0;
+        for (int k = 0; k < nclouds; ++k) {
+            CloudAcc& a = acc[k];
+            i128 sv = 0, sb = 0, ev = 0, eb = 0;
+            long long alive = 0, maj = 0, kn = 0;
+            for (int i = i0; i < i0 + natoms[k]; ++i) {
+                if (fate[i] == FATE_ALIVE) {
+                    ++alive;
+                    sv += fx_from((double)v2[i]);
+                    sb += fx_from((double)absB[i]);
+                } else {
+                    ev += fx_from((double)v2[i]);
+                    eb += fx_from((double)absB[i]);
+                    if (fate[i] == FATE_MAJORANA) ++maj; else ++kn;
+                }
+            }
+            a.step = step_no + 1;
+            a.n_alive = alive;
+            a.sum_v2 = sv;
+            a.sum_B = sb;
+            a.cum_evap += maj + kn;
+            a.cum_maj += maj;
+            a.cum_knife += kn;
+            a.cum_evap_v2 += ev;
+            a.cum_evap_B += eb;
+            a.cum_coll += coll[k];
+            a.cum_cand += cand[k];
+            a.cum_atom_steps += natoms[k];
+            const CloudPhys<R>& C = phys[k];
+            a.T_knife = knife_temperature(C.mass, C.kB, C.T0, (C.flags & F_KNIFE_FIXED_T) != 0, sv, alive);
+            i0 += natoms[k];
+            natoms[k] = (int)alive;
+        }
+        std::fill(start.begin(), start.end(), 0);
+        for (int j = 0; j < (int)order.size(); ++j) start[newcell[order[j]] + 1]++;
+        for (int c = 0; c < total_cells; ++c) start[c + 1] += start[c];
+        pos.swap(P2); vel.swap(V2); psi.swap(S2);
+        ++step_no;
+    }
+
+    // The same order as the stable sort, built in parallel: for every new cell its stayers
+    // (old order), then the atoms that entered it (old order).
+    std::vector<int> fast_order(const std::vector<int>& newcell, const std::vector<int>& fate,
+                                const std::vector<unsigned char>& moved) {
+        const int n = (int)newcell.size();
+        std::vector<int> stay(total_cells, 0), inc(total_cells, 0), dest(n, -1);
+        // stayers are contiguous per old cell: rank them cell by cell
+#pragma omp parallel for schedule(dynamic, 1024) if (fast)
+        for (int c = 0; c < total_cells; ++c) {
+            int r = 0;
+            for (int i = start[c]; i < start[c + 1]; ++i)
+                if (fate[i] == FATE_ALIVE && !moved[i]) dest[i] = r++;
+            stay[c] = r;
+        }
+        for (int i = 0; i < n; ++i)
+            if (fate[i] == FATE_ALIVE && moved[i]) inc[newcell[i]]++;
+        std::vector<int> ns(total_cells + 1, 0), cur(total_cells);
+        for (int c = 0; c < total_cells; ++c) ns[c + 1] = ns[c] + stay[c] + inc[c];
+        for (int c = 0; c < total_cells; ++c) cur[c] = ns[c] + stay[c];
+        std::vector<int> order(ns[total_cells]);
+#pragma omp parallel for schedule(static) if (fast)
+        for (int i = 0; i < n; ++i)
+            if (fate[i] == FATE_ALIVE && !moved[i]) order[ns[newcell[i]] + dest[i]] = i;
+        for (int i = 0; i < n; ++i)
+            if (fate[i] == FATE_ALIVE && moved[i]) order[cur[newcell[i]]++] = i;
+        return order;
+    }
+
+    // --------------------------------------------------------------- outputs
+    void diag(int cloud, dsmc_diag* out) override {
+        if (!ready) throw OFail{"diag before init"};
+        int k0 = cloud < 0 ? 0 : cloud, k1 = cloud < 0 ? nclouds : cloud + 1;
+        memset(out, 0, sizeof(*out));
+        i128 sv = 0, sb = 0;
+        double e_kin = 0, e_pot = 0, e_evap = 0, msum = 0;
+        for (int k = k0; k < k1; ++k) {
+            const CloudAcc& a = acc[k];
+            const CloudPhys<R>& C = phys[k];
+            out->step = step_no;
+            out->n_alive += a.n_alive;
+            sv += a.sum_v2;
+            sb += a.sum_B;
+            out->n_evaporated += a.cum_evap;
+            out->n_majorana += a.cum_maj;
+            out->n_knife += a.cum_knife;
+            out->collisions += a.cum_coll;
+            out->candidates += a.cum_cand;
+            out->atom_steps += a.cum_atom_steps;
+            e_kin += 0.5 * C.mass * fx_to_double(a.sum_v2);
+            e_pot += C.moment * fx_to_double(a.sum_B);
+            e_evap += 0.5 * C.mass * fx_to_double(a.cum_evap_v2) + C.moment * fx_to_double(a.cum_evap_B);
+            msum += C.mass * fx_to_double(a.sum_v2);
+        }
+        out->time = (double)step_no * run.dt;
+        out->e_kin = e_kin;
+        out->e_pot = e_pot;
+        out->sum_v2 = fx_to_double(sv);
+        out->sum_absB = fx_to_double(sb);
+        out->temperature = out->n_alive > 0 ? msum / (3.0 * phys[k0].kB * (double)out->n_alive) : 0.0;
+        out->e_evaporated = e_evap;
+    }
+
+    void get_state(dsmc_state_buffers* o) override {
+        const int n = (int)pos.size();
+        if (o->n < n) throw OFail{"state buffers too small"};
+        if (o->pos) memcpy(o->pos, pos.data(), n * sizeof(V));
+        if (o->vel) memcpy(o->vel, vel.data(), n * sizeof(V));
+        if (o->psi) memcpy(o->psi, psi.data(), n * sizeof(V));
+        o->n = n;
+        if (o->cloud_counts)
+            for (int k = 0; k < nclouds; ++k) o->cloud_counts[k] = natoms[k];
+    }
+    void cell_starts(int32_t* st, int64_t cap, int64_t* total) override {
+        if (total) *total = total_cells;
+        if (!st) return;
+        if (cap < total_cells + 1) throw OFail{"cell start buffer too small"};
+        memcpy(st, start.data(), (total_cells + 1) * sizeof(int));
+    }
+    void get_sigvrmax(void* out, int64_t cap) override {
+        if (cap < total_cells) throw OFail{"sigvrmax buffer too small"};
+        memcpy(out, sigvrmax.data(), total_cells * sizeof(R));
+    }
+    void set_sigvrmax(const void* in, int64_t n) override {
+        if (n != total_cells) throw OFail{"sigvrmax length must equal the number of cells"};
+        memcpy(sigvrmax.data(), in, total_cells * sizeof(R));
+    }
+};
+
+template <class F> int oguard(OracleBase* o, F&& f) {
+    try {
+        f();
+        if (o) o->err.clear();
+        return 0;
+    } catch (const OFail& e) {
+        if (o) o->err = e.msg;
+        return 1;
+    }
+}
+
+thread_local std::string g_err;
+
+}  // namespace
+
+#define OAPI extern "C" __attribute__((visibility("default")))
+
+OAPI int oracle_create(const dsmc_params* run, const dsmc_cloud_params* clouds, int n, int fast, void** out) {
+    try {
+        if (run->precision == DSMC_FP32) *out = new Oracle<float>(*run, clouds, n, fast != 0);
+        else *out = new Oracle<double>(*run, clouds, n, fast != 0);
+        return 0;
+    } catch (const OFail& e) {
+        g_err = e.msg;
+        *out = nullptr;
+        return 1;
+    }
+}
+OAPI const char* oracle_last_error(void* h) { return h ? ((OracleBase*)h)->err.c_str() : g_err.c_str(); }
+OAPI void oracle_destroy(void* h) { delete (OracleBase*)h; }
+OAPI int oracle_init(void* h, uint64_t seed) { return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->init(seed); }); }
+OAPI int oracle_step(void* h, int n) { return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->step(n); }); }
+OAPI int oracle_diag(void* h, int cloud, dsmc_diag* out) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->diag(cloud, out); });
+}
+OAPI int oracle_get_state(void* h, dsmc_state_buffers* o) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->get_state(o); });
+}
+OAPI int oracle_set_state(void* h, const dsmc_state_buffers* in) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->set_state(in); });
+}
+OAPI int oracle_get_cell_starts(void* h, int32_t* st, int64_t cap, int64_t* total) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->cell_starts(st, cap, total); });
+}
+OAPI int oracle_get_sigvrmax(void* h, void* out, int64_t cap) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->get_sigvrmax(out, cap); });
+}
+OAPI int oracle_set_sigvrmax(void* h, const void* in, int64_t n) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->set_sigvrmax(in, n); });
+}
+OAPI int oracle_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+OAPI void oracle_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+OAPI int oracle_preset(int which, dsmc_params* run, dsmc_cloud_params* c) { return (int)fill_preset(which, run, c); }
+
+// ---- primitives for unit tests ------------------------------------------------------------
+OAPI void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    u32x4 c{ctr[0], ctr[1], ctr[2], ctr[3]};
+    u32x4 r = philox4x32_10(c, key[0], key[1]);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
+}
+// which: 0 sin, 1 cos, 2 log, 3 exp
+OAPI void oracle_math_f(int which, const float* x, float* y, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        float s, c;
+        switch (which) {
+        case 0: xsincos(x[i], &s, &c); y[i] = s; break;
+        case 1: xsincos(x[i], &s, &c); y[i] = c; break;
+        case 2: y[i] = xlog(x[i]); break;
+        default: y[i] = xexp(x[i]); break;
+        }
+    }
+}
+OAPI void oracle_math_d(int which, const double* x, double* y, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        double s, c;
+        switch (which) {
+        case 0: xsincos(x[i], &s, &c); y[i] = s; break;
+        case 1: xsincos(x[i], &s, &c); y[i] = c; break;
+        case 2: y[i] = xlog(x[i]); break;
+        default: y[i] = xexp(x[i]); break;
+        }
+    }
+}
+// trap field at n points for one cloud: out[7i..] = B^x, B^y, B^z, |B|, dB/dx, dB/dy, dB/dz
+OAPI int oracle_field_d(const dsmc_params* run, const dsmc_cloud_params* c, const double* xyz, double* out, int64_t n) {
+    CloudPhys<double> P;
+    make_cloud_phys<double>(*run, *c, 0, 0, P);
+    for (int64_t i = 0; i < n; ++i) {
+        Field<double> f;
+        trap_field(P, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], f);
+        double* o = out + 7 * i;
+        o[0] = f.bx; o[1] = f.by; o[2] = f.bz; o[3] = f.absB; o[4] = f.gx; o[5] = f.gy; o[6] = f.gz;
+    }
+    return 0;
+}

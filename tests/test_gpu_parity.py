@@ -1,0 +1,243 @@
+"""GPU engine vs CPU oracle on the same seeded inputs, through the C ABI.
+
+The engine and the oracle share the IEEE-exact per-atom arithmetic, so the bar is bit
+equality of the whole state (positions, velocities, spinors, atom ids), of the cell
+bookkeeping (cell starts = sorted order), of (sigma v_r)max and of the exact fixed-point
+diagnostics, in FP32 and in FP64.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cudadsmc_b200 import (FP32, FP64, F_COLLIDE, F_KNIFE, F_KNIFE_FIXED_T, F_LARMOR, F_MAJORANA,
+                           F_NORMALISE, TRAP_BOX, TRAP_IOFFE_PRITCHARD, INIT_THERMAL, Simulation, preset)
+from cudadsmc_b200.engine import DSMCError
+
+pytestmark = pytest.mark.gpu
+
+ALL = F_COLLIDE | F_LARMOR | F_NORMALISE | F_MAJORANA | F_KNIFE
+
+
+def scaled(which, n=None, cells=None, precision=None, flags=None, **kw):
+    run, c = preset(which)
+    if precision is not None:
+        run.precision = precision
+    if n is not None:
+        c.n_atoms = n
+        c.capacity = n
+    if cells is not None:
+        c.cells[0] = c.cells[1] = c.cells[2] = cells
+    if flags is not None:
+        c.flags = flags
+    for k, v in kw.items():
+        if hasattr(run, k):
+            setattr(run, k, v)
+        else:
+            setattr(c, k, v)
+    return run, c
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def assert_same(sim, orc, diag=True):
+    g, o = sim.get_state(), orc.get_state()
+    assert list(g["cloud_counts"]) == list(o["cloud_counts"])
+    for key in ("pos", "vel", "psi"):
+        assert g[key].shape == o[key].shape, key
+        bad = np.nonzero(np.any(bits(g[key]) != bits(o[key]), axis=1))[0]
+        assert bad.size == 0, f"{key}: {bad.size} atoms differ, first {bad[:5]}: {g[key][bad[:2]]} vs {o[key][bad[:2]]}"
+    np.testing.assert_array_equal(sim.cell_starts(), orc.cell_starts())
+    np.testing.assert_array_equal(bits(sim.sigvrmax()), bits(orc.sigvrmax()))
+    if diag:
+        dg, do = sim.diagnostics(), orc.diagnostics()
+        for k in ("step", "n_alive", "sum_v2", "sum_absB", "n_evaporated", "n_majorana", "n_knife", "collisions",
+                  "candidates", "e_kin", "e_pot", "e_evaporated", "temperature"):
+            assert dg[k] == do[k], (k, dg[k], do[k])
+        assert dg["error"] == 0
+
+
+def run_pair(run, clouds, steps, check_every=None, seed=1234):
+    sim = Simulation(run, clouds)
+    orc = oracle.Oracle(run, clouds)
+    sim.init_cloud(seed)
+    orc.init_cloud(seed)
+    assert_same(sim, orc)
+    done = 0
+    for s in (check_every or [steps]):
+        sim.step(s)
+        orc.step(s)
+        done += s
+        assert_same(sim, orc)
+    return sim, orc
+
+
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_init_bit_exact(precision):
+    run, c = scaled(0, n=30000, precision=precision)
+    sim = Simulation(run, c)
+    orc = oracle.Oracle(run, c)
+    sim.init_cloud(99)
+    orc.init_cloud(99)
+    assert_same(sim, orc)
+    st = sim.get_state()
+    ids = st["pos"][:, 3].view(np.uint32 if precision == FP32 else np.uint64).astype(np.int64)
+    assert np.array_equal(np.sort(ids), np.arange(30000))
+
+
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_small_trap_steps_bit_exact(precision):
+    # the small trapped configuration (1e4 atoms, 50^3 cells, alpha = 300), 120 steps
+    run, c = scaled(0, precision=precision)
+    run_pair(run, c, 120, check_every=[1, 1, 18, 100])
+
+
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_full_step_with_evaporation_bit_exact(precision):
+    # Larmor + Majorana + knife ramp; a hotter cloud and a tight knife so atoms are removed
+    run, c = scaled(2, n=60000, cells=40, precision=precision, flags=ALL, alpha=200.0)
+    c.knife_eta[0] = 4.0
+    c.knife_eta[1] = 3.0
+    c.knife_step[1] = 200
+    sim, orc = run_pair(run, c, 60, check_every=[1, 9, 50])
+    d = sim.diagnostics()
+    assert d["n_knife"] > 0 and d["collisions"] > 0
+
+
+def test_box_bit_exact():
+    run, c = scaled(1, n=120000, cells=24)
+    sim, orc = run_pair(run, c, 40, check_every=[1, 39])
+    assert sim.diagnostics()["collisions"] > 0
+
+
+def test_ioffe_pritchard_reference_trap_bit_exact():
+    # the trap of CUDADSMC/src/moveAtoms.cu:135-142 with its constants
+    # (include/deviceSystemParameters.cuh:25-27), 1 mm grid, 20 uK, rejection-sampled cloud
+    run, c = scaled(0, n=8000, precision=FP64)
+    c.trap = TRAP_IOFFE_PRITCHARD
+    c.B0, c.dBdz, c.d2Bdz2 = 0.01, 20.0, 40000.0
+    c.moment = 0.25 * 9.27400915e-24
+    for a in range(3):
+        c.grid_min[a], c.grid_max[a] = -1e-3, 1e-3
+    c.cells[0] = c.cells[1] = c.cells[2] = 20
+    c.flags = F_COLLIDE | F_LARMOR | F_NORMALISE | F_MAJORANA
+    run_pair(run, c, 30, check_every=[1, 29])
+
+
+def test_collide_every_and_odd_steps_graph_vs_plain():
+    run, c = scaled(2, n=40000, cells=32, flags=ALL, alpha=100.0, collide_every=3)
+    a = Simulation(run, c)
+    run2 = run.copy()
+    run2.use_graphs = 0
+    b = Simulation(run2, c)
+    orc = oracle.Oracle(run, c)
+    for s in (a, b, orc):
+        s.init_cloud(5)
+    for n in (1, 4, 7):
+        a.step(n)
+        b.step(n)
+        orc.step(n)
+        assert_same(a, orc)
+        assert_same(b, orc)
+
+
+def test_profiling_mode_identical():
+    run, c = scaled(2, n=30000, cells=32, flags=ALL)
+    a = Simulation(run, c)
+    orc = oracle.Oracle(run, c)
+    a.init_cloud(3)
+    orc.init_cloud(3)
+    a.set_profiling(True)
+    a.step(5)
+    orc.step(5)
+    assert_same(a, orc)
+    t = a.kernel_times()
+    assert len(t) == a.launches_per_step() == 8
+    assert all(v[1] == 5 for v in t.values())
+
+
+def test_batched_clouds_match_oracle_and_single_runs():
+    rng = np.random.default_rng(7)
+    clouds = []
+    for k in range(5):
+        run, c = scaled(2, n=int(rng.integers(500, 20000)), cells=int(rng.integers(8, 24)), flags=ALL, alpha=50.0)
+        c.dBdz = float(rng.uniform(1.5, 4.0))
+        c.temperature = float(rng.uniform(5e-6, 50e-6))
+        from cudadsmc_b200.engine import load_library  # noqa
+        # grid of +-5 thermal radii for this cloud
+        rz = 1.3806503e-23 * c.temperature / (c.moment * c.dBdz)
+        for a, r in ((0, 2 * rz), (1, 2 * rz), (2, rz)):
+            c.grid_min[a], c.grid_max[a] = -5 * r, 5 * r
+        c.stream_id = 11 + k
+        clouds.append(c)
+    clouds[2].n_atoms = clouds[2].capacity = 0  # an empty cloud
+    sim, orc = run_pair(run, clouds, 25, check_every=[1, 24])
+    batched = sim.get_state()
+    off = np.concatenate([[0], np.cumsum(batched["cloud_counts"])])
+    for k, c in enumerate(clouds):
+        single = Simulation(run, c)
+        single.init_cloud(1234)
+        single.step(25)
+        s = single.get_state()
+        for key in ("pos", "vel", "psi"):
+            assert np.array_equal(bits(s[key]), bits(batched[key][off[k]:off[k + 1]])), (k, key)
+        ds, db = single.diagnostics(), sim.diagnostics(k)
+        for f in ("n_alive", "sum_v2", "sum_absB", "collisions", "n_evaporated"):
+            assert ds[f] == db[f], (k, f)
+
+
+def test_set_state_unsorted_input():
+    run, c = scaled(2, n=30000, cells=24, flags=ALL)
+    src = Simulation(run, c)
+    src.init_cloud(21)
+    src.step(3)
+    st = src.get_state()
+    perm = np.random.default_rng(3).permutation(st["pos"].shape[0])
+    sim = Simulation(run, c)
+    orc = oracle.Oracle(run, c)
+    for s in (sim, orc):
+        s.set_state(st["pos"][perm], st["vel"][perm], st["psi"][perm], st["cloud_counts"])
+    assert_same(sim, orc, diag=False)
+    sim.step(10)
+    orc.step(10)
+    assert_same(sim, orc, diag=False)
+
+
+def test_overflow_spanning_many_tiles():
+    # a grid much smaller than the cloud: most atoms live in the overflow cell, which is split
+    # across tiles and carries its stayer count from tile to tile
+    run, c = scaled(2, n=50000, cells=8, flags=ALL, tile_atoms=256)
+    for a in range(3):
+        c.grid_min[a] *= 0.15
+        c.grid_max[a] *= 0.15
+    sim, orc = run_pair(run, c, 20, check_every=[1, 19])
+    starts = sim.cell_starts()
+    assert starts[-1] - starts[-2] > 20000
+
+
+def test_dense_cells_and_tiny_clouds():
+    # hundreds of atoms per central cell of an 8^3 grid, next to a one-atom cloud
+    run, c = scaled(2, n=12000, cells=8, flags=ALL, alpha=1.0)
+    run2, c1 = scaled(2, n=1, cells=4, flags=ALL)
+    c1.stream_id = 1
+    sim, orc = run_pair(run, [c, c1], 12, check_every=[1, 11])
+    occ = np.diff(sim.cell_starts())
+    assert occ[:-1].max() > 300
+
+
+def test_cell_too_full_fails_loudly():
+    # 4000 atoms in one cell cannot be staged by one tile: the step reports DSMC_ERR_CELL_FULL
+    run, c = scaled(2, n=4000, cells=1, flags=F_COLLIDE | F_LARMOR)
+    for a in range(3):
+        c.grid_min[a] *= 4
+        c.grid_max[a] *= 4
+    sim = Simulation(run, c)
+    sim.init_cloud(1)
+    sim.step(1)
+    with pytest.raises(DSMCError):
+        sim.synchronize()
+        d = sim.diagnostics()
+        if d["error"]:
+            raise DSMCError(5, "error bits set")
