@@ -22,6 +22,7 @@ ROOT = os.path.dirname(PKG_DIR)
 CSRC = os.path.join(PKG_DIR, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 ENGINE_SO = os.path.join(PKG_DIR, "libdsmc_b200.so")
+DRIVER_BIN = os.path.join(PKG_DIR, "dsmc_driver")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "build", "liboracle.so")
 
@@ -81,6 +82,15 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     return ENGINE_SO
 
 
+def build_driver(force: bool = False) -> str:
+    """The command-line driver (csrc/driver.cpp) linked against libdsmc_b200.so."""
+    src = os.path.join(CSRC, "driver.cpp")
+    if force or _stale(DRIVER_BIN, [src, ENGINE_SO, os.path.join(INCLUDE, "dsmc.h")]):
+        _run([_cxx(), "-O2", "-std=c++17", "-I", INCLUDE, "-o", DRIVER_BIN, src, "-L", PKG_DIR, "-ldsmc_b200",
+              "-Wl,-rpath,$ORIGIN"])
+    return DRIVER_BIN
+
+
 def build_oracle(force: bool = False) -> str:
     src = os.path.join(ORACLE_DIR, "dsmc_oracle.cpp")
     deps = [src] + [os.path.join(CSRC, h) for h in ("dsmc_physics.h", "dsmc_setup.h")] + [os.path.join(INCLUDE, "dsmc.h")]
@@ -93,6 +103,7 @@ def build_oracle(force: bool = False) -> str:
 
 def build_all(force: bool = False) -> None:
     build_engine(force)
+    build_driver(force)
     build_oracle(force)
 
 

@@ -149,7 +149,11 @@ inline dsmc_status fill_preset(int which, dsmc_params* run, dsmc_cloud_params* c
         c->n_atoms = 10000000;
         c->temperature = 50e-6;
         c->dBdz = 2.5;
-        c->flags = DSMC_F_COLLIDE | DSMC_F_LARMOR | DSMC_F_NORMALISE | DSMC_F_MAJORANA | DSMC_F_KNIFE;
+        // the knife ramps eta against the initial temperature (an absolute energy ramp): a cut
+        // that follows the running T of the just-truncated cloud moves down every step and
+        // evaporates everything
+        c->flags = DSMC_F_COLLIDE | DSMC_F_LARMOR | DSMC_F_NORMALISE | DSMC_F_MAJORANA | DSMC_F_KNIFE |
+                   DSMC_F_KNIFE_FIXED_T;
         c->knife_nknots = 2;
         c->knife_step[0] = 0; c->knife_eta[0] = 6.0;
         c->knife_step[1] = 1e5; c->knife_eta[1] = 4.0;
@@ -160,7 +164,7 @@ inline dsmc_status fill_preset(int which, dsmc_params* run, dsmc_cloud_params* c
         c->temperature = 30e-6;
         c->dBdz = 2.5;
         c->B0 = 1e-4;
-        c->flags = DSMC_F_COLLIDE | DSMC_F_LARMOR | DSMC_F_NORMALISE | DSMC_F_KNIFE;
+        c->flags = DSMC_F_COLLIDE | DSMC_F_LARMOR | DSMC_F_NORMALISE | DSMC_F_KNIFE | DSMC_F_KNIFE_FIXED_T;
         c->knife_nknots = 9;
         for (int i = 0; i < 9; ++i) {
             c->knife_step[i] = 250.0 * i;

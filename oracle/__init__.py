@@ -48,6 +48,9 @@ def load() -> C.CDLL:
             "oracle_math_d": (None, [i32, C.POINTER(C.c_double), C.POINTER(C.c_double), i64]),
             "oracle_field_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), i64]),
+            "oracle_advance_atoms_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
+                                             i64, i32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -91,6 +94,18 @@ def field(run: RunParams, cloud: CloudParams, xyz: np.ndarray) -> np.ndarray:
     load().oracle_field_d(C.byref(run), C.byref(cloud), xyz.ctypes.data_as(C.POINTER(C.c_double)),
                           out.ctypes.data_as(C.POINTER(C.c_double)), xyz.shape[0])
     return out
+
+
+def advance_atoms(run: RunParams, cloud: CloudParams, pos, vel, psi, nsteps: int):
+    """FP64 per-atom advance (Larmor, Verlet, evaporation tests) without collisions or sort."""
+    pos = np.array(pos, np.float64, order="C", copy=True)
+    vel = np.array(vel, np.float64, order="C", copy=True)
+    psi = np.array(psi, np.float64, order="C", copy=True)
+    fate = np.zeros(pos.shape[0], np.int32)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    load().oracle_advance_atoms_d(C.byref(run), C.byref(cloud), dp(pos), dp(vel), dp(psi),
+                                  fate.ctypes.data_as(C.POINTER(C.c_int32)), pos.shape[0], int(nsteps))
+    return pos, vel, psi, fate
 
 
 def max_threads() -> int:

@@ -499,3 +499,26 @@ OAPI int oracle_field_d(const dsmc_params* run, const dsmc_cloud_params* c, cons
     }
     return 0;
 }
+// advance n atoms by nsteps (Larmor + Verlet + evaporation tests, no collisions, no sort) in
+// FP64: the per-atom part of the step, for comparison with the reference's own kernels.
+// fate[i] receives the fate after the last step (0 alive, 1 Majorana, 2 knife).
+OAPI int oracle_advance_atoms_d(const dsmc_params* run, const dsmc_cloud_params* c, double* pos, double* vel,
+                                double* psi, int32_t* fate, int64_t n, int nsteps) {
+    CloudPhys<double> P;
+    make_cloud_phys<double>(*run, *c, 0, 0, P);
+    for (int64_t i = 0; i < n; ++i) {
+        Atom<double> a;
+        a.x = pos[4 * i]; a.y = pos[4 * i + 1]; a.z = pos[4 * i + 2];
+        a.vx = vel[4 * i]; a.vy = vel[4 * i + 1]; a.vz = vel[4 * i + 2];
+        a.ur = psi[4 * i]; a.ui = psi[4 * i + 1]; a.dr = psi[4 * i + 2]; a.di = psi[4 * i + 3];
+        a.flags = lane_to_u32(vel[4 * i + 3]);
+        AtomOut<double> o;
+        o.fate = FATE_ALIVE;
+        for (int s = 0; s < nsteps; ++s) advance_atom(P, 0.0, a, o);
+        pos[4 * i] = a.x; pos[4 * i + 1] = a.y; pos[4 * i + 2] = a.z;
+        vel[4 * i] = a.vx; vel[4 * i + 1] = a.vy; vel[4 * i + 2] = a.vz;
+        psi[4 * i] = a.ur; psi[4 * i + 1] = a.ui; psi[4 * i + 2] = a.dr; psi[4 * i + 3] = a.di;
+        if (fate) fate[i] = o.fate;
+    }
+    return 0;
+}

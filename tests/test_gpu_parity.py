@@ -15,7 +15,7 @@ from cudadsmc_b200.engine import DSMCError
 
 pytestmark = pytest.mark.gpu
 
-ALL = F_COLLIDE | F_LARMOR | F_NORMALISE | F_MAJORANA | F_KNIFE
+ALL = F_COLLIDE | F_LARMOR | F_NORMALISE | F_MAJORANA | F_KNIFE | F_KNIFE_FIXED_T
 
 
 def scaled(which, n=None, cells=None, precision=None, flags=None, **kw):
@@ -97,8 +97,8 @@ def test_small_trap_steps_bit_exact(precision):
 @pytest.mark.parametrize("precision", [FP32, FP64])
 def test_full_step_with_evaporation_bit_exact(precision):
     # Larmor + Majorana + knife ramp; a hotter cloud and a tight knife so atoms are removed
-    run, c = scaled(2, n=60000, cells=40, precision=precision, flags=ALL, alpha=200.0)
-    c.knife_eta[0] = 4.0
+    run, c = scaled(2, n=60000, cells=40, precision=precision, flags=ALL, alpha=4000.0)
+    c.knife_eta[0] = 6.0
     c.knife_eta[1] = 3.0
     c.knife_step[1] = 200
     sim, orc = run_pair(run, c, 60, check_every=[1, 9, 50])
@@ -126,8 +126,16 @@ def test_ioffe_pritchard_reference_trap_bit_exact():
     run_pair(run, c, 30, check_every=[1, 29])
 
 
+def test_running_temperature_knife_bit_exact():
+    # the knife of the running temperature (F_KNIFE_FIXED_T off) feeds the exact fixed-point T of
+    # each step into the next cut
+    run, c = scaled(2, n=30000, cells=32, flags=ALL & ~F_KNIFE_FIXED_T, alpha=4000.0)
+    c.knife_eta[0] = c.knife_eta[1] = 7.0
+    run_pair(run, c, 20, check_every=[1, 19])
+
+
 def test_collide_every_and_odd_steps_graph_vs_plain():
-    run, c = scaled(2, n=40000, cells=32, flags=ALL, alpha=100.0, collide_every=3)
+    run, c = scaled(2, n=40000, cells=32, flags=ALL, alpha=4000.0, collide_every=3)
     a = Simulation(run, c)
     run2 = run.copy()
     run2.use_graphs = 0
@@ -162,7 +170,7 @@ def test_batched_clouds_match_oracle_and_single_runs():
     rng = np.random.default_rng(7)
     clouds = []
     for k in range(5):
-        run, c = scaled(2, n=int(rng.integers(500, 20000)), cells=int(rng.integers(8, 24)), flags=ALL, alpha=50.0)
+        run, c = scaled(2, n=int(rng.integers(500, 20000)), cells=int(rng.integers(8, 24)), flags=ALL, alpha=2000.0)
         c.dBdz = float(rng.uniform(1.5, 4.0))
         c.temperature = float(rng.uniform(5e-6, 50e-6))
         from cudadsmc_b200.engine import load_library  # noqa
