@@ -350,6 +350,8 @@ template <class R> struct CloudPhys {
     R v_init;                     // sqrt(kB T0 / m)
     R r0_init;                    // kB T0 / mu  (quadrupole thermal length)
     R inv_kT_over_mu;             // mu / (kB T0) for rejection sampling
+    R prop_min_x, prop_min_y, prop_min_z;  // proposal box of the rejection sampler
+    R prop_len_x, prop_len_y, prop_len_z;
     int32_t knife_nknots;
     int32_t pad0;
     double knife_step[9];
@@ -604,8 +606,9 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
 // Initial state of one atom (generateInitialDist, setUp.cu:129-165, with an exact sampler):
 //   quadrupole: scaled radius rho = sqrt(x^2/4+y^2/4+z^2) has density ~ rho^2 exp(-rho/r0),
 //     i.e. Gamma(3, r0): rho = -r0 log(u1 u2 u3); direction isotropic in (x/2, y/2, z);
-//   Ioffe-Pritchard: bounded rejection sampling, uniform proposal over the grid box,
-//     acceptance exp(-mu (|B| - B_floor) / kT);
+//   Ioffe-Pritchard: bounded rejection sampling, uniform proposal over a box of +-7 thermal
+//     widths of the harmonic approximation (clipped to the grid box), acceptance
+//     exp(-mu (|B| - B_floor) / kT);
 //   box: uniform over the grid box.
 // Velocities: Maxwellian N(0, kT/m) per axis by Box-Muller.  Spinor aligned with B^
 // (the +1 eigenvector of s.B^, without the rsqrt(1 + B^x) singularity of setUp.cu:240).
@@ -644,9 +647,9 @@ DSMC_HD bool init_atom(const CloudPhys<R>& P, int init_mode, uint32_t local_id, 
         for (uint32_t t = 0; t < 4096u; ++t) {
             u32x4 w = draw(local_id, t, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 0u, seed);
             u32x4 w2 = draw(local_id, t, PURPOSE_INIT_POS, (uint32_t)P.cloud_id, 1u, seed);
-            R x = P.gmin_x + P.box_x * u01<R>(w.x, w2.x);
-            R y = P.gmin_y + P.box_y * u01<R>(w.y, w2.y);
-            R z = P.gmin_z + P.box_z * u01<R>(w.z, w2.z);
+            R x = P.prop_min_x + P.prop_len_x * u01<R>(w.x, w2.x);
+            R y = P.prop_min_y + P.prop_len_y * u01<R>(w.y, w2.y);
+            R z = P.prop_min_z + P.prop_len_z * u01<R>(w.z, w2.z);
             Field<R> f;
             trap_field(P, x, y, z, f);
             R pr = xexp(-(P.inv_kT_over_mu * (f.absB - P.B_floor)));

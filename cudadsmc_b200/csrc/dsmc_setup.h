@@ -4,6 +4,7 @@
 #ifndef DSMC_SETUP_H
 #define DSMC_SETUP_H
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -76,6 +77,42 @@ inline void make_cloud_phys(const dsmc_params& run, const dsmc_cloud_params& c, 
     P.v_init = (R)std::sqrt(kB * c.temperature / c.mass);
     P.r0_init = (R)((c.moment > 0 && c.dBdz != 0) ? kB * c.temperature / (c.moment * std::fabs(c.dBdz)) : 0.0);
     P.inv_kT_over_mu = (R)(c.moment / (kB * c.temperature));
+    // proposal box of the rejection sampler: along each axis, 1.25 x the distance at which
+    // mu (|B| - B_floor) reaches 40 kB T (bisection on the field), clipped to the grid box; the
+    // Boltzmann weight left outside is below exp(-40)
+    {
+        double lo[3] = {c.grid_min[0], c.grid_min[1], c.grid_min[2]};
+        double hi[3] = {c.grid_max[0], c.grid_max[1], c.grid_max[2]};
+        if (c.trap == DSMC_TRAP_IOFFE_PRITCHARD && c.moment > 0) {
+            CloudPhys<double> Q;
+            memset(&Q, 0, sizeof(Q));
+            Q.trap = TRAP_IOFFE_PRITCHARD;
+            Q.Bp = c.dBdz; Q.Bpp = c.d2Bdz2; Q.B0 = c.B0;
+            const double target = 40.0 * kB * c.temperature / c.moment + std::fabs(c.B0);
+            for (int axis = 0; axis < 3; ++axis) {
+                for (int side = -1; side <= 1; side += 2) {
+                    const double lim = side < 0 ? -c.grid_min[axis] : c.grid_max[axis];
+                    if (!(lim > 0)) continue;
+                    double a0 = 0.0, a1 = lim;
+                    double pt[3] = {0, 0, 0};
+                    pt[axis] = side * a1;
+                    Field<double> f;
+                    trap_field(Q, pt[0], pt[1], pt[2], f);
+                    if (f.absB < target) continue;  // the grid box is the bound
+                    for (int it = 0; it < 200; ++it) {
+                        const double m = 0.5 * (a0 + a1);
+                        pt[axis] = side * m;
+                        trap_field(Q, pt[0], pt[1], pt[2], f);
+                        if (f.absB < target) a0 = m; else a1 = m;
+                    }
+                    const double w = std::min(1.25 * a1, lim);
+                    if (side < 0) lo[axis] = -w; else hi[axis] = w;
+                }
+            }
+        }
+        P.prop_min_x = (R)lo[0]; P.prop_min_y = (R)lo[1]; P.prop_min_z = (R)lo[2];
+        P.prop_len_x = (R)(hi[0] - lo[0]); P.prop_len_y = (R)(hi[1] - lo[1]); P.prop_len_z = (R)(hi[2] - lo[2]);
+    }
     P.knife_nknots = c.knife_nknots;
     for (int i = 0; i < DSMC_MAX_KNOTS; ++i) {
         P.knife_step[i] = c.knife_step[i];

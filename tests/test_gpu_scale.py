@@ -1,0 +1,65 @@
+"""The engine at the benchmark size (1e7 atoms, 128^3 cells): size-independent properties, and
+the drift of the FP32 engine's diagnostics against an FP64 run of the same cloud."""
+import numpy as np
+import pytest
+
+from cudadsmc_b200 import FP64, Simulation, preset
+
+pytestmark = pytest.mark.gpu
+
+
+def test_full_size_invariants():
+    run, c = preset(2)
+    sim = Simulation(run, c)
+    sim.init_cloud(1234)
+    d0 = sim.diagnostics()
+    sim.step(30)
+    d = sim.diagnostics()
+    assert d["error"] == 0
+    # atom accounting and energy accounting (what stays plus what was evaporated)
+    assert d["n_alive"] + d["n_evaporated"] == c.n_atoms
+    e0 = d0["e_kin"] + d0["e_pot"]
+    e1 = d["e_kin"] + d["e_pot"] + d["e_evaporated"]
+    assert abs(e1 - e0) / e0 < 1e-4
+    assert d["atom_steps"] > 0 and d["collisions"] > 0
+    st = sim.get_state()
+    pos = st["pos"]
+    ids = pos[:, 3].view(np.uint32)
+    assert ids.size == d["n_alive"] and np.unique(ids).size == ids.size
+    # the order is sorted by cell: recompute every cell in float32 with the engine's formula
+    lo = np.array([c.grid_min[a] for a in range(3)], np.float32)
+    inv = np.array([np.float32(1.0 / ((c.grid_max[a] - c.grid_min[a]) / c.cells[a])) for a in range(3)], np.float32)
+    f = (pos[:, :3] - lo) * inv
+    n = np.array(c.cells)
+    inside = np.all((f >= 0) & (f < n), axis=1)
+    idx = np.floor(np.where(inside[:, None], f, 0)).astype(np.int64)
+    cell = np.where(inside, (idx[:, 2] * n[1] + idx[:, 1]) * n[0] + idx[:, 0], n.prod())
+    assert np.all(np.diff(cell) >= 0)
+    starts = sim.cell_starts()
+    assert np.array_equal(np.bincount(cell, minlength=n.prod() + 1), np.diff(starts))
+
+
+def test_fp32_drift_against_fp64():
+    # the same 1e6-atom cloud (FP64 initial state, rounded to FP32) advanced 200 steps in both
+    run, c = preset(2)
+    c.n_atoms = c.capacity = 1_000_000
+    run64 = run.copy()
+    run64.precision = FP64
+    s64 = Simulation(run64, c)
+    s64.init_cloud(77)
+    st = s64.get_state()
+    s32 = Simulation(run, c)
+
+    def lanes32(a):
+        out = a.astype(np.float32)
+        out[:, 3] = a[:, 3].view(np.uint64).astype(np.uint32).view(np.float32)  # id / flag bits
+        return out
+
+    s32.set_state(lanes32(st["pos"]), lanes32(st["vel"]), st["psi"].astype(np.float32), st["cloud_counts"])
+    s64.step(200)
+    s32.step(200)
+    a, b = s32.diagnostics(), s64.diagnostics()
+    rel = {k: abs(a[k] - b[k]) / abs(b[k]) for k in ("n_alive", "temperature", "e_kin", "e_pot", "e_evaporated")}
+    print("FP32 vs FP64 relative drift after 200 steps:", rel,
+          "collisions", a["collisions"], b["collisions"])
+    assert rel["n_alive"] < 1e-3 and rel["temperature"] < 1e-3 and rel["e_kin"] < 2e-3
