@@ -200,27 +200,29 @@ def main():
     kt = sim.kernel_times()
     sim.set_profiling(False)
     n_now = sim.diagnostics()["n_alive"]
-    commit_ms = kt["tile_pass_commit"][0] / kt["tile_pass_commit"][1]
-    plan_ms = kt["tile_pass_plan"][0] / kt["tile_pass_plan"][1]
-    bytes_atom_commit = 96  # read pos, vel, psi (48 B) + write them at the sorted slot (48 B)
-    bytes_atom_plan = 48
+    step_ms = kt["step_pass"][0] / kt["step_pass"][1]
+    perm_ms = kt["permute_pass"][0] / kt["permute_pass"][1]
+    # step_pass: gather pos, vel, psi (48 B) through src (4 B), write them back (48 B) with an
+    # 8-byte sort key; permute_pass: read the key (8 B), write the next permutation (4 B)
+    bytes_atom_step = 48 + 4 + 48 + 8
+    bytes_atom_perm = 8 + 4
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         with open(peaks_path) as f:
             peak = float(json.load(f)["hbm_gbs"])
         peak_src = "measured"
-    achieved = bytes_atom_commit * n_now / (commit_ms * 1e-3) / 1e9
+    achieved = bytes_atom_step * n_now / (step_ms * 1e-3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "tile_pass_commit_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "step_pass_traffic.json")
     if os.path.exists(prof):
         with open(prof) as f:
             traffic = float(json.load(f)["dram_bytes_per_atom"]) * n_now
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "tile_pass_commit", "peak_source": peak_src,
-                "algorithmic_bytes_per_atom": bytes_atom_commit,
+                "traffic": traffic, "kernel": "step_pass", "peak_source": peak_src,
+                "algorithmic_bytes_per_atom": bytes_atom_step,
                 "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()},
-                "plan_pass_frac": bytes_atom_plan * n_now / (plan_ms * 1e-3) / 1e9 / peak}
+                "permute_pass_frac": bytes_atom_perm * n_now / (perm_ms * 1e-3) / 1e9 / peak}
 
     # ------------------------------------------------------------------ end to end, host buffers
     e2e = None

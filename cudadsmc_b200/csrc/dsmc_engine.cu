@@ -47,8 +47,8 @@ template <class T> struct DevBuf {
     ~DevBuf() { free(); }
 };
 
-const char* kKernelNames[] = {"tile_pass_plan", "scan_reduce", "scan_top",  "scan_down",
-                              "mover_place",    "mover_rank",  "tile_pass_commit", "finalize"};
+const char* kKernelNames[] = {"step_pass",   "scan_reduce", "scan_top",     "scan_down",
+                              "mover_place", "mover_rank",  "permute_pass", "finalize"};
 constexpr int kNumStepKernels = 8;
 
 }  // namespace
@@ -89,8 +89,10 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
     // device memory
     DevBuf<R4> pos[2], vel[2], psi[2];
     DevBuf<int> start[2], tile_begin[2], tile_cloud[2];
-    DevBuf<int> Lc, Ic, mover_base, in_list, tile_movers, tile_ovf, tile_ovf_carry;
+    DevBuf<int> src[2];
+    DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry;
     DevBuf<int4> mrec;
+    DevBuf<int2> keys;
     DevBuf<R> sigvrmax;
     DevBuf<TilePartial> partials;
     DevBuf<CloudPhys<R>> d_phys;
@@ -126,10 +128,8 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
-        smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int));
-        CU(cudaFuncSetAttribute(tile_pass<R, BLOCK, CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_tile));
-        CU(cudaFuncSetAttribute(tile_pass<R, BLOCK, CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        smem_tile = (size_t)CAP * (sizeof(R4) + 2 * sizeof(int));
+        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         build_args();
     }
@@ -168,6 +168,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
     void allocate() {
         for (int i = 0; i < 2; ++i) {
             pos[i].alloc(capacity); vel[i].alloc(capacity); psi[i].alloc(capacity);
+            src[i].alloc(capacity);
             start[i].alloc(total_cells + 1);
             tile_begin[i].alloc(max_tiles + 1);
             tile_cloud[i].alloc(max_tiles);
@@ -180,7 +181,8 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         CU(cudaMemset(Ic.p, 0, total_cells * sizeof(int)));
         in_list.alloc(capacity);
         mrec.alloc(capacity);
-        tile_movers.alloc(max_tiles); tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles);
+        keys.alloc(capacity);
+        tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles);
         sigvrmax.alloc(total_cells);
         partials.alloc(max_tiles);
         d_phys.alloc(nclouds);
@@ -214,13 +216,14 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
             const int q = 1 - p;
             A.pos_in = pos[p].p; A.vel_in = vel[p].p; A.psi_in = psi[p].p;
             A.pos_out = pos[q].p; A.vel_out = vel[q].p; A.psi_out = psi[q].p;
+            A.src_in = src[p].p; A.src_out = src[q].p; A.keys = keys.p;
             A.old_start = start[p].p; A.new_start = start[q].p;
             A.Lc = Lc.p; A.Ic = Ic.p; A.mover_base = mover_base.p;
             A.sigvrmax = sigvrmax.p;
             A.mrec = mrec.p; A.in_list = in_list.p;
             A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p;
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
-            A.tile_movers = tile_movers.p; A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
+            A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
             A.partials = partials.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.block_sums = block_sums.p; A.block_off = block_off.p;
@@ -237,17 +240,13 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0:
-            tile_pass<R, BLOCK, CAP, false><<<max_tiles, BLOCK, smem_tile, stream>>>(A);
-            break;
+        case 0: step_pass<R, BLOCK, CAP><<<max_tiles, BLOCK, smem_tile, stream>>>(A); break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
         case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
-        case 4: mover_place<R><<<max_tiles, 256, 0, stream>>>(A); break;
-        case 5: mover_rank<R><<<max_tiles, 256, 0, stream>>>(A); break;
-        case 6:
-            tile_pass<R, BLOCK, CAP, true><<<max_tiles, BLOCK, smem_tile, stream>>>(A);
-            break;
+        case 4: mover_place<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 5: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 6: permute_pass<R, 256, CAP><<<max_tiles, 256, 0, stream>>>(A); break;
         case 7: finalize<R, false><<<nclouds, 256, 0, stream>>>(A); break;
         }
     }
@@ -361,6 +360,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         if (n > 0) {
             fs_place<R><<<ab, 256, 0, stream>>>(S, A);
             fs_scatter<R><<<ab, 256, 0, stream>>>(S, A);
+            fill_identity<<<ab, 256, 0, stream>>>(src[0].p, n);
         }
         CU(cudaGetLastError());
         parity = 0;
@@ -484,9 +484,15 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         if (o->n < n) throw Fail{DSMC_ERR_INVALID, "state buffers too small: need " + std::to_string(n)};
         std::vector<CloudDyn> d(nclouds);
         CU(cudaMemcpy(d.data(), cdyn.p, nclouds * sizeof(CloudDyn), cudaMemcpyDeviceToHost));
-        if (o->pos) CU(cudaMemcpyAsync(o->pos, pos[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
-        if (o->vel) CU(cudaMemcpyAsync(o->vel, vel[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
-        if (o->psi) CU(cudaMemcpyAsync(o->psi, psi[parity].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        // the state is stored in the order of the previous step; gather it into sorted order in
+        // the other buffer set (free between steps) and copy that
+        const int q = 1 - parity;
+        if (n > 0)
+            materialize<R><<<(n + 255) / 256, 256, 0, stream>>>(args[parity], n, pos[q].p, vel[q].p, psi[q].p);
+        CU(cudaGetLastError());
+        if (o->pos) CU(cudaMemcpyAsync(o->pos, pos[q].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        if (o->vel) CU(cudaMemcpyAsync(o->vel, vel[q].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
+        if (o->psi) CU(cudaMemcpyAsync(o->psi, psi[q].p, (size_t)n * sizeof(R4), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
         o->n = n;
         if (o->cloud_counts)

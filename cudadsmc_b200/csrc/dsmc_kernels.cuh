@@ -2,23 +2,27 @@
 //
 // Data layout in HBM (per precision R = float | double, R4 = float4 | double4):
 //   pos[i] = (x, y, z, atom id bits)   vel[i] = (vx, vy, vz, flag bits)   psi[i] = (u_re, u_im, d_re, d_im)
-//   three structure-of-arrays streams of 16 B (FP32) per atom, double-buffered; atoms are kept
-//   sorted by global cell (clouds one after another, each cloud's grid cells then its overflow
-//   cell), so every cell is a contiguous range and start[c] gives its first atom.
+//   three structure-of-arrays streams of 16 B (FP32) per atom, double-buffered, plus a
+//   permutation src[] (4 B per atom): the atom in sorted position j is stored at src[j].  The
+//   sorted order groups atoms by global cell (clouds one after another, each cloud's grid cells
+//   then its overflow cell), so every cell is a contiguous range [start[c], start[c+1]) of j.
 //
-// One step = 8 launches, all sized statically so the sequence can be captured in a CUDA graph:
-//   tile_pass<PLAN>   per tile: collide its cells, move every atom, classify stayer/mover/lost,
-//                     count leavers L[c] and incoming movers I[c], record movers
-//   scan_reduce/top/down   new per-cell counts n_c - L_c + I_c -> new start[], next tiling,
-//                     mover base per cell, overflow carries
-//   mover_place / mover_rank   deterministic rank of incoming movers by their old index
-//   tile_pass<COMMIT> recompute the identical step, write every surviving atom at its sorted
-//                     destination, per-tile exact diagnostics
-//   finalize          per-cloud diagnostics, knife temperature, step counter
-// The sort is stable by (new cell, moved?, old index): in each new cell the atoms that stayed
-// keep their previous order and are followed by the atoms that entered it, by old index.
-// Tiles are contiguous, cloud-pure atom ranges of ~T atoms whose boundaries snap to cell starts
-// (the overflow cell, which never collides, is split at nominal boundaries).
+// One step = 8 launches with static grids, captured in a CUDA graph:
+//   step_pass        per tile of ~T sorted positions: gather the atoms through src, collide the
+//                    tile's cells in shared memory, then move + spin + evaporate every atom once,
+//                    write the new state at its current position j (coalesced) with an 8-byte
+//                    sort key, count leavers L[c] / incoming movers I[c], list movers, and reduce
+//                    exact diagnostics.  The only heavy pass: the step is computed once.
+//   scan_reduce/top/down   per-cell counts n_c - L_c + I_c -> new start[], next tiling, movers'
+//                    base slot, overflow prefix over tiles
+//   mover_place/rank deterministic rank of each incoming mover by its old position
+//   permute_pass     per tile: rank the stayers inside their old cell and write the next
+//                    permutation src'[dest] = j (4 B per atom instead of moving 48 B)
+//   finalize         per-cloud diagnostics, knife temperature, step counter
+// The new order is the stable sort by (new cell, moved?, old position): in each new cell the atoms
+// that stayed keep their order, followed by the atoms that entered it, by old position.  Tiles are
+// contiguous, cloud-pure ranges of sorted positions whose boundaries snap to cell starts (the
+// overflow cell, which never collides, is split at nominal boundaries).
 #ifndef DSMC_KERNELS_CUH
 #define DSMC_KERNELS_CUH
 
@@ -37,8 +41,11 @@ enum : int {
     EB_CAPACITY = 4,
     EB_INIT_REJECT = 8,
     EB_TILE_OVERFLOW = 16,
-    EB_INCONSISTENT = 32
+    EB_INCONSISTENT = 32,
+    EB_TIMEOUT = 64
 };
+
+constexpr int MOVER_GRID = 148 * 8;  // grid-stride kernels over the mover list
 
 struct __align__(16) TilePartial {
     i128 sum_v2, sum_B, evap_v2, evap_B;
@@ -64,8 +71,11 @@ struct Ctl {
     int ntiles[2];
     int step[2];
     int err;
-    int pad;
+    int movers;  // movers listed by the current step (reset by finalize)
 };
+
+// sort keys written by step_pass for every current position j
+enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2 };
 
 template <class R> struct Args {
     typedef typename V4T<R>::type R4;
@@ -75,6 +85,9 @@ template <class R> struct Args {
     R4* pos_out;
     R4* vel_out;
     R4* psi_out;
+    const int* src_in;   // sorted position -> storage index of the current state
+    int* src_out;        // the same for the state this step writes
+    int2* keys;          // per current position: sort key written by step_pass
     const int* old_start;
     int* new_start;
     int* Lc;
@@ -87,7 +100,6 @@ template <class R> struct Args {
     const int* tile_cloud;
     int* tile_begin_next;
     int* tile_cloud_next;
-    int* tile_movers;
     int* tile_ovf;
     int* tile_ovf_carry;
     TilePartial* partials;
@@ -208,21 +220,18 @@ __device__ __forceinline__ R knife_cut_for(const CloudPhys<R>& P, double T, int 
 }
 
 // ---------------------------------------------------------------------------------------------
-// tile_pass: the fused collide + move + classify kernel, run twice per step.
-//   COMMIT = false (plan):   leaver / mover counts, mover records, overflow stayers per tile
-//   COMMIT = true  (commit): the same arithmetic again, then scatter + diagnostics
-// Shared memory per tile: pos, vel (R4 each), old cell (int), packed prefix (uint32) x CAP atoms.
+// step_pass: the timestep of one tile.
+// Shared memory per tile: velocities (R4, the collide works on them in place), old cell and
+// storage index of each position, CAP positions.
 // ---------------------------------------------------------------------------------------------
-template <class R, int BLOCK, int CAP, bool COMMIT>
-__global__ void __launch_bounds__(BLOCK) tile_pass(Args<R> A) {
+template <class R, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
     typedef typename V4T<R>::type R4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R4* s_pos = reinterpret_cast<R4*>(smem_raw);
-    R4* s_vel = s_pos + CAP;
+    R4* s_vel = reinterpret_cast<R4*>(smem_raw);
     int* s_cell = reinterpret_cast<int*>(s_vel + CAP);
-    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_cell + CAP);
+    int* s_src = s_cell + CAP;
     __shared__ CloudPhys<R> P;
-    __shared__ uint32_t wsum[32];
     __shared__ TilePartial red[BLOCK / 32];
 
     const int p = A.parity;
@@ -232,34 +241,44 @@ __global__ void __launch_bounds__(BLOCK) tile_pass(Args<R> A) {
     const int te = A.tile_begin[b + 1];
     const int L = te - tb;
     const int cloud = A.tile_cloud[b];
-    if (L > CAP || L < 0) {
-        // cannot stage this tile: flag it and leave a consistent, empty contribution so that
-        // every later kernel only touches indices it computed itself
+    const int nprev = A.ctl->n[p];
+    const int lane = threadIdx.x & 31;
+    load_cloud(P, A.clouds + cloud);
+    __syncthreads();
+    const bool box = (P.trap == TRAP_BOX);
+
+    if (L > CAP || L < 0 || te > nprev) {
+        // cannot stage this tile: every atom in it leaves the simulation (flagged), so the cell
+        // counts stay consistent and every later kernel only touches indices it computed itself
+        if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_CELL_FULL);
+        for (int t = threadIdx.x; t < L && tb + t < nprev; t += BLOCK) {
+            int s = A.src_in[tb + t];
+            s = (s >= 0 && s < nprev) ? s : 0;
+            const R4 q = A.pos_in[s];
+            atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
+            A.keys[tb + t] = make_int2(-1, KIND_LOST);
+        }
         if (threadIdx.x == 0) {
-            atomicOr(&A.ctl->err, EB_CELL_FULL);
-            if (!COMMIT) {
-                A.tile_movers[b] = 0;
-                A.tile_ovf[b] = 0;
-            } else {
-                TilePartial z;
-                zero_partial(z);
-                A.partials[b] = z;
-            }
+            TilePartial z;
+            zero_partial(z);
+            A.partials[b] = z;
+            A.tile_ovf[b] = 0;
         }
         return;
     }
-    load_cloud(P, A.clouds + cloud);
     const int step = A.ctl->step[p];
-    __syncthreads();
-    const bool box = (P.trap == TRAP_BOX);
     const R cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
 
-    // phase 1: stage the tile's positions and velocities, old cells
+    // phase 1: gather the tile's velocities into shared memory, old cell of every atom
     for (int t = threadIdx.x; t < L; t += BLOCK) {
-        R4 q = A.pos_in[tb + t];
-        R4 v = A.vel_in[tb + t];
-        s_pos[t] = q;
-        s_vel[t] = v;
+        int s = A.src_in[tb + t];
+        if (s < 0 || s >= nprev) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            s = 0;
+        }
+        const R4 q = A.pos_in[s];
+        s_src[t] = s;
+        s_vel[t] = A.vel_in[s];
         s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
     }
     __syncthreads();
@@ -280,34 +299,34 @@ __global__ void __launch_bounds__(BLOCK) tile_pass(Args<R> A) {
             R svm = A.sigvrmax[c];
             CollideResult<R> cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
                                                       (uint32_t)step, A.seed);
-            if (COMMIT) {
-                A.sigvrmax[c] = svm;
-                my_coll += cr.accepted;
-                my_cand += cr.candidates;
-            }
+            A.sigvrmax[c] = svm;
+            my_coll += cr.accepted;
+            my_cand += cr.candidates;
         }
         __syncthreads();
     }
 
-    // phase 3: move + classify, in chunks of BLOCK atoms with a running packed prefix
+    // phase 3: move, spin, evaporate and classify every atom once
     TilePartial acc;
     zero_partial(acc);
     acc.coll = my_coll;
     acc.cand = my_cand;
-    uint32_t carry = 0;
-    const int lane = threadIdx.x & 31;
+    long long ovf_stayers = 0;
     for (int base = 0; base < L; base += BLOCK) {
         const int t = base + threadIdx.x;
         const bool valid = t < L;
         Atom<R> a;
         AtomOut<R> o;
+        o.fate = FATE_ALIVE;
+        o.cell = 0;
         bool stayer = false, mover = false;
         int c_old = 0;
         R4 q, v, s;
         if (valid) {
-            q = s_pos[t];
+            const int sidx = s_src[t];
+            q = A.pos_in[sidx];
+            s = A.psi_in[sidx];
             v = s_vel[t];
-            s = A.psi_in[tb + t];
             a.x = q.x; a.y = q.y; a.z = q.z;
             a.vx = v.x; a.vy = v.y; a.vz = v.z;
             a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
@@ -319,83 +338,117 @@ __global__ void __launch_bounds__(BLOCK) tile_pass(Args<R> A) {
             mover = alive && !stayer;
             if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
         }
-        uint32_t tot;
-        uint32_t ex = block_excl_scan_u32<BLOCK>(((uint32_t)stayer << 16) | (uint32_t)mover, wsum, tot);
-        ex += carry;
-        carry += tot;
-        if (valid) s_pre[t] = ex;
-        __syncthreads();
-        if (!COMMIT) {
-            const bool leaver = valid && !stayer;
-            const unsigned lm = __ballot_sync(0xffffffffu, leaver);
-            if (leaver) {
-                const unsigned peers = __match_any_sync(lm, c_old);
-                if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
-            }
-            const unsigned mm = __ballot_sync(0xffffffffu, mover);
-            if (mover) {
-                const unsigned peers = __match_any_sync(mm, o.cell);
-                const int leader = __ffs(peers) - 1;
-                int base_ticket = 0;
-                if (lane == leader) base_ticket = atomicAdd(&A.Ic[o.cell], __popc(peers));
-                base_ticket = __shfl_sync(peers, base_ticket, leader);
-                const int ticket = base_ticket + __popc(peers & ((1u << lane) - 1u));
-                A.mrec[tb + (int)(ex & 0xFFFFu)] = make_int4(o.cell, tb + t, ticket, 0);
-            }
-        } else if (valid) {
-            int dest = -1;
-            if (stayer) {
-                const int seg = A.old_start[c_old];
-                const int sl = seg > tb ? seg - tb : 0;
-                if (sl <= t) {
-                    int rank = (int)(ex >> 16) - (int)(s_pre[sl] >> 16);
-                    if (seg < tb)
-                        rank += A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
-                    dest = A.new_start[c_old] + rank;
-                    if (dest < A.new_start[c_old] || dest >= A.new_start[c_old + 1]) dest = -2;
-                } else {
-                    dest = -2;
-                }
-            } else if (mover) {
-                dest = A.mrec[tb + (int)(ex & 0xFFFFu)].w;
-                if (dest < 0 || dest >= A.capacity) dest = -2;
-            }
-            if (dest == -2) {
-                atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            } else if (dest >= 0) {
+        // leavers of the old cell (movers and lost atoms), warp-aggregated
+        const bool leaver = valid && !stayer;
+        const unsigned lm = __ballot_sync(0xffffffffu, leaver);
+        if (leaver) {
+            const unsigned peers = __match_any_sync(lm, c_old);
+            if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
+        }
+        // movers: a slot in the step's mover list and a ticket in the target cell
+        const unsigned mm = __ballot_sync(0xffffffffu, mover);
+        int slot = 0;
+        if (mm) {
+            const int leader = __ffs(mm) - 1;
+            int sbase = 0;
+            if (lane == leader) sbase = atomicAdd(&A.ctl->movers, __popc(mm));
+            sbase = __shfl_sync(0xffffffffu, sbase, leader);
+            slot = sbase + __popc(mm & ((1u << lane) - 1u));
+        }
+        if (mover) {
+            const unsigned peers = __match_any_sync(mm, o.cell);
+            const int leader = __ffs(peers) - 1;
+            int tbase = 0;
+            if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
+            tbase = __shfl_sync(peers, tbase, leader);
+            const int ticket = tbase + __popc(peers & ((1u << lane) - 1u));
+            A.mrec[slot] = make_int4(o.cell, tb + t, ticket, 0);
+        }
+        if (valid) {
+            const int j = tb + t;
+            if (stayer || mover) {
                 R4 qo, vo, so;
                 qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
                 vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = v.w;
                 so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
-                A.pos_out[dest] = qo;
-                A.vel_out[dest] = vo;
-                A.psi_out[dest] = so;
+                A.pos_out[j] = qo;
+                A.vel_out[j] = vo;
+                A.psi_out[j] = so;
                 acc.n_alive += 1;
                 acc.sum_v2 += fx_from((double)o.v2);
                 acc.sum_B += fx_from((double)o.absB);
-            } else if (!stayer && !mover) {
+                A.keys[j] = stayer ? make_int2(c_old, KIND_STAY) : make_int2(slot, KIND_MOVE);
+                if (stayer && c_old == P.ovf_cell) ovf_stayers += 1;
+            } else {
                 acc.evap_v2 += fx_from((double)o.v2);
                 acc.evap_B += fx_from((double)o.absB);
                 if (o.fate == FATE_MAJORANA) acc.n_maj += 1;
                 else acc.n_knife += 1;
+                A.keys[j] = make_int2(-1, KIND_LOST);
             }
         }
     }
+    acc.pad0 = ovf_stayers;
+    block_reduce_partial<BLOCK>(acc, red);
+    if (threadIdx.x == 0) {
+        A.tile_ovf[b] = (int)acc.pad0;
+        acc.pad0 = 0;
+        A.partials[b] = acc;
+    }
+}
 
-    if (!COMMIT) {
-        if (threadIdx.x == 0) {
-            A.tile_movers[b] = (int)(carry & 0xFFFFu);
-            int ovf = 0;
-            if (L > 0 && s_cell[L - 1] == P.ovf_cell) {
-                const int seg = A.old_start[P.ovf_cell];
+// ---------------------------------------------------------------------------------------------
+// permute_pass: destination of every surviving atom in the new order, written as the next
+// permutation.  Stayers rank inside their old cell by a block-wide prefix count (a grid cell
+// never straddles tiles; the overflow cell adds the count of its stayers in earlier tiles),
+// movers take the slot mover_rank computed.
+// ---------------------------------------------------------------------------------------------
+template <class R, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
+    __shared__ uint32_t s_pre[CAP];
+    __shared__ uint32_t wsum[32];
+    const int p = A.parity;
+    const int b = blockIdx.x;
+    if (b >= A.ctl->ntiles[p]) return;
+    const int tb = A.tile_begin[b];
+    const int te = A.tile_begin[b + 1];
+    const int L = te - tb;
+    if (L > CAP || L < 0) return;  // step_pass marked every atom of such a tile as lost
+    const int cloud = A.tile_cloud[b];
+    const int carry_base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
+    uint32_t carry = 0;
+    for (int base = 0; base < L; base += BLOCK) {
+        const int t = base + threadIdx.x;
+        const bool valid = t < L;
+        int2 key = make_int2(-1, KIND_LOST);
+        if (valid) key = A.keys[tb + t];
+        const bool stayer = valid && key.y == KIND_STAY;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan_u32<BLOCK>(stayer ? 1u : 0u, wsum, tot) + carry;
+        carry += tot;
+        if (valid) s_pre[t] = ex;
+        __syncthreads();
+        if (valid) {
+            int dest = -1;
+            if (stayer) {
+                const int c = key.x;
+                const int seg = A.old_start[c];
                 const int sl = seg > tb ? seg - tb : 0;
-                ovf = (int)(carry >> 16) - (int)(s_pre[sl] >> 16);
+                if (sl <= t) {
+                    int rank = (int)(ex - s_pre[sl]);
+                    if (seg < tb) rank += carry_base;
+                    dest = A.new_start[c] + rank;
+                    if (dest < A.new_start[c] || dest >= A.new_start[c + 1]) dest = -2;
+                } else {
+                    dest = -2;
+                }
+            } else if (key.y == KIND_MOVE) {
+                dest = (key.x >= 0 && key.x < A.capacity) ? A.mrec[key.x].w : -2;
+                if (dest < 0 || dest >= A.capacity) dest = -2;
             }
-            A.tile_ovf[b] = ovf;
+            if (dest >= 0) A.src_out[dest] = tb + t;
+            else if (dest == -2) atomicOr(&A.ctl->err, EB_INCONSISTENT);
         }
-    } else {
-        block_reduce_partial<BLOCK>(acc, red);
-        if (threadIdx.x == 0) A.partials[b] = acc;
     }
 }
 
@@ -581,42 +634,36 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
     }
 }
 
-// incoming movers: each writes its old index into its cell's incoming slots (ticket order)
+// incoming movers: each writes its old position into its cell's incoming slots (ticket order)
 template <class R>
 __global__ void __launch_bounds__(256) mover_place(Args<R> A) {
-    const int b = blockIdx.x;
-    if (b >= A.ctl->ntiles[A.parity]) return;
-    const int tb = A.tile_begin[b];
-    const int m = A.tile_movers[b];
-    for (int i = threadIdx.x; i < m; i += 256) {
-        const int4 r = A.mrec[tb + i];
+    const int m = A.ctl->movers;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
+        const int4 r = A.mrec[i];
         const int slot = A.mover_base[r.x] + r.z;
         if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
         else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
 
-// rank = number of incoming movers of the same cell with a smaller old index
+// rank = number of incoming movers of the same cell with a smaller old position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
-    const int b = blockIdx.x;
-    if (b >= A.ctl->ntiles[A.parity]) return;
-    const int tb = A.tile_begin[b];
-    const int m = A.tile_movers[b];
-    for (int i = threadIdx.x; i < m; i += 256) {
-        int4 r = A.mrec[tb + i];
+    const int m = A.ctl->movers;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
+        int4 r = A.mrec[i];
         const int lo = A.mover_base[r.x];
         const int hi = A.new_start[r.x + 1];
         if (lo < 0 || hi > A.capacity || lo > hi) {
             atomicOr(&A.ctl->err, EB_INCONSISTENT);
             r.w = -1;
-            A.mrec[tb + i] = r;
+            A.mrec[i] = r;
             continue;
         }
         int rank = 0;
         for (int k = lo; k < hi; ++k) rank += (A.in_list[k] < r.y) ? 1 : 0;
         r.w = lo + rank;
-        A.mrec[tb + i] = r;
+        A.mrec[i] = r;
     }
 }
 
@@ -668,7 +715,10 @@ __global__ void __launch_bounds__(256) finalize(Args<R> A) {
         g.err = A.ctl->err;
         d.T_knife = knife_temperature(P.mass, P.kB, P.T0, (P.flags & F_KNIFE_FIXED_T) != 0, acc.sum_v2,
                                       acc.n_alive);
-        if (k == 0 && !INIT) A.ctl->step[1 - p] = step_now + 1;
+        if (k == 0 && !INIT) {
+            A.ctl->step[1 - p] = step_now + 1;
+            A.ctl->movers = 0;
+        }
     }
 }
 
@@ -687,8 +737,9 @@ __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
     TilePartial acc;
     zero_partial(acc);
     for (int i = tb + threadIdx.x; i < te; i += BLOCK) {
-        const R4 q = A.pos_in[i];
-        const R4 v = A.vel_in[i];
+        const int s = A.src_in[i];
+        const R4 q = A.pos_in[s];
+        const R4 v = A.vel_in[s];
         Field<R> f;
         trap_field(P, q.x, q.y, q.z, f);
         const R v2 = v.x * v.x + v.y * v.y + v.z * v.z;
@@ -843,6 +894,23 @@ __global__ void __launch_bounds__(256) init_atoms(Args<R> A, const int* cloud_at
     pos[i] = q;
     vel[i] = v;
     psi[i] = s;
+}
+
+// sorted copy of the current state (for get_state): out[j] = state[src[j]]
+template <class R>
+__global__ void __launch_bounds__(256) materialize(Args<R> A, int n, typename V4T<R>::type* pos,
+                                                   typename V4T<R>::type* vel, typename V4T<R>::type* psi) {
+    const int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= n) return;
+    const int s = A.src_in[j];
+    pos[j] = A.pos_in[s];
+    vel[j] = A.vel_in[s];
+    psi[j] = A.psi_in[s];
+}
+
+__global__ void fill_identity(int* a, int n) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i < n) a[i] = i;
 }
 
 template <class R>

@@ -219,6 +219,28 @@ DSMC_HD void xsincos(double x, double* s, double* c) {
     *c = cc;
 }
 
+// 1/sqrt(x) for positive normal x by Newton's iteration y <- y (3/2 - x y^2 / 2) from the
+// bit-level initial guess of Lomont, "Fast inverse square root" (2003): 3 iterations in float,
+// 5 in double reach the working precision (within ~2 ulp; deterministic, not correctly rounded).
+DSMC_HD float xrsqrt(float x) {
+    float y = u2f(0x5f375a86u - (f2u(x) >> 1));
+    const float hx = 0.5f * x;
+    y = y * xfma(-(hx * y), y, 1.5f);
+    y = y * xfma(-(hx * y), y, 1.5f);
+    y = y * xfma(-(hx * y), y, 1.5f);
+    return y;
+}
+DSMC_HD double xrsqrt(double x) {
+    double y = u2d(0x5fe6eb50c7b537a9ull - (d2u(x) >> 1));
+    const double hx = 0.5 * x;
+    y = y * xfma(-(hx * y), y, 1.5);
+    y = y * xfma(-(hx * y), y, 1.5);
+    y = y * xfma(-(hx * y), y, 1.5);
+    y = y * xfma(-(hx * y), y, 1.5);
+    y = y * xfma(-(hx * y), y, 1.5);
+    return y;
+}
+
 // natural log for normal positive x
 DSMC_HD float xlog(float x) {
     uint32_t u = f2u(x);
@@ -388,44 +410,51 @@ template <class R> struct Field {
 
 template <class R>
 DSMC_HD void trap_field(const CloudPhys<R>& P, R x, R y, R z, Field<R>& f) {
-    R Bx, By, Bz;
-    R jxx, jxy, jxz, jyx, jyy, jyz, jzx, jzy, jzz;  // dB_i / dx_j stored as j{i}{j}
     if (P.trap == TRAP_QUADRUPOLE) {
+        // B = (h x, h y, B0 - B' z), h = B'/2;  grad|B| = (h B^x, h B^y, -B' B^z)
         const R h = R(0.5) * P.Bp;
-        Bx = h * x;
-        By = h * y;
-        Bz = P.B0 - P.Bp * z;
-        jxx = h; jxy = R(0); jxz = R(0);
-        jyx = R(0); jyy = h; jyz = R(0);
-        jzx = R(0); jzy = R(0); jzz = -P.Bp;
-    } else if (P.trap == TRAP_IOFFE_PRITCHARD) {
-        // CUDADSMC/src/moveAtoms.cu:135-157
-        const R hc = R(0.5) * P.Bpp;
-        Bx = P.Bp * x - hc * (x * z);
-        By = -(P.Bp * y) - hc * (y * z);
-        Bz = P.B0 + hc * (z * z - R(0.5) * (x * x + y * y));
-        jxx = P.Bp - hc * z; jxy = R(0); jxz = -(hc * x);
-        jyx = R(0); jyy = -P.Bp - hc * z; jyz = -(hc * y);
-        jzx = -(hc * x); jzy = -(hc * y); jzz = P.Bpp * z;
-    } else {
-        f.bx = R(0); f.by = R(0); f.bz = R(1);
-        f.absB = R(0);
-        f.gx = R(0); f.gy = R(0); f.gz = R(0);
+        const R Bx = h * x, By = h * y, Bz = P.B0 - P.Bp * z;
+        const R b2 = Bx * Bx + By * By + Bz * Bz;
+        if (b2 > R(0)) {
+            const R inv = xrsqrt(b2);
+            f.absB = b2 * inv;
+            f.bx = Bx * inv; f.by = By * inv; f.bz = Bz * inv;
+        } else {
+            f.absB = R(0);
+            f.bx = R(0); f.by = R(0); f.bz = R(1);
+        }
+        f.gx = h * f.bx;
+        f.gy = h * f.by;
+        f.gz = -(P.Bp * f.bz);
         return;
     }
-    R b2 = Bx * Bx + By * By + Bz * Bz;
-    R ab = xsqrt(b2);
-    if (ab > R(0)) {
-        R inv = R(1) / ab;
-        f.bx = Bx * inv; f.by = By * inv; f.bz = Bz * inv;
-    } else {
-        f.bx = R(0); f.by = R(0); f.bz = R(1);
+    if (P.trap == TRAP_IOFFE_PRITCHARD) {
+        // CUDADSMC/src/moveAtoms.cu:135-157
+        const R hc = R(0.5) * P.Bpp;
+        const R Bx = P.Bp * x - hc * (x * z);
+        const R By = -(P.Bp * y) - hc * (y * z);
+        const R Bz = P.B0 + hc * (z * z - R(0.5) * (x * x + y * y));
+        const R b2 = Bx * Bx + By * By + Bz * Bz;
+        if (b2 > R(0)) {
+            const R inv = xrsqrt(b2);
+            f.absB = b2 * inv;
+            f.bx = Bx * inv; f.by = By * inv; f.bz = Bz * inv;
+        } else {
+            f.absB = R(0);
+            f.bx = R(0); f.by = R(0); f.bz = R(1);
+        }
+        // d|B|/dx_j = B^ . dB/dx_j  (columns of the Jacobian, moveAtoms.cu:144-157)
+        const R jxx = P.Bp - hc * z, jxz = -(hc * x);
+        const R jyy = -P.Bp - hc * z, jyz = -(hc * y);
+        const R jzx = -(hc * x), jzy = -(hc * y), jzz = P.Bpp * z;
+        f.gx = f.bx * jxx + f.bz * jzx;
+        f.gy = f.by * jyy + f.bz * jzy;
+        f.gz = f.bx * jxz + f.by * jyz + f.bz * jzz;
+        return;
     }
-    f.absB = ab;
-    // d|B|/dx_j = B^ . dB/dx_j  (columns of the Jacobian, moveAtoms.cu:97-107)
-    f.gx = f.bx * jxx + f.by * jyx + f.bz * jzx;
-    f.gy = f.bx * jxy + f.by * jyy + f.bz * jzy;
-    f.gz = f.bx * jxz + f.by * jyz + f.bz * jzz;
+    f.bx = R(0); f.by = R(0); f.bz = R(1);
+    f.absB = R(0);
+    f.gx = R(0); f.gy = R(0); f.gz = R(0);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -495,7 +524,7 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
         a.ur = nur; a.ui = nui; a.dr = ndr; a.di = ndi;
         if (P.flags & F_NORMALISE) {
             R n2 = a.ur * a.ur + a.ui * a.ui + a.dr * a.dr + a.di * a.di;
-            R inv = R(1) / xsqrt(n2);
+            R inv = xrsqrt(n2);
             a.ur = a.ur * inv; a.ui = a.ui * inv; a.dr = a.dr * inv; a.di = a.di * inv;
         }
     }
@@ -545,8 +574,8 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
 // each candidate is a uniformly chosen distinct pair (i, j) accepted with probability
 // sigma v_r alpha dt_c Mc / (V Ncand); accepted pairs scatter isotropically about their
 // centre of mass (collisions.cu:425-437, 537-546).  vel points at n consecutive atoms
-// (4 reals each).  Random numbers: two Philox blocks per candidate keyed by
-// (cell, step, cloud, candidate).
+// (4 reals each).  Random numbers: one Philox block per candidate keyed by
+// (cell, step, cloud, candidate), the second one only for accepted pairs.
 // ---------------------------------------------------------------------------------------
 template <class R> struct CollideResult {
     int32_t accepted;
@@ -568,8 +597,7 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
     const R pacc = (P.cand_pref * Mc) / ncf;
     const R two_pi = R(6.283185307179586476925286766559);
     for (int k = 0; k < ncand; ++k) {
-        u32x4 w = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k, seed);
-        u32x4 w2 = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k + 1u, seed);
+        const u32x4 w = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k, seed);
         uint32_t i = index_below(w.x, (uint32_t)n);
         uint32_t j = index_below(w.y, (uint32_t)(n - 1));
         j += (j >= i) ? 1u : 0u;
@@ -580,12 +608,14 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
         R svr = P.sigma * vr;
         if (svr > sigvrmax) sigvrmax = svr;
         R pa = svr * pacc;
-        R u = u01<R>(w.z, w2.z);
+        R u = u01<R>(w.z, w.w);
         if (u < pa) {
-            R ct = R(2) * u01<R>(w.w, w2.w) - R(1);
+            // the scattering angles come from a second block, drawn only for accepted pairs
+            const u32x4 w2 = draw(local_cell, step, PURPOSE_COLLIDE, (uint32_t)P.cloud_id, 2u * (uint32_t)k + 1u, seed);
+            R ct = R(2) * u01<R>(w2.x, w2.y) - R(1);
             R st2 = R(1) - ct * ct;
             R st = xsqrt(st2 > R(0) ? st2 : R(0));
-            R phi = two_pi * u01<R>(w2.x, w2.y);
+            R phi = two_pi * u01<R>(w2.z, w2.w);
             R sp, cp;
             xsincos(phi, &sp, &cp);
             R hv = R(0.5) * vr;

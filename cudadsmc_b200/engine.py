@@ -37,11 +37,11 @@ class DSMCError(RuntimeError):
 
 
 def load_library(path: str | None = None) -> C.CDLL:
-    """Loads libdsmc_b200.so (raises if it has not been built)."""
+    """Loads libdsmc_b200.so (raises if it has not been built); DSMC_LIB overrides the path."""
     global _LIB
     if _LIB is not None and path is None:
         return _LIB
-    p = path or LIB_PATH
+    p = path or os.environ.get("DSMC_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise FileNotFoundError(f"{p} is missing: build it with `python -m cudadsmc_b200.build`")
     lib = C.CDLL(p)

@@ -76,7 +76,7 @@ def philox4x32_10(ctr, key) -> np.ndarray:
 
 
 def math(which: str, x: np.ndarray) -> np.ndarray:
-    code = {"sin": 0, "cos": 1, "log": 2, "exp": 3}[which]
+    code = {"sin": 0, "cos": 1, "log": 2, "exp": 3, "rsqrt": 4}[which]
     x = np.ascontiguousarray(x)
     y = np.empty_like(x)
     if x.dtype == np.float32:

@@ -464,7 +464,7 @@ OAPI void oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out)
     u32x4 r = philox4x32_10(c, key[0], key[1]);
     out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
 }
-// which: 0 sin, 1 cos, 2 log, 3 exp
+// which: 0 sin, 1 cos, 2 log, 3 exp, 4 rsqrt
 OAPI void oracle_math_f(int which, const float* x, float* y, int64_t n) {
     for (int64_t i = 0; i < n; ++i) {
         float s, c;
@@ -472,7 +472,8 @@ OAPI void oracle_math_f(int which, const float* x, float* y, int64_t n) {
         case 0: xsincos(x[i], &s, &c); y[i] = s; break;
         case 1: xsincos(x[i], &s, &c); y[i] = c; break;
         case 2: y[i] = xlog(x[i]); break;
-        default: y[i] = xexp(x[i]); break;
+        case 3: y[i] = xexp(x[i]); break;
+        default: y[i] = xrsqrt(x[i]); break;
         }
     }
 }
@@ -483,7 +484,8 @@ OAPI void oracle_math_d(int which, const double* x, double* y, int64_t n) {
         case 0: xsincos(x[i], &s, &c); y[i] = s; break;
         case 1: xsincos(x[i], &s, &c); y[i] = c; break;
         case 2: y[i] = xlog(x[i]); break;
-        default: y[i] = xexp(x[i]); break;
+        case 3: y[i] = xexp(x[i]); break;
+        default: y[i] = xrsqrt(x[i]); break;
         }
     }
 }

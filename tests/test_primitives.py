@@ -37,6 +37,15 @@ def test_log_exp_accuracy():
     assert oracle.math("exp", np.array([-100.0], np.float32))[0] == 0.0
 
 
+def test_rsqrt_accuracy():
+    rng = np.random.default_rng(3)
+    x32 = np.exp(rng.uniform(-80, 80, 200000)).astype(np.float32)
+    x32 = x32[np.isfinite(x32) & (x32 > np.finfo(np.float32).tiny)]
+    assert np.max(ulps(oracle.math("rsqrt", x32), 1 / np.sqrt(x32.astype(np.float64)), np.float32)) <= 3
+    x64 = np.exp(rng.uniform(-600, 600, 200000))
+    assert np.max(ulps(oracle.math("rsqrt", x64), 1 / np.sqrt(x64), np.float64)) <= 3
+
+
 def test_philox_keying_and_avalanche():
     a = oracle.philox4x32_10([1, 2, 3, 4], [5, 6])
     assert np.array_equal(a, oracle.philox4x32_10([1, 2, 3, 4], [5, 6]))
