@@ -49,7 +49,7 @@ constexpr int MOVER_GRID = 148 * 8;  // grid-stride kernels over the mover list
 
 struct __align__(16) TilePartial {
     i128 sum_v2, sum_B, evap_v2, evap_B;
-    long long n_alive, n_maj, n_knife, coll, cand, pad0, pad1, pad2;
+    long long n_alive, n_maj, n_knife, coll, cand, ovf_stayers, pad1, pad2;
 };
 
 struct CloudDyn {
@@ -180,6 +180,7 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
     t.n_knife = warp_sum_ll(t.n_knife);
     t.coll = warp_sum_ll(t.coll);
     t.cand = warp_sum_ll(t.cand);
+    t.ovf_stayers = warp_sum_ll(t.ovf_stayers);
     if (lane == 0) sm[warp] = t;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -193,6 +194,7 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
             t.n_knife += sm[w].n_knife;
             t.coll += sm[w].coll;
             t.cand += sm[w].cand;
+            t.ovf_stayers += sm[w].ovf_stayers;
         }
     }
     __syncthreads();
@@ -201,7 +203,7 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
 __device__ __forceinline__ void zero_partial(TilePartial& t) {
     t.sum_v2 = 0; t.sum_B = 0; t.evap_v2 = 0; t.evap_B = 0;
     t.n_alive = 0; t.n_maj = 0; t.n_knife = 0; t.coll = 0; t.cand = 0;
-    t.pad0 = 0; t.pad1 = 0; t.pad2 = 0;
+    t.ovf_stayers = 0; t.pad1 = 0; t.pad2 = 0;
 }
 
 template <class R>
@@ -388,11 +390,10 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
             }
         }
     }
-    acc.pad0 = ovf_stayers;
+    acc.ovf_stayers = ovf_stayers;
     block_reduce_partial<BLOCK>(acc, red);
     if (threadIdx.x == 0) {
-        A.tile_ovf[b] = (int)acc.pad0;
-        acc.pad0 = 0;
+        A.tile_ovf[b] = (int)acc.ovf_stayers;
         A.partials[b] = acc;
     }
 }
