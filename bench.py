@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -123,6 +125,55 @@ def cpu_baseline(run, cloud, steps: int, threads: int | None = None) -> dict:
     return {"value": atom_steps / (t1 - t0), "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{cloud.n_atoms:.0e} atoms, {steps} timed steps after init + 1 warm-up step "
                       f"({t1 - t0:.1f} s), OpenMP float build of oracle/dsmc_oracle.cpp"}
+
+
+def batched_vs_sequential(stream, steps: int) -> dict:
+    """256 clouds stepped together in one handle vs the same clouds as 256 single-cloud handles
+    run one after another on the same stream; per-cloud results are identical (checked)."""
+    import torch
+    from cudadsmc_b200 import Simulation
+    from cudadsmc_b200.workloads import batched_ensemble
+    run, clouds = batched_ensemble()
+    batch = Simulation(run, clouds)
+    batch.set_stream(stream.cuda_stream)
+    batch.init_cloud(run.seed)
+    tile, _ = batch.autotune(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d0 = batch.diagnostics()
+    e0.record(stream)
+    batch.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    d1 = batch.diagnostics()
+    singles = []
+    for c in clouds:
+        s = Simulation(run, c)
+        s.set_stream(stream.cuda_stream)
+        s.init_cloud(run.seed)
+        singles.append(s)
+    # bring the single runs to the batch's step count before timing
+    pre = d0["step"]
+    for s in singles:
+        s.step(pre)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for s in singles:
+        s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    same = all(singles[k].diagnostics()["sum_v2"] == batch.diagnostics(k)["sum_v2"] and
+               singles[k].diagnostics()["n_alive"] == batch.diagnostics(k)["n_alive"] for k in range(len(clouds)))
+    for s in singles:
+        s.close()
+    atoms = d1["atom_steps"] - d0["atom_steps"]
+    batch.close()
+    return {"clouds": len(clouds), "atoms": int(sum(c.n_atoms for c in clouds)), "steps": steps,
+            "tile_atoms": tile, "batched_atom_steps_per_s": atoms / (ms_batch * 1e-3),
+            "sequential_atom_steps_per_s": atoms / (ms_seq * 1e-3), "speedup": ms_seq / ms_batch,
+            "ms_per_step_batched": ms_batch / steps, "ms_per_step_sequential": ms_seq / steps,
+            "identical_per_cloud_results": bool(same)}
 
 
 def run_reference(args):
@@ -273,6 +324,11 @@ def main():
                "wall_s": wall}
         sim2.close()
 
+    # ------------------------------------------------------------------ batched vs sequential
+    batched = None
+    if rank == 0 and ws == 1 and not args.no_batched:
+        batched = batched_vs_sequential(stream, steps=args.batched_steps)
+
     # ------------------------------------------------------------------ CPU baseline
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -289,7 +345,7 @@ def main():
                            "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
                            "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"},
                 "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
                 "n_alive_end": d1["n_alive"]}
         print(json.dumps(line), flush=True)
     sim.close()

@@ -105,3 +105,33 @@ class StateBuffers(C.Structure):
         ("n", C.c_int64),
         ("cloud_counts", C.POINTER(C.c_int64)),
     ]
+
+
+class AdjParams(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32),
+        ("checkpoint_every", C.c_int32),
+        ("precision", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("sigmoid_width_kT", C.c_double),
+    ]
+
+
+class Grad(C.Structure):
+    _fields_ = [
+        ("loss", C.c_double),
+        ("mean_energy_kT", C.c_double),
+        ("retained_fraction", C.c_double),
+        ("dL_dBp", C.c_double),
+        ("dL_dB0", C.c_double),
+        ("dL_deta", C.c_double * 9),
+        ("collisions", C.c_int64),
+        ("ms_record", C.c_double),
+        ("ms_forward", C.c_double),
+        ("ms_backward", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["dL_deta"] = list(self.dL_deta)
+        return d

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "dsmc.h"
+#include "dsmc_adjoint.cuh"
 #include "dsmc_kernels.cuh"
 #include "dsmc_setup.h"
 
@@ -47,6 +48,8 @@ template <class T> struct DevBuf {
     ~DevBuf() { free(); }
 };
 
+constexpr int kMinTile = 128;  // smallest tile the autotuner tries (sizes the tile tables)
+
 const char* kKernelNames[] = {"step_pass",   "scan_reduce", "scan_top",     "scan_down",
                               "mover_place", "mover_rank",  "permute_pass", "finalize"};
 constexpr int kNumStepKernels = 8;
@@ -68,6 +71,11 @@ struct dsmc_handle {
     virtual void set_stream(cudaStream_t s) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) = 0;
+    virtual void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) = 0;
+    virtual void adjoint_run(const dsmc_adj_params* p, dsmc_grad* g) = 0;
+    virtual void adjoint_loss(const double* theta, double* loss, double* grad) = 0;
+    virtual void adjoint_export(double* x0, double* v0, int64_t atoms_cap, int32_t* off, int64_t off_cap, int32_t* ij,
+                                double* nv, int64_t log_cap, int64_t* n_atoms, int64_t* n_log, int32_t* steps) = 0;
 };
 
 namespace {
@@ -112,7 +120,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
     bool profiling = false;
     double prof_ms[kNumStepKernels] = {0};
     int64_t prof_n[kNumStepKernels] = {0};
-    cudaEvent_t ev[kNumStepKernels + 1] = {};
+    cudaEvent_t ev[kNumStepKernels + 1] = {};  // also reused by the autotuner and the adjoint (>= 4)
     size_t smem_tile = 0;
 
     Engine(const dsmc_params& r, const dsmc_cloud_params* clouds, int n) {
@@ -122,7 +130,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         use_graphs = r.use_graphs != 0;
         tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP / 2;
         if (tile_nominal > CAP / 2) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP / 2)};
-        if (tile_nominal < 32) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= 32"};
+        if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
         allocate();
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -162,7 +170,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         if (cap >= ((int64_t)1 << 31)) throw Fail{DSMC_ERR_INVALID, "more than 2^31 atoms"};
         total_cells = (int)cells;
         capacity = (int)std::max<int64_t>(cap, 1);
-        max_tiles = capacity / tile_nominal + nclouds + 2;
+        max_tiles = capacity / std::min(tile_nominal, kMinTile) + nclouds + 2;
     }
 
     void allocate() {
@@ -550,6 +558,266 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         profiling = on;
         for (int k = 0; k < kNumStepKernels; ++k) { prof_ms[k] = 0; prof_n[k] = 0; }
     }
+    // Times dsmc_step with each candidate tile size (the simulation advances meanwhile; results do
+    // not depend on the tiling) and keeps the fastest.  A new size takes effect one step after it
+    // is set (the tiling of a step is built by the scan of the step before).
+    void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
+        if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
+        const int cands[] = {128, 192, 256, 384, 512, 768, 1024};
+        int best = tile_nominal;
+        double best_ms = 1e300;
+        const bool prof = profiling;
+        profiling = false;
+        for (int T : cands) {
+            if (T > CAP / 2) continue;
+            set_tile(T);
+            step(1);  // builds the tiling of size T
+            CU(cudaEventRecord(ev[0], stream));
+            step(steps_per_candidate);
+            CU(cudaEventRecord(ev[1], stream));
+            CU(cudaEventSynchronize(ev[1]));
+            float ms = 0;
+            CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            const double per = ms / steps_per_candidate;
+            if (per < best_ms) { best_ms = per; best = T; }
+        }
+        set_tile(best);
+        step(1);
+        profiling = prof;
+        check_err();
+        if (chosen) *chosen = best;
+        if (ms_per_step) *ms_per_step = best_ms;
+    }
+
+    void set_tile(int T) {
+        sync();
+        tile_nominal = T;
+        for (int p = 0; p < 2; ++p) args[p].tile_nominal = T;
+        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+    }
+
+    // ------------------------------------------------------------------ adjoint
+    // record: the physical run's initial state by atom id and its collision events
+    DevBuf<double> adj_x0, adj_v0, adj_n, adj_sums, adj_theta_b;
+    DevBuf<int2> adj_ij;
+    DevBuf<int> adj_off, adj_count;
+    int adj_steps = -1, adj_natoms = 0, adj_nlog = 0, adj_K = 100, adj_prec = DSMC_FP64;
+    double adj_width = 0.2;
+
+    void adjoint_run(const dsmc_adj_params* ap, dsmc_grad* g) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "adjoint before init"};
+        if (nclouds != 1 || cp[0].trap != DSMC_TRAP_QUADRUPOLE)
+            throw Fail{DSMC_ERR_UNSUPPORTED, "the adjoint supports one cloud in the linear (quadrupole) trap"};
+        if (steps_taken != 0) throw Fail{DSMC_ERR_STATE, "call dsmc_adjoint_run right after dsmc_init_cloud"};
+        if (ap->steps < 1 || ap->checkpoint_every < 1 || !(ap->sigmoid_width_kT > 0))
+            throw Fail{DSMC_ERR_INVALID, "adjoint: steps, checkpoint_every and sigmoid_width_kT must be positive"};
+        if (ap->precision != DSMC_FP32 && ap->precision != DSMC_FP64) throw Fail{DSMC_ERR_INVALID, "adjoint precision"};
+        sync();
+        Ctl h;
+        CU(cudaMemcpy(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        const int n = h.n[parity];
+        if (n != (int)cp[0].n_atoms) throw Fail{DSMC_ERR_STATE, "adjoint: atoms were lost before the run"};
+        adj_steps = ap->steps; adj_natoms = n; adj_K = ap->checkpoint_every; adj_prec = ap->precision;
+        adj_width = ap->sigmoid_width_kT;
+        adj_x0.alloc(3 * (size_t)std::max(n, 1)); adj_v0.alloc(3 * (size_t)std::max(n, 1));
+        if (n > 0)
+            state_by_id<R><<<(n + 255) / 256, 256, 0, stream>>>(args[parity], n, adj_x0.p, adj_v0.p, &ctl.p->err);
+        const int cap = 1 << 22;
+        adj_ij.alloc(cap); adj_n.alloc(3 * (size_t)cap); adj_off.alloc(ap->steps + 1); adj_count.alloc(1);
+        CU(cudaMemsetAsync(adj_off.p, 0, (ap->steps + 1) * sizeof(int), stream));
+        CU(cudaMemsetAsync(adj_count.p, 0, sizeof(int), stream));
+        // the physical run, recording every accepted collision
+        for (int p = 0; p < 2; ++p) {
+            args[p].clog_ij = adj_ij.p; args[p].clog_n = adj_n.p; args[p].clog_count = adj_count.p;
+            args[p].clog_off = adj_off.p; args[p].clog_cap = cap; args[p].clog_step0 = 0;
+            args[p].clog_steps = ap->steps;
+        }
+        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        cudaEvent_t e0 = ev[0], e1 = ev[1];
+        CU(cudaEventRecord(e0, stream));
+        step(ap->steps);
+        CU(cudaEventRecord(e1, stream));
+        CU(cudaEventSynchronize(e1));
+        float ms_rec = 0;
+        CU(cudaEventElapsedTime(&ms_rec, e0, e1));
+        for (int p = 0; p < 2; ++p) {
+            args[p].clog_ij = nullptr; args[p].clog_n = nullptr; args[p].clog_count = nullptr;
+            args[p].clog_off = nullptr; args[p].clog_cap = 0;
+        }
+        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        check_err();
+        int cnt = 0;
+        CU(cudaMemcpy(&cnt, adj_count.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (cnt > cap) throw Fail{DSMC_ERR_CAPACITY, "adjoint: more than 2^22 collisions recorded; run fewer steps"};
+        adj_nlog = cnt;
+        // the smoothed model at the run's own parameters, forward and backward
+        double theta[ADJ_NPARAM];
+        own_theta(theta);
+        double loss = 0, tb[ADJ_NPARAM] = {0}, W = 0, Sm = 0, ms_f = 0, ms_b = 0;
+        smoothed(theta, true, &loss, tb, &W, &Sm, &ms_f, &ms_b);
+        memset(g, 0, sizeof(*g));
+        g->loss = loss;
+        const double kT = phys[0].kB * cp[0].temperature;
+        g->mean_energy_kT = 0.5 * cp[0].mass * Sm / W / kT;
+        g->retained_fraction = W / (double)n;
+        g->dL_dBp = tb[0];
+        g->dL_dB0 = tb[1];
+        for (int k = 0; k < 9; ++k) g->dL_deta[k] = tb[2 + k];
+        g->collisions = adj_nlog;
+        g->ms_record = ms_rec;
+        g->ms_forward = ms_f;
+        g->ms_backward = ms_b;
+    }
+
+    void own_theta(double* theta) const {
+        theta[0] = cp[0].dBdz;
+        theta[1] = cp[0].B0;
+        for (int k = 0; k < 9; ++k) theta[2 + k] = cp[0].knife_eta[k];
+    }
+
+    void smoothed(const double* theta, bool grad, double* loss, double* tb, double* W, double* Sm, double* ms_f,
+                  double* ms_b) {
+        if (adj_prec == DSMC_FP64) smoothed_t<double>(theta, grad, loss, tb, W, Sm, ms_f, ms_b);
+        else smoothed_t<float>(theta, grad, loss, tb, W, Sm, ms_f, ms_b);
+    }
+
+    template <class S>
+    void smoothed_t(const double* theta, bool grad, double* loss, double* tb, double* Wout, double* Sout,
+                    double* ms_f, double* ms_b) {
+        typedef typename V4T<S>::type S4;
+        const int n = adj_natoms, steps = adj_steps, K = adj_K;
+        const dsmc_cloud_params& c = cp[0];
+        const double kB = phys[0].kB;
+        SmoothArgs<S> A;
+        memset(&A, 0, sizeof(A));
+        A.C.Bp = (S)theta[0];
+        A.C.B0 = (S)theta[1];
+        A.C.B_floor = (S)0;
+        A.C.dt = (S)run.dt;
+        A.C.half_dt = (S)(0.5 * run.dt);
+        A.C.accel_scale = (S)(c.moment / c.mass);
+        A.C.kappa = (S)(2.0 * c.moment / c.mass);
+        A.C.inv_width = (S)(1.0 / (2.0 * adj_width * kB * c.temperature / c.mass));
+        A.C.cut_scale = 2.0 * kB * c.temperature / c.mass;
+        A.n = n;
+        const int nn = std::max(n, 1);
+        DevBuf<S4> x, v, xb, vb, vpre, seg_x, seg_v, ck_x, ck_v;
+        DevBuf<S> w, e, wb, seg_w, ck_w;
+        x.alloc(nn); v.alloc(nn); w.alloc(nn); e.alloc(nn);
+        const int nseg = (steps + K - 1) / K;
+        const int ab = (nn + 255) / 256;
+        const int sum_blocks = std::min(ab, 1184);
+        partials_buf.alloc(sum_blocks);
+        adj_sums.alloc(2);
+        A.x = x.p; A.v = v.p; A.w = w.p; A.e = e.p;
+        A.ij = adj_ij.p; A.nv = adj_n.p; A.off = adj_off.p; A.partials = partials_buf.p;
+        if (grad) {
+            vpre.alloc(2 * (size_t)std::max(adj_nlog, 1));
+            seg_x.alloc((size_t)K * nn); seg_v.alloc((size_t)K * nn); seg_w.alloc((size_t)K * nn);
+            ck_x.alloc((size_t)nseg * nn); ck_v.alloc((size_t)nseg * nn); ck_w.alloc((size_t)nseg * nn);
+            xb.alloc(nn); vb.alloc(nn); wb.alloc(nn);
+            adj_theta_b.alloc(ADJ_NPARAM);
+            CU(cudaMemsetAsync(adj_theta_b.p, 0, ADJ_NPARAM * sizeof(double), stream));
+            A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_w = seg_w.p;
+            A.xb = xb.p; A.vb = vb.p; A.wb = wb.p; A.theta_b = adj_theta_b.p;
+        }
+        std::vector<S> cuts(steps);
+        for (int t = 0; t < steps; ++t)
+            cuts[t] = (S)(A.C.cut_scale * knife_eta(c.knife_nknots, c.knife_step, theta + 2, (double)t));
+        CU(cudaEventRecord(ev[0], stream));
+        if (n > 0) sm_load<S><<<ab, 256, 0, stream>>>(A, adj_x0.p, adj_v0.p);
+        for (int t = 0; t < steps; ++t) {
+            if (grad && t % K == 0) {
+                const size_t o = (size_t)(t / K) * nn;
+                CU(cudaMemcpyAsync(ck_x.p + o, x.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+                CU(cudaMemcpyAsync(ck_v.p + o, v.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+                CU(cudaMemcpyAsync(ck_w.p + o, w.p, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
+            }
+            sm_collide<S><<<1, 32, 0, stream>>>(A, t, 0);
+            if (n > 0) sm_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], -1, t == steps - 1 ? 1 : 0);
+        }
+        if (n > 0) sm_sums<S><<<sum_blocks, 256, 0, stream>>>(A);
+        sm_sums_final<<<1, 32, 0, stream>>>(partials_buf.p, n > 0 ? sum_blocks : 0, adj_sums.p);
+        CU(cudaEventRecord(ev[1], stream));
+        double sums[2];
+        CU(cudaMemcpyAsync(sums, adj_sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        float mf = 0;
+        CU(cudaEventElapsedTime(&mf, ev[0], ev[1]));
+        if (ms_f) *ms_f = mf;
+        const double kT = kB * c.temperature;
+        const double Wd = sums[0], Sd = sums[1];
+        *loss = 0.5 * c.mass * Sd / Wd / kT + Wd / (double)n;
+        if (Wout) *Wout = Wd;
+        if (Sout) *Sout = Sd;
+        CU(cudaGetLastError());
+        if (!grad) return;
+        CU(cudaEventRecord(ev[2], stream));
+        const double half_m_over_kT = 0.5 * c.mass / kT;
+        if (n > 0) adj_seed<S><<<ab, 256, 0, stream>>>(A, adj_sums.p, half_m_over_kT);
+        for (int s = nseg - 1; s >= 0; --s) {
+            const int t0 = s * K, t1 = std::min(steps, t0 + K);
+            const size_t o = (size_t)s * nn;
+            CU(cudaMemcpyAsync(x.p, ck_x.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(v.p, ck_v.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(w.p, ck_w.p + o, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
+            for (int t = t0; t < t1; ++t) {
+                sm_collide<S><<<1, 32, 0, stream>>>(A, t, 1);
+                if (n > 0) sm_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], t - t0, 0);
+            }
+            for (int t = t1 - 1; t >= t0; --t) {
+                int k0 = 0;
+                double f = 0;
+                knot_weights(c.knife_nknots, c.knife_step, (double)t, &k0, &f);
+                if (n > 0) adj_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], t - t0, k0, f);
+                sm_collide_adjoint<S><<<1, 32, 0, stream>>>(A, t);
+            }
+        }
+        CU(cudaEventRecord(ev[3], stream));
+        CU(cudaMemcpyAsync(tb, adj_theta_b.p, ADJ_NPARAM * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        CU(cudaGetLastError());
+        float mb = 0;
+        CU(cudaEventElapsedTime(&mb, ev[2], ev[3]));
+        if (ms_b) *ms_b = mb;
+    }
+    DevBuf<TilePartial> partials_buf;
+
+    void adjoint_loss(const double* theta, double* loss, double* grad) override {
+        if (adj_steps < 0) throw Fail{DSMC_ERR_STATE, "dsmc_adjoint_loss needs a recorded run (dsmc_adjoint_run)"};
+        double own[ADJ_NPARAM];
+        own_theta(own);
+        const double* th = theta ? theta : own;
+        double tb[ADJ_NPARAM] = {0};
+        smoothed(th, grad != nullptr, loss, tb, nullptr, nullptr, nullptr, nullptr);
+        if (grad)
+            for (int k = 0; k < ADJ_NPARAM; ++k) grad[k] = tb[k];
+    }
+
+    void adjoint_export(double* x0, double* v0, int64_t atoms_cap, int32_t* off, int64_t off_cap, int32_t* ij,
+                        double* nv, int64_t log_cap, int64_t* n_atoms, int64_t* n_log, int32_t* steps_out) override {
+        if (adj_steps < 0) throw Fail{DSMC_ERR_STATE, "nothing recorded (dsmc_adjoint_run)"};
+        if (n_atoms) *n_atoms = adj_natoms;
+        if (n_log) *n_log = adj_nlog;
+        if (steps_out) *steps_out = adj_steps;
+        sync();
+        if (x0 && v0) {
+            if (atoms_cap < adj_natoms) throw Fail{DSMC_ERR_INVALID, "atom buffers too small"};
+            CU(cudaMemcpy(x0, adj_x0.p, 3 * (size_t)adj_natoms * sizeof(double), cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(v0, adj_v0.p, 3 * (size_t)adj_natoms * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        if (off) {
+            if (off_cap < adj_steps + 1) throw Fail{DSMC_ERR_INVALID, "offset buffer too small"};
+            CU(cudaMemcpy(off, adj_off.p, (adj_steps + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        if (ij && nv) {
+            if (log_cap < adj_nlog) throw Fail{DSMC_ERR_INVALID, "record buffers too small"};
+            CU(cudaMemcpy(ij, adj_ij.p, 2 * (size_t)adj_nlog * sizeof(int), cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(nv, adj_n.p, 3 * (size_t)adj_nlog * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+    }
+
     void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) override {
         const int n = std::min(cap, kNumStepKernels);
         for (int k = 0; k < n; ++k) {
@@ -702,3 +970,24 @@ DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, doubl
     return guard(h, [&] { h->kernel_times(names, ms, launches, cap, count); });
 }
 DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h) { return h ? kNumStepKernels : 0; }
+DSMC_API dsmc_status dsmc_adjoint_run(dsmc_handle* h, const dsmc_adj_params* p, dsmc_grad* g) {
+    NEED_H;
+    if (!p || !g) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->adjoint_run(p, g); });
+}
+DSMC_API dsmc_status dsmc_adjoint_loss(dsmc_handle* h, const double* theta, double* loss, double* grad) {
+    NEED_H;
+    if (!loss) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->adjoint_loss(theta, loss, grad); });
+}
+DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0, int64_t atoms_cap, int32_t* off,
+                                         int64_t off_cap, int32_t* ij, double* nv, int64_t log_cap,
+                                         int64_t* n_atoms, int64_t* n_log, int32_t* steps) {
+    NEED_H;
+    return guard(h, [&] { h->adjoint_export(x0, v0, atoms_cap, off, off_cap, ij, nv, log_cap, n_atoms, n_log, steps); });
+}
+DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, int32_t* tile_atoms,
+                                   double* ms_per_step) {
+    NEED_H;
+    return guard(h, [&] { h->autotune(steps_per_candidate, tile_atoms, ms_per_step); });
+}

@@ -42,7 +42,8 @@ enum : int {
     EB_INIT_REJECT = 8,
     EB_TILE_OVERFLOW = 16,
     EB_INCONSISTENT = 32,
-    EB_TIMEOUT = 64
+    EB_TIMEOUT = 64,
+    EB_LOG_FULL = 128
 };
 
 constexpr int MOVER_GRID = 148 * 8;  // grid-stride kernels over the mover list
@@ -114,6 +115,12 @@ template <class R> struct Args {
     const int* cloud_first_blk;  // nclouds + 1
     int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
     int capacity;
+    // collision record (adjoint runs): pairs by atom id, directions, per-step offsets
+    int2* clog_ij;
+    double* clog_n;
+    int* clog_count;
+    int* clog_off;
+    int clog_cap, clog_step0, clog_steps;
     unsigned long long seed;
 };
 
@@ -221,6 +228,31 @@ __device__ __forceinline__ R knife_cut_for(const CloudPhys<R>& P, double T, int 
     return (R)knife_cut_v2(eta, P.kB, T, P.mass);
 }
 
+// records accepted collisions of one cell: the atom ids of the pair and the direction n^
+template <class R> struct TileCollisionLog {
+    typedef typename V4T<R>::type R4;
+    const int* src;  // storage index of the cell's atoms (shared memory)
+    const R4* pos;
+    int2* ij;
+    double* nv;
+    int* count;
+    int cap;
+    int* err;
+    template <class RR> __host__ __device__ void accept(uint32_t i, uint32_t j, RR nx, RR ny, RR nz) {
+#if defined(__CUDA_ARCH__)
+        const int slot = atomicAdd(count, 1);
+        if (slot < cap) {
+            ij[slot] = make_int2((int)lane_to_u32(pos[src[i]].w), (int)lane_to_u32(pos[src[j]].w));
+            nv[3 * slot] = (double)nx;
+            nv[3 * slot + 1] = (double)ny;
+            nv[3 * slot + 2] = (double)nz;
+        } else {
+            atomicOr(err, EB_LOG_FULL);
+        }
+#endif
+    }
+};
+
 // ---------------------------------------------------------------------------------------------
 // step_pass: the timestep of one tile.
 // Shared memory per tile: velocities (R4, the collide works on them in place), old cell and
@@ -255,7 +287,7 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
         if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_CELL_FULL);
         for (int t = threadIdx.x; t < L && tb + t < nprev; t += BLOCK) {
             int s = A.src_in[tb + t];
-            s = (s >= 0 && s < nprev) ? s : 0;
+            s = (s >= 0 && s < A.capacity) ? s : 0;
             const R4 q = A.pos_in[s];
             atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
             A.keys[tb + t] = make_int2(-1, KIND_LOST);
@@ -271,10 +303,12 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
     const int step = A.ctl->step[p];
     const R cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
 
-    // phase 1: gather the tile's velocities into shared memory, old cell of every atom
+    // phase 1: gather the tile's velocities into shared memory, old cell of every atom.  src
+    // values index the buffer the previous step wrote, which held the atoms before that step's
+    // losses: they are bounded by the capacity, not by the current count.
     for (int t = threadIdx.x; t < L; t += BLOCK) {
         int s = A.src_in[tb + t];
-        if (s < 0 || s >= nprev) {
+        if (s < 0 || s >= A.capacity) {
             atomicOr(&A.ctl->err, EB_INCONSISTENT);
             s = 0;
         }
@@ -299,8 +333,14 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
             }
             if (n < 2) continue;
             R svm = A.sigvrmax[c];
-            CollideResult<R> cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                      (uint32_t)step, A.seed);
+            CollideResult<R> cr;
+            if (A.clog_ij) {
+                TileCollisionLog<R> lg{s_src + t, A.pos_in, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
+                cr = collide_cell<R, R4, TileCollisionLog<R>>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                               (uint32_t)step, A.seed, &lg);
+            } else {
+                cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
+            }
             A.sigvrmax[c] = svm;
             my_coll += cr.accepted;
             my_cand += cr.candidates;
@@ -719,6 +759,11 @@ __global__ void __launch_bounds__(256) finalize(Args<R> A) {
         if (k == 0 && !INIT) {
             A.ctl->step[1 - p] = step_now + 1;
             A.ctl->movers = 0;
+            if (A.clog_off) {
+                const int rel = step_now + 1 - A.clog_step0;
+                const int cnt = *A.clog_count;
+                if (rel >= 1 && rel <= A.clog_steps) A.clog_off[rel] = cnt < A.clog_cap ? cnt : A.clog_cap;
+            }
         }
     }
 }

@@ -582,9 +582,15 @@ template <class R> struct CollideResult {
     int32_t candidates;
 };
 
-template <class R, class V4>
+// receives every accepted collision (cell-local indices i, j and the direction n^); the
+// default records nothing
+struct NoCollisionLog {
+    template <class R> DSMC_HD void accept(uint32_t, uint32_t, R, R, R) {}
+};
+
+template <class R, class V4, class Log = NoCollisionLog>
 DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPhys<R>& P,
-                                      uint32_t local_cell, uint32_t step, uint64_t seed) {
+                                      uint32_t local_cell, uint32_t step, uint64_t seed, Log* log = nullptr) {
     CollideResult<R> res;
     res.accepted = 0;
     res.candidates = 0;
@@ -626,6 +632,7 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
             vel[i] = vi;
             vel[j] = vj;
             res.accepted += 1;
+            if (log) log->accept(i, j, nx, ny, nz);
         }
     }
     res.candidates = ncand;

@@ -15,7 +15,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _abi
-from ._abi import CloudParams, Diag, RunParams, StateBuffers
+from ._abi import AdjParams, CloudParams, Diag, Grad, RunParams, StateBuffers
 
 _LIB = None
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdsmc_b200.so")
@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = (
     "dsmc_destroy", "dsmc_set_stream", "dsmc_init_cloud", "dsmc_step", "dsmc_synchronize",
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
-    "dsmc_launches_per_step",
+    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_export",
 )
 
 
@@ -67,6 +67,12 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_kernel_times": (i32, [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(i64), i32,
                                     C.POINTER(i32)]),
         "dsmc_launches_per_step": (i32, [vp]),
+        "dsmc_autotune": (i32, [vp, i32, C.POINTER(i32), C.POINTER(C.c_double)]),
+        "dsmc_adjoint_run": (i32, [vp, C.POINTER(AdjParams), C.POINTER(Grad)]),
+        "dsmc_adjoint_loss": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "dsmc_adjoint_export": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, C.POINTER(i32), i64,
+                                      C.POINTER(i32), C.POINTER(C.c_double), i64, C.POINTER(i64), C.POINTER(i64),
+                                      C.POINTER(i32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -208,3 +214,43 @@ class Simulation:
 
     def launches_per_step(self) -> int:
         return int(self.lib.dsmc_launches_per_step(self._h))
+
+    # -- pathwise adjoint -----------------------------------------------------------------------------
+    def adjoint_run(self, steps: int, checkpoint_every: int = 100, precision: int = _abi.FP64,
+                    sigmoid_width_kT: float = 0.2) -> dict:
+        """Runs `steps` physical steps recording the collisions, then the smoothed loss and its
+        gradient w.r.t. (B', B0, knife knots); see dsmc_adjoint_run in include/dsmc.h."""
+        p = AdjParams(int(steps), int(checkpoint_every), int(precision), 0, float(sigmoid_width_kT))
+        g = Grad()
+        self._check(self.lib.dsmc_adjoint_run(self._h, C.byref(p), C.byref(g)))
+        return g.as_dict()
+
+    def adjoint_loss(self, theta=None, grad: bool = False):
+        """Smoothed loss of the recorded run at theta = (B', B0, eta_0..eta_8), same collisions."""
+        loss = C.c_double()
+        g = np.zeros(11, np.float64)
+        th = None if theta is None else np.ascontiguousarray(theta, np.float64)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.dsmc_adjoint_loss(self._h, dp(th) if th is not None else None, C.byref(loss),
+                                               dp(g) if grad else None))
+        return (loss.value, g) if grad else loss.value
+
+    def adjoint_export(self) -> dict:
+        na, nl, st = C.c_int64(), C.c_int64(), C.c_int32()
+        self._check(self.lib.dsmc_adjoint_export(self._h, None, None, 0, None, 0, None, None, 0, C.byref(na),
+                                                 C.byref(nl), C.byref(st)))
+        n, m, steps = na.value, nl.value, st.value
+        x0 = np.zeros((n, 3)); v0 = np.zeros((n, 3))
+        off = np.zeros(steps + 1, np.int32); ij = np.zeros((max(m, 1), 2), np.int32); nv = np.zeros((max(m, 1), 3))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._check(self.lib.dsmc_adjoint_export(self._h, dp(x0), dp(v0), n, ip(off), steps + 1, ip(ij), dp(nv),
+                                                 max(m, 1), C.byref(na), C.byref(nl), C.byref(st)))
+        return {"x0": x0, "v0": v0, "off": off, "ij": ij[:m], "n": nv[:m], "steps": steps}
+
+    def autotune(self, steps_per_candidate: int = 5) -> tuple[int, float]:
+        """Chooses the tile size by timing (advances the simulation); returns (tile, ms/step)."""
+        t = C.c_int32()
+        ms = C.c_double()
+        self._check(self.lib.dsmc_autotune(self._h, int(steps_per_candidate), C.byref(t), C.byref(ms)))
+        return int(t.value), float(ms.value)

@@ -199,4 +199,51 @@ DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, doubl
 /* Number of kernel launches one dsmc_step(h, 1) issues. */
 DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h);
 
+/* ---- pathwise adjoint ----------------------------------------------------------------------
+ * Gradient of a smoothed loss of the physical run with respect to the trap gradient B', the bias
+ * B0 and the knife knot heights eta_0..eta_8, with every random choice of the run held fixed.
+ * dsmc_adjoint_run, called right after dsmc_init_cloud on a one-cloud quadrupole handle, runs the
+ * physical simulation for `steps` steps recording every accepted collision (pair of atom ids,
+ * scattering direction), then evaluates the smoothed model -- all atoms kept, each with a
+ * survival weight multiplied every step by sigmoid((cut - E)/(width kB T0)) -- and its adjoint,
+ * checkpointed every `checkpoint_every` steps with per-segment recomputation.
+ * Loss: (sum w E / sum w) / (kB T0) + sum w / N0.  No counterpart in the reference. */
+typedef struct dsmc_adj_params {
+    int32_t steps;             /* physical steps recorded and differentiated */
+    int32_t checkpoint_every;  /* checkpoint interval K of the smoothed model */
+    int32_t precision;         /* DSMC_FP32 or DSMC_FP64 for the smoothed model and its adjoint */
+    int32_t reserved0;
+    double sigmoid_width_kT;   /* width of the survival sigmoid in units of kB T0 */
+} dsmc_adj_params;
+
+typedef struct dsmc_grad {
+    double loss;               /* mean_energy_kT + retained_fraction */
+    double mean_energy_kT;     /* sum w E / sum w / (kB T0) after the last step */
+    double retained_fraction;  /* sum w / N0 */
+    double dL_dBp;             /* d loss / d B' (per T/m) */
+    double dL_dB0;             /* d loss / d bias (per T) */
+    double dL_deta[9];         /* d loss / d knot height */
+    int64_t collisions;        /* collision events recorded */
+    double ms_record;          /* device time of the recorded physical run */
+    double ms_forward;         /* device time of the smoothed forward pass */
+    double ms_backward;        /* device time of the recomputation + adjoint pass */
+} dsmc_grad;
+
+DSMC_API dsmc_status dsmc_adjoint_run(dsmc_handle* h, const dsmc_adj_params* p, dsmc_grad* out);
+/* Smoothed loss of the recorded run at theta = (B', B0, eta_0..eta_8) (NULL: the run's own
+ * parameters); grad (11 doubles, may be NULL) receives its gradient.  Same recorded collisions:
+ * central differences of this function are common-random-number finite differences. */
+DSMC_API dsmc_status dsmc_adjoint_loss(dsmc_handle* h, const double* theta, double* loss, double* grad);
+/* The recorded run: initial positions and velocities by atom id (3 doubles each), per-step
+ * offsets (steps + 1), collision pairs (2 ints) and directions (3 doubles).  NULL buffers skip. */
+DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0, int64_t atoms_cap, int32_t* off,
+                                         int64_t off_cap, int32_t* ij, double* nv, int64_t log_cap,
+                                         int64_t* n_atoms, int64_t* n_log, int32_t* steps);
+
+/* Autotuner: times dsmc_step for each candidate tile size (atoms per tile, 128..CAP/2) over
+ * steps_per_candidate steps and keeps the fastest; the simulation advances meanwhile (results do
+ * not depend on the tiling).  Replaces no reference interface (the reference launches with
+ * cudaOccupancyMaxPotentialBlockSize or 256*SMs x 512, CUDADSMC/src/main.cu:389-406). */
+DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, int32_t* tile_atoms,
+                                   double* ms_per_step);
 #endif /* DSMC_B200_H */

@@ -48,6 +48,10 @@ def load() -> C.CDLL:
             "oracle_math_d": (None, [i32, C.POINTER(C.c_double), C.POINTER(C.c_double), i64]),
             "oracle_field_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), i64]),
+            "oracle_smooth_loss": (C.c_double, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
+                                                C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, i32,
+                                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double), i32]),
             "oracle_advance_atoms_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                              i64, i32]),
@@ -106,6 +110,23 @@ def advance_atoms(run: RunParams, cloud: CloudParams, pos, vel, psi, nsteps: int
     load().oracle_advance_atoms_d(C.byref(run), C.byref(cloud), dp(pos), dp(vel), dp(psi),
                                   fate.ctypes.data_as(C.POINTER(C.c_int32)), pos.shape[0], int(nsteps))
     return pos, vel, psi, fate
+
+
+def smooth_loss(run, cloud, theta, width_kT, x, v, steps, log_off, log_ij, log_n, grad=False, fp64=True):
+    """Smoothed-knife loss of the recorded run and, with grad=True, its gradient (B', B0, knots)."""
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    theta = np.ascontiguousarray(theta, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    v = np.ascontiguousarray(v, np.float64)
+    off = np.ascontiguousarray(log_off, np.int32)
+    ij = np.ascontiguousarray(log_ij, np.int32)
+    ln = np.ascontiguousarray(log_n, np.float64)
+    g = np.zeros(11, np.float64)
+    loss = load().oracle_smooth_loss(C.byref(run), C.byref(cloud), dp(theta), float(width_kT), dp(x), dp(v),
+                                     x.shape[0], int(steps), ip(off), ip(ij), dp(ln),
+                                     dp(g) if grad else None, 1 if fp64 else 0)
+    return (loss, g) if grad else loss
 
 
 def max_threads() -> int:

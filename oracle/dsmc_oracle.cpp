@@ -524,3 +524,116 @@ OAPI int oracle_advance_atoms_d(const dsmc_params* run, const dsmc_cloud_params*
     }
     return 0;
 }
+
+// ---- smoothed model (gradient path) ---------------------------------------------------------
+// theta = (B', B0, eta_0 .. eta_8); x, v: n x 3 in atom-id order; log_off: steps + 1 offsets into
+// the recorded collisions (pairs log_ij, directions log_n).  Returns the smoothed loss and, if
+// grad is not null, its gradient by the hand-written adjoint (all states stored, serial).
+#include "dsmc_adjoint.h"
+
+namespace {
+template <class R>
+SmoothConsts<R> smooth_consts(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT) {
+    const double kB = run_kB(run);
+    SmoothConsts<R> C;
+    C.Bp = (R)theta[0];
+    C.B0 = (R)theta[1];
+    C.B_floor = (R)0;
+    C.dt = (R)run.dt;
+    C.half_dt = (R)(0.5 * run.dt);
+    C.accel_scale = (R)(c.moment / c.mass);
+    C.kappa = (R)(2.0 * c.moment / c.mass);
+    C.inv_width = (R)(1.0 / (2.0 * width_kT * kB * c.temperature / c.mass));
+    C.cut_scale = 2.0 * kB * c.temperature / c.mass;
+    return C;
+}
+
+template <class R>
+double smooth_run(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT,
+                  const double* x0, const double* v0, int64_t n, int steps, const int* off, const int* ij,
+                  const double* ln, double* grad) {
+    const SmoothConsts<R> C = smooth_consts<R>(run, c, theta, width_kT);
+    const int nk = c.knife_nknots;
+    const double kB = run_kB(run);
+    std::vector<R> x(3 * n), v(3 * n), w(n, R(1)), e(n);
+    for (int64_t i = 0; i < 3 * n; ++i) { x[i] = (R)x0[i]; v[i] = (R)v0[i]; }
+    const bool keep = grad != nullptr;
+    std::vector<R> xs, vs, ws, vpre;  // per step: start x, post-collision v, start w; pre-collision pairs
+    if (keep) { xs.resize((size_t)steps * 3 * n); vs.resize((size_t)steps * 3 * n); ws.resize((size_t)steps * n);
+                vpre.resize((size_t)off[steps] * 6); }
+    std::vector<double> cuts(steps);
+    for (int t = 0; t < steps; ++t) {
+        for (int k = off[t]; k < off[t + 1]; ++k) {
+            R* vi = &v[3 * ij[2 * k]];
+            R* vj = &v[3 * ij[2 * k + 1]];
+            if (keep) for (int a = 0; a < 3; ++a) { vpre[6 * k + a] = vi[a]; vpre[6 * k + 3 + a] = vj[a]; }
+            const R nn[3] = {(R)ln[3 * k], (R)ln[3 * k + 1], (R)ln[3 * k + 2]};
+            collide_fixed(vi, vj, nn);
+        }
+        const double eta = knife_eta(nk, c.knife_step, theta + 2, (double)t);
+        const R cut = (R)(C.cut_scale * eta);
+        cuts[t] = (double)cut;
+        if (keep) {
+            memcpy(&xs[(size_t)t * 3 * n], x.data(), 3 * n * sizeof(R));
+            memcpy(&vs[(size_t)t * 3 * n], v.data(), 3 * n * sizeof(R));
+            memcpy(&ws[(size_t)t * n], w.data(), n * sizeof(R));
+        }
+        for (int64_t i = 0; i < n; ++i) e[i] = smooth_step(C, cut, &x[3 * i], &v[3 * i], w[i]);
+    }
+    i128 W = 0, S = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        W += fx_from((double)w[i]);
+        S += fx_from((double)w[i] * (double)e[i]);
+    }
+    const double Wd = fx_to_double(W), Sd = fx_to_double(S), kT = kB * c.temperature;
+    const double loss = 0.5 * c.mass * Sd / Wd / kT + Wd / (double)n;
+    if (!keep) return loss;
+    // adjoint seeds at the final state
+    std::vector<R> xb(3 * n), vb(3 * n), wb(n);
+    double th[ADJ_NPARAM] = {0};
+    for (int64_t i = 0; i < n; ++i) {
+        const double dLdw = 0.5 * c.mass * ((double)e[i] / Wd - Sd / (Wd * Wd)) / kT + 1.0 / (double)n;
+        const double dLde = 0.5 * c.mass * (double)w[i] / (Wd * kT);
+        QuadField<R> f;
+        quad_field(C.Bp, C.B0, x[3 * i], x[3 * i + 1], x[3 * i + 2], true, f);
+        for (int a = 0; a < 3; ++a) {
+            xb[3 * i + a] = (R)(dLde * (double)C.kappa * (double)f.g[a]);
+            vb[3 * i + a] = (R)(dLde * 2.0 * (double)v[3 * i + a]);
+        }
+        wb[i] = (R)dLdw;
+        th[0] += dLde * (double)C.kappa * (double)f.dabs_dBp;
+        th[1] += dLde * (double)C.kappa * (double)f.dabs_dB0;
+    }
+    for (int t = steps - 1; t >= 0; --t) {
+        const R cut = (R)cuts[t];
+        double cutb_sum = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            R tb[2] = {0, 0};
+            R cb = 0;
+            smooth_step_adjoint(C, cut, &xs[(size_t)t * 3 * n + 3 * i], &vs[(size_t)t * 3 * n + 3 * i],
+                                ws[(size_t)t * n + i], &xb[3 * i], &vb[3 * i], wb[i], tb, cb);
+            th[0] += (double)tb[0];
+            th[1] += (double)tb[1];
+            cutb_sum += (double)cb;
+        }
+        int k0;
+        double f;
+        knot_weights(nk, c.knife_step, (double)t, &k0, &f);
+        th[2 + k0] += cutb_sum * C.cut_scale * (1.0 - f);
+        if (f != 0.0) th[2 + k0 + 1] += cutb_sum * C.cut_scale * f;
+        for (int k = off[t + 1] - 1; k >= off[t]; --k) {
+            const R nn[3] = {(R)ln[3 * k], (R)ln[3 * k + 1], (R)ln[3 * k + 2]};
+            collide_fixed_adjoint(&vpre[6 * k], &vpre[6 * k + 3], nn, &vb[3 * ij[2 * k]], &vb[3 * ij[2 * k + 1]]);
+        }
+    }
+    for (int p = 0; p < ADJ_NPARAM; ++p) grad[p] = th[p];
+    return loss;
+}
+}  // namespace
+
+OAPI double oracle_smooth_loss(const dsmc_params* run, const dsmc_cloud_params* c, const double* theta,
+                               double width_kT, const double* x, const double* v, int64_t n, int steps,
+                               const int* off, const int* ij, const double* ln, double* grad, int fp64) {
+    if (fp64) return smooth_run<double>(*run, *c, theta, width_kT, x, v, n, steps, off, ij, ln, grad);
+    return smooth_run<float>(*run, *c, theta, width_kT, x, v, n, steps, off, ij, ln, grad);
+}

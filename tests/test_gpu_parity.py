@@ -252,3 +252,20 @@ def test_cell_too_full_fails_loudly():
         d = sim.diagnostics()
         if d["error"]:
             raise DSMCError(5, "error bits set")
+
+
+def test_autotune_changes_speed_not_results():
+    # the tiling is a performance choice only: after the autotuner has stepped with every tile
+    # size the state is bit-identical to the oracle's after the same number of steps
+    run, c = scaled(2, n=60000, cells=32, flags=ALL, alpha=4000.0)
+    sim = Simulation(run, c)
+    orc = oracle.Oracle(run, c)
+    sim.init_cloud(17)
+    orc.init_cloud(17)
+    tile, ms = sim.autotune(2)
+    assert 128 <= tile <= 1024 and ms > 0
+    orc.step(sim.diagnostics()["step"])
+    assert_same(sim, orc)
+    sim.step(3)
+    orc.step(3)
+    assert_same(sim, orc)
