@@ -26,7 +26,7 @@ DRIVER_BIN = os.path.join(PKG_DIR, "dsmc_driver")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "build", "liboracle.so")
 
-ENGINE_SOURCES = ["dsmc_engine.cu"]
+ENGINE_SOURCES = ["dsmc_engine.cu", "dsmc_noalloc.cu"]
 ENGINE_HEADERS = ["dsmc_kernels.cuh", "dsmc_physics.h", "dsmc_setup.h"]
 
 NVCC_FLAGS = [

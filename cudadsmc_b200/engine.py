@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = (
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
     "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_export",
+    "dsmc_sort_cells_noalloc",
 )
 
 
@@ -73,6 +74,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_adjoint_export": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, C.POINTER(i32), i64,
                                       C.POINTER(i32), C.POINTER(C.c_double), i64, C.POINTER(i64), C.POINTER(i64),
                                       C.POINTER(i32)]),
+        "dsmc_sort_cells_noalloc": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), vp, i64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -246,4 +246,21 @@ DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0,
  * cudaOccupancyMaxPotentialBlockSize or 256*SMs x 512, CUDADSMC/src/main.cu:389-406). */
 DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, int32_t* tile_atoms,
                                    double* ms_per_step);
+
+/* Sorts the n atoms of one cloud by cell without allocating any memory.  No counterpart in the
+ * reference: it serves callers whose device memory is owned by another allocator (a PyTorch
+ * process, for example), for whom cudaMalloc can fail on memory the pool is holding, and
+ * cudaMalloc / cudaFree would synchronise the whole device.  Inputs and outputs are device
+ * pointers on the current device: pos_dev holds n x 4 reals (float for DSMC_FP32, double for
+ * DSMC_FP64; x, y, z used), order_dev receives n indices (order_dev[j] = input index of the atom
+ * in sorted position j, stable by (cell, input index)), cell_start_dev receives
+ * cells[0]*cells[1]*cells[2] + 2 ints (start of every grid cell, then of the overflow cell, then n).
+ * Work is enqueued on cuda_stream.  Scratch lives in a fixed device array of about 6.3 MB inside
+ * the library: at most 262144 atoms and 262144 grid cells per call (DSMC_ERR_CAPACITY beyond).
+ * The first call on a device looks up that array's address (make it before any stream capture);
+ * every call shares the array, so calls that overlap on the GPU race and must be serialised. */
+DSMC_API dsmc_status dsmc_sort_cells_noalloc(const dsmc_params* run, const dsmc_cloud_params* cloud,
+                                             const void* pos_dev, int64_t n, int32_t* order_dev,
+                                             int32_t* cell_start_dev, void* cuda_stream);
+
 #endif /* DSMC_B200_H */
