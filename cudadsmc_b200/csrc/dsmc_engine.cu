@@ -50,6 +50,18 @@ template <class T> struct DevBuf {
 
 constexpr int kMinTile = 128;  // smallest tile the autotuner tries (sizes the tile tables)
 
+// launch shape of the FP32 step_pass: threads per tile, atoms staged per tile (48 B + 4 B of
+// shared memory each), blocks per SM requested from the compiler
+#ifndef DSMC_FP32_BLOCK
+#define DSMC_FP32_BLOCK 256
+#endif
+#ifndef DSMC_FP32_CAP
+#define DSMC_FP32_CAP 1024
+#endif
+#ifndef DSMC_FP32_MINB
+#define DSMC_FP32_MINB 4
+#endif
+
 const char* kKernelNames[] = {"step_pass",   "scan_reduce", "scan_top",     "scan_down",
                               "mover_place", "mover_rank",  "permute_pass", "finalize"};
 constexpr int kNumStepKernels = 8;
@@ -80,7 +92,8 @@ struct dsmc_handle {
 
 namespace {
 
-template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
+// BLOCK threads per step_pass tile, CAP atoms staged per tile, MINB blocks per SM requested
+template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_handle {
     typedef typename V4T<R>::type R4;
     // configuration
     dsmc_params run{};
@@ -136,8 +149,8 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
-        smem_tile = (size_t)CAP * (sizeof(R4) + 2 * sizeof(int));
-        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int));
+        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         build_args();
     }
@@ -248,14 +261,14 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0: step_pass<R, BLOCK, CAP><<<max_tiles, BLOCK, smem_tile, stream>>>(A); break;
+        case 0: step_pass<R, BLOCK, CAP, MINB><<<max_tiles, BLOCK, smem_tile, stream>>>(A); break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
         case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 4: mover_place<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         case 5: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         case 6: permute_pass<R, 256, CAP><<<max_tiles, 256, 0, stream>>>(A); break;
-        case 7: finalize<R, false><<<nclouds, 256, 0, stream>>>(A); break;
+        case 7: finalize<R, false><<<nclouds, 512, 0, stream>>>(A); break;
         }
     }
 
@@ -374,7 +387,7 @@ template <class R, int BLOCK, int CAP> struct Engine final : dsmc_handle {
         parity = 0;
         // step counter and diagnostics of the sorted state
         measure_tiles<R, 256><<<max_tiles, 256, 0, stream>>>(args[0]);
-        finalize<R, true><<<nclouds, 256, 0, stream>>>(args[0]);
+        finalize<R, true><<<nclouds, 512, 0, stream>>>(args[0]);
         CU(cudaGetLastError());
         CU(cudaStreamSynchronize(stream));
         initialised = true;
@@ -891,9 +904,9 @@ DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params
             return DSMC_ERR_CUDA;
         }
         if (run->precision == DSMC_FP32)
-            *out = new Engine<float, 256, 2048>(*run, clouds, nclouds);
+            *out = new Engine<float, DSMC_FP32_BLOCK, DSMC_FP32_CAP, DSMC_FP32_MINB>(*run, clouds, nclouds);
         else if (run->precision == DSMC_FP64)
-            *out = new Engine<double, 256, 1024>(*run, clouds, nclouds);
+            *out = new Engine<double, 256, 1024, 2>(*run, clouds, nclouds);
         else {
             g_create_error = "precision must be DSMC_FP32 or DSMC_FP64";
             return DSMC_ERR_INVALID;

@@ -231,8 +231,7 @@ __device__ __forceinline__ R knife_cut_for(const CloudPhys<R>& P, double T, int 
 // records accepted collisions of one cell: the atom ids of the pair and the direction n^
 template <class R> struct TileCollisionLog {
     typedef typename V4T<R>::type R4;
-    const int* src;  // storage index of the cell's atoms (shared memory)
-    const R4* pos;
+    const R4* pos;   // the cell's staged positions (shared memory; atom id in the fourth lane)
     int2* ij;
     double* nv;
     int* count;
@@ -242,7 +241,7 @@ template <class R> struct TileCollisionLog {
 #if defined(__CUDA_ARCH__)
         const int slot = atomicAdd(count, 1);
         if (slot < cap) {
-            ij[slot] = make_int2((int)lane_to_u32(pos[src[i]].w), (int)lane_to_u32(pos[src[j]].w));
+            ij[slot] = make_int2((int)lane_to_u32(pos[i].w), (int)lane_to_u32(pos[j].w));
             nv[3 * slot] = (double)nx;
             nv[3 * slot + 1] = (double)ny;
             nv[3 * slot + 2] = (double)nz;
@@ -253,18 +252,35 @@ template <class R> struct TileCollisionLog {
     }
 };
 
+// 16-byte asynchronous global -> shared copies (cp.async, L2 only); a gather, unlike TMA
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src) {
+#pragma unroll
+    for (int o = 0; o < (int)sizeof(R4); o += 16)
+        cp_async16(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o);
+}
+
 // ---------------------------------------------------------------------------------------------
 // step_pass: the timestep of one tile.
-// Shared memory per tile: velocities (R4, the collide works on them in place), old cell and
-// storage index of each position, CAP positions.
+// The tile's atoms are gathered through src into shared memory with asynchronous 16-byte copies
+// issued all at once (positions, velocities, spinors: CAP x 3 x R4), then the cells collide and
+// every atom moves straight from shared memory; only the new state, the keys and the counters
+// go back to global memory.
 // ---------------------------------------------------------------------------------------------
-template <class R, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
+template <class R, int BLOCK, int CAP, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     typedef typename V4T<R>::type R4;
+    constexpr int PER = CAP / BLOCK;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R4* s_vel = reinterpret_cast<R4*>(smem_raw);
-    int* s_cell = reinterpret_cast<int*>(s_vel + CAP);
-    int* s_src = s_cell + CAP;
+    R4* s_pos = reinterpret_cast<R4*>(smem_raw);
+    R4* s_vel = s_pos + CAP;
+    R4* s_psi = s_vel + CAP;
+    int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
     __shared__ CloudPhys<R> P;
     __shared__ TilePartial red[BLOCK / 32];
 
@@ -303,18 +319,33 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
     const int step = A.ctl->step[p];
     const R cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
 
-    // phase 1: gather the tile's velocities into shared memory, old cell of every atom.  src
-    // values index the buffer the previous step wrote, which held the atoms before that step's
-    // losses: they are bounded by the capacity, not by the current count.
-    for (int t = threadIdx.x; t < L; t += BLOCK) {
-        int s = A.src_in[tb + t];
-        if (s < 0 || s >= A.capacity) {
-            atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            s = 0;
+    // phase 1: all storage indices, then all gathers in flight at once.  src values index the
+    // buffer the previous step wrote, which held the atoms before that step's losses: they are
+    // bounded by the capacity, not by the current count.
+    int sidx[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int t = threadIdx.x + k * BLOCK;
+        sidx[k] = t < L ? A.src_in[tb + t] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int t = threadIdx.x + k * BLOCK;
+        if (t < L) {
+            int s = sidx[k];
+            if (s < 0 || s >= A.capacity) {
+                atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                s = 0;
+            }
+            stage(s_pos + t, A.pos_in + s);
+            stage(s_vel + t, A.vel_in + s);
+            stage(s_psi + t, A.psi_in + s);
         }
-        const R4 q = A.pos_in[s];
-        s_src[t] = s;
-        s_vel[t] = A.vel_in[s];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int t = threadIdx.x; t < L; t += BLOCK) {
+        const R4 q = s_pos[t];
         s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
     }
     __syncthreads();
@@ -335,7 +366,7 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
             R svm = A.sigvrmax[c];
             CollideResult<R> cr;
             if (A.clog_ij) {
-                TileCollisionLog<R> lg{s_src + t, A.pos_in, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
+                TileCollisionLog<R> lg{s_pos + t, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
                 cr = collide_cell<R, R4, TileCollisionLog<R>>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
                                                                (uint32_t)step, A.seed, &lg);
             } else {
@@ -365,10 +396,9 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
         int c_old = 0;
         R4 q, v, s;
         if (valid) {
-            const int sidx = s_src[t];
-            q = A.pos_in[sidx];
-            s = A.psi_in[sidx];
+            q = s_pos[t];
             v = s_vel[t];
+            s = s_psi[t];
             a.x = q.x; a.y = q.y; a.z = q.z;
             a.vx = v.x; a.vy = v.y; a.vz = v.z;
             a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
@@ -417,13 +447,13 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
                 A.vel_out[j] = vo;
                 A.psi_out[j] = so;
                 acc.n_alive += 1;
-                acc.sum_v2 += fx_from((double)o.v2);
-                acc.sum_B += fx_from((double)o.absB);
+                acc.sum_v2 += fx_from(o.v2);
+                acc.sum_B += fx_from(o.absB);
                 A.keys[j] = stayer ? make_int2(c_old, KIND_STAY) : make_int2(slot, KIND_MOVE);
                 if (stayer && c_old == P.ovf_cell) ovf_stayers += 1;
             } else {
-                acc.evap_v2 += fx_from((double)o.v2);
-                acc.evap_B += fx_from((double)o.absB);
+                acc.evap_v2 += fx_from(o.v2);
+                acc.evap_B += fx_from(o.absB);
                 if (o.fate == FATE_MAJORANA) acc.n_maj += 1;
                 else acc.n_knife += 1;
                 A.keys[j] = make_int2(-1, KIND_LOST);
@@ -446,6 +476,7 @@ __global__ void __launch_bounds__(BLOCK, 3) step_pass(Args<R> A) {
 // ---------------------------------------------------------------------------------------------
 template <class R, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
+    constexpr int K = CAP / BLOCK;  // positions per thread, a contiguous run
     __shared__ uint32_t s_pre[CAP];
     __shared__ uint32_t wsum[32];
     const int p = A.parity;
@@ -457,39 +488,45 @@ __global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
     if (L > CAP || L < 0) return;  // step_pass marked every atom of such a tile as lost
     const int cloud = A.tile_cloud[b];
     const int carry_base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
-    uint32_t carry = 0;
-    for (int base = 0; base < L; base += BLOCK) {
-        const int t = base + threadIdx.x;
-        const bool valid = t < L;
-        int2 key = make_int2(-1, KIND_LOST);
-        if (valid) key = A.keys[tb + t];
-        const bool stayer = valid && key.y == KIND_STAY;
-        uint32_t tot;
-        const uint32_t ex = block_excl_scan_u32<BLOCK>(stayer ? 1u : 0u, wsum, tot) + carry;
-        carry += tot;
-        if (valid) s_pre[t] = ex;
-        __syncthreads();
-        if (valid) {
-            int dest = -1;
-            if (stayer) {
-                const int c = key.x;
-                const int seg = A.old_start[c];
-                const int sl = seg > tb ? seg - tb : 0;
-                if (sl <= t) {
-                    int rank = (int)(ex - s_pre[sl]);
-                    if (seg < tb) rank += carry_base;
-                    dest = A.new_start[c] + rank;
-                    if (dest < A.new_start[c] || dest >= A.new_start[c + 1]) dest = -2;
-                } else {
-                    dest = -2;
-                }
-            } else if (key.y == KIND_MOVE) {
-                dest = (key.x >= 0 && key.x < A.capacity) ? A.mrec[key.x].w : -2;
-                if (dest < 0 || dest >= A.capacity) dest = -2;
+    const int t0 = threadIdx.x * K;
+    int2 key[K];
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        key[k] = (t0 + k < L) ? A.keys[tb + t0 + k] : make_int2(-1, KIND_LOST);
+        mine += (key[k].y == KIND_STAY) ? 1u : 0u;
+    }
+    uint32_t tot;
+    uint32_t run = block_excl_scan_u32<BLOCK>(mine, wsum, tot);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (t0 + k < L) s_pre[t0 + k] = run;
+        run += (key[k].y == KIND_STAY) ? 1u : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int t = t0 + k;
+        if (t >= L) break;
+        int dest = -1;
+        if (key[k].y == KIND_STAY) {
+            const int c = key[k].x;
+            const int seg = A.old_start[c];
+            const int sl = seg > tb ? seg - tb : 0;
+            if (sl <= t) {
+                int rank = (int)(s_pre[t] - s_pre[sl]);
+                if (seg < tb) rank += carry_base;
+                dest = A.new_start[c] + rank;
+                if (dest < A.new_start[c] || dest >= A.new_start[c + 1]) dest = -2;
+            } else {
+                dest = -2;
             }
-            if (dest >= 0) A.src_out[dest] = tb + t;
-            else if (dest == -2) atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        } else if (key[k].y == KIND_MOVE) {
+            dest = (key[k].x >= 0 && key[k].x < A.capacity) ? A.mrec[key[k].x].w : -2;
+            if (dest < 0 || dest >= A.capacity) dest = -2;
         }
+        if (dest >= 0) A.src_out[dest] = tb + t;
+        else if (dest == -2) atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
 
@@ -578,8 +615,9 @@ __global__ void __launch_bounds__(1024) scan_top(Args<R> A) {
         A.new_start[A.total_cells] = total;
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
     }
-    // 3. cloud of every next tile: binary search of the per-cloud first tiles
-    for (int t = threadIdx.x; t < ntiles_next && t < A.max_tiles; t += 1024) {
+    // 3. cloud of every next tile: binary search of the per-cloud first tiles (a one-cloud
+    //    handle's table is all zeros from the start)
+    for (int t = threadIdx.x; A.nclouds > 1 && t < ntiles_next && t < A.max_tiles; t += 1024) {
         int lo = 0, hi = A.nclouds;  // largest k with tile_off[k] <= t and ntiles[k] > 0
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -710,15 +748,16 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
 
 // per-cloud diagnostics from the tile partials; block k handles cloud k
 template <class R, bool INIT>
-__global__ void __launch_bounds__(256) finalize(Args<R> A) {
-    __shared__ TilePartial red[8];
+__global__ void __launch_bounds__(512) finalize(Args<R> A) {
+    __shared__ TilePartial red[32];
     const int p = A.parity;
     const int k = blockIdx.x;
     CloudDyn& d = A.cdyn[k];
     const int t0 = d.tile_off[p], nt = d.ntiles[p];
     TilePartial acc;
     zero_partial(acc);
-    for (int j = threadIdx.x; j < nt; j += 256) {
+#pragma unroll 4
+    for (int j = threadIdx.x; j < nt; j += 512) {
         const TilePartial& t = A.partials[t0 + j];
         acc.sum_v2 += t.sum_v2;
         acc.sum_B += t.sum_B;
@@ -730,7 +769,7 @@ __global__ void __launch_bounds__(256) finalize(Args<R> A) {
         acc.coll += t.coll;
         acc.cand += t.cand;
     }
-    block_reduce_partial<256>(acc, red);
+    block_reduce_partial<512>(acc, red);
     if (threadIdx.x == 0) {
         const CloudPhys<R>& P = A.clouds[k];
         CloudDiagDev& g = A.cdiag[k];
@@ -790,8 +829,8 @@ __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
         trap_field(P, q.x, q.y, q.z, f);
         const R v2 = v.x * v.x + v.y * v.y + v.z * v.z;
         acc.n_alive += 1;
-        acc.sum_v2 += fx_from((double)v2);
-        acc.sum_B += fx_from((double)f.absB);
+        acc.sum_v2 += fx_from(v2);
+        acc.sum_B += fx_from(f.absB);
     }
     block_reduce_partial<BLOCK>(acc, red);
     if (threadIdx.x == 0) A.partials[b] = acc;

@@ -331,6 +331,17 @@ DSMC_HD i128 fx_from(double d) {
     uint64_t lo = (uint64_t)fr;
     return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
 }
+// the same value for a non-negative float, from its bits: f = M 2^(E-150) for the 24-bit
+// significand M, so f 2^64 = M 2^(E-86) -- a shift, no floating-point work
+DSMC_HD i128 fx_from(float f) {
+    const uint32_t u = f2u(f);
+    const int E = (int)(u >> 23);
+    if (E == 0) return 0;  // zero or subnormal: below 2^-64
+    const unsigned __int128 M = (unsigned __int128)((u & 0x7FFFFFu) | 0x800000u);
+    const int sh = E - 86;
+    if (sh > 100) return (i128)((unsigned __int128)1 << 124);  // beyond 2^38: not a physical v^2 or |B|
+    return (i128)(sh >= 0 ? (M << sh) : (sh > -24 ? (M >> -sh) : (unsigned __int128)0));
+}
 DSMC_HD double fx_to_double(i128 q) {
     int64_t hi = (int64_t)(q >> 64);
     uint64_t lo = (uint64_t)q;

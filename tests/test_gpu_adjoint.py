@@ -75,3 +75,18 @@ def test_fp32_adjoint_close_to_fp64():
     v32 = np.array([g32["dL_dBp"], g32["dL_dB0"]] + g32["dL_deta"])
     big = np.abs(v64) > 1e-3 * np.max(np.abs(v64))
     np.testing.assert_allclose(v32[big], v64[big], rtol=2e-2)
+
+
+def test_torch_autograd_function():
+    import torch
+    from cudadsmc_b200.autograd import smoothed_knife_loss
+    run, c = adjoint_cloud(n=10000, steps=120)
+    th = torch.tensor(theta_of(c), dtype=torch.float64, requires_grad=True)
+    loss = smoothed_knife_loss(th, run, c, steps=120, checkpoint_every=40, seed=5)
+    loss.backward()
+    sim = Simulation(run, c)
+    sim.init_cloud(5)
+    g = sim.adjoint_run(120, checkpoint_every=40)
+    assert loss.item() == g["loss"]
+    ref = np.array([g["dL_dBp"], g["dL_dB0"]] + g["dL_deta"])
+    np.testing.assert_allclose(th.grad.numpy(), ref, rtol=1e-9, atol=1e-14)
