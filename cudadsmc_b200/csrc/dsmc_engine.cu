@@ -115,7 +115,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<int4> mrec;
     DevBuf<int2> keys;
     DevBuf<R> sigvrmax;
-    DevBuf<TilePartial> partials;
+    DevBuf<CloudAccum> accum;
     DevBuf<CloudPhys<R>> d_phys;
     DevBuf<CloudDyn> cdyn;
     DevBuf<CloudDiagDev> cdiag;
@@ -135,6 +135,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     int64_t prof_n[kNumStepKernels] = {0};
     cudaEvent_t ev[kNumStepKernels + 1] = {};  // also reused by the autotuner and the adjoint (>= 4)
     size_t smem_tile = 0;
+    // resident blocks of the tile kernels on the whole device (their grid-stride loops cover
+    // any tile count, so a launch never needs more blocks than fit at once)
+    int resident_step = 0, resident_permute = 0, resident_measure = 0;
 
     Engine(const dsmc_params& r, const dsmc_cloud_params* clouds, int n) {
         run = r;
@@ -152,7 +155,23 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
+        int dev = 0, nsm = 0, occ = 0;
+        CU(cudaGetDevice(&dev));
+        CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB>, BLOCK, smem_tile));
+        resident_step = nsm * std::max(occ, 1);
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R, 256, CAP>, 256, 0));
+        resident_permute = nsm * std::max(occ, 1);
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, measure_tiles<R, 256>, 256, 0));
+        resident_measure = nsm * std::max(occ, 1);
         build_args();
+    }
+
+    // blocks for a tile kernel: no more than the tiles of a tiling of the current nominal size
+    // (a cloud of n atoms has at most n / T + 1 tiles) nor than fit on the device at once
+    int tile_grid(int resident) const {
+        const int bound = capacity / tile_nominal + nclouds + 2;
+        return std::max(1, std::min(bound, resident));
     }
 
     ~Engine() override {
@@ -205,7 +224,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         keys.alloc(capacity);
         tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles);
         sigvrmax.alloc(total_cells);
-        partials.alloc(max_tiles);
+        accum.alloc((size_t)nclouds * ACC_BUCKETS);
+        CU(cudaMemset(accum.p, 0, (size_t)nclouds * ACC_BUCKETS * sizeof(CloudAccum)));
         d_phys.alloc(nclouds);
         CU(cudaMemcpy(d_phys.p, phys.data(), nclouds * sizeof(CloudPhys<R>), cudaMemcpyHostToDevice));
         cdyn.alloc(nclouds); cdiag.alloc(nclouds); ctl.alloc(1);
@@ -245,7 +265,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p;
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
             A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
-            A.partials = partials.p;
+            A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.block_sums = block_sums.p; A.block_off = block_off.p;
             A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
@@ -261,14 +281,14 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0: step_pass<R, BLOCK, CAP, MINB><<<max_tiles, BLOCK, smem_tile, stream>>>(A); break;
+        case 0: step_pass<R, BLOCK, CAP, MINB><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A); break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
         case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 4: mover_place<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         case 5: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
-        case 6: permute_pass<R, 256, CAP><<<max_tiles, 256, 0, stream>>>(A); break;
-        case 7: finalize<R, false><<<nclouds, 512, 0, stream>>>(A); break;
+        case 6: permute_pass<R, 256, CAP><<<tile_grid(resident_permute), 256, 0, stream>>>(A); break;
+        case 7: finalize<R, false><<<nclouds, 32, 0, stream>>>(A); break;
         }
     }
 
@@ -386,8 +406,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaGetLastError());
         parity = 0;
         // step counter and diagnostics of the sorted state
-        measure_tiles<R, 256><<<max_tiles, 256, 0, stream>>>(args[0]);
-        finalize<R, true><<<nclouds, 512, 0, stream>>>(args[0]);
+        measure_tiles<R, 256><<<tile_grid(resident_measure), 256, 0, stream>>>(args[0]);
+        finalize<R, true><<<nclouds, 32, 0, stream>>>(args[0]);
         CU(cudaGetLastError());
         CU(cudaStreamSynchronize(stream));
         initialised = true;

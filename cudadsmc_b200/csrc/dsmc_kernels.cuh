@@ -53,6 +53,16 @@ struct __align__(16) TilePartial {
     long long n_alive, n_maj, n_knife, coll, cand, ovf_stayers, pad1, pad2;
 };
 
+// Per-cloud totals of one step, gathered in ACC_BUCKETS buckets per cloud (tile b adds into bucket
+// b mod ACC_BUCKETS) with 64-bit atomic adds whose results are not read.  Each 128-bit sum (all of
+// them non-negative, below 2^126) is split into three 42-bit limbs, so a bucket's limb sum cannot
+// wrap before 2^21 tiles.  finalize recombines and clears the buckets.
+constexpr int ACC_BUCKETS = 16;
+struct __align__(16) CloudAccum {
+    unsigned long long v2[3], B[3], ev2[3], eB[3];
+    unsigned long long n_alive, n_maj, n_knife, coll, cand, pad[3];
+};
+
 struct CloudDyn {
     int n[2];         // atoms, by parity
     int start[2];     // first atom index, by parity
@@ -103,7 +113,7 @@ template <class R> struct Args {
     int* tile_cloud_next;
     int* tile_ovf;
     int* tile_ovf_carry;
-    TilePartial* partials;
+    CloudAccum* accum;  // nclouds x ACC_BUCKETS
     const CloudPhys<R>* clouds;
     CloudDyn* cdyn;
     CloudDiagDev* cdiag;
@@ -173,6 +183,68 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
     return v;
 }
 
+// Exact warp sum of non-negative 128-bit values: five 26-bit limbs (the top one 24 bits), each
+// summed over the 32 lanes by redux.sync without overflow (32 x 2^26 < 2^32), recombined mod 2^128.
+__device__ __forceinline__ i128 warp_sum_u128_redux(i128 v) {
+    const unsigned long long lo = (unsigned long long)v;
+    const unsigned long long hi = (unsigned long long)((unsigned __int128)v >> 64);
+    constexpr unsigned M26 = (1u << 26) - 1u;
+    const unsigned s0 = __reduce_add_sync(0xffffffffu, (unsigned)lo & M26);
+    const unsigned s1 = __reduce_add_sync(0xffffffffu, (unsigned)(lo >> 26) & M26);
+    const unsigned s2 = __reduce_add_sync(0xffffffffu, (unsigned)((lo >> 52) | (hi << 12)) & M26);
+    const unsigned s3 = __reduce_add_sync(0xffffffffu, (unsigned)(hi >> 14) & M26);
+    const unsigned s4 = __reduce_add_sync(0xffffffffu, (unsigned)(hi >> 40));
+    const unsigned __int128 r = (unsigned __int128)s0 + ((unsigned __int128)s1 << 26) +
+                                ((unsigned __int128)s2 << 52) + ((unsigned __int128)s3 << 78) +
+                                ((unsigned __int128)s4 << 104);
+    return (i128)r;
+}
+
+// per-thread accumulators of step_pass and their block reduction into a TilePartial
+struct StepAcc {
+    i128 sum_v2, sum_B, evap_v2, evap_B;
+    unsigned n_alive, n_maj, n_knife, coll, cand, ovf_stayers;
+};
+__device__ __forceinline__ void zero_acc(StepAcc& a) {
+    a.sum_v2 = 0; a.sum_B = 0; a.evap_v2 = 0; a.evap_B = 0;
+    a.n_alive = 0; a.n_maj = 0; a.n_knife = 0; a.coll = 0; a.cand = 0; a.ovf_stayers = 0;
+}
+__device__ __forceinline__ void warp_reduce_acc(StepAcc& a) {
+    a.sum_v2 = warp_sum_u128_redux(a.sum_v2);
+    a.sum_B = warp_sum_u128_redux(a.sum_B);
+    if (__any_sync(0xffffffffu, (a.n_maj | a.n_knife) != 0u)) {  // only warps that lost atoms
+        a.evap_v2 = warp_sum_u128_redux(a.evap_v2);
+        a.evap_B = warp_sum_u128_redux(a.evap_B);
+    }
+    a.n_alive = __reduce_add_sync(0xffffffffu, a.n_alive);
+    a.n_maj = __reduce_add_sync(0xffffffffu, a.n_maj);
+    a.n_knife = __reduce_add_sync(0xffffffffu, a.n_knife);
+    a.coll = __reduce_add_sync(0xffffffffu, a.coll);
+    a.cand = __reduce_add_sync(0xffffffffu, a.cand);
+    a.ovf_stayers = __reduce_add_sync(0xffffffffu, a.ovf_stayers);
+}
+// every thread of the block calls; thread 0 receives the block total in `out`
+template <int BLOCK>
+__device__ __forceinline__ void block_reduce_acc(StepAcc& a, StepAcc* sm, TilePartial& out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = BLOCK / 32;
+    static_assert(NW <= 32, "one warp reduces the warp totals");
+    warp_reduce_acc(a);
+    if (lane == 0) sm[warp] = a;
+    __syncthreads();
+    if (warp == 0) {
+        StepAcc w;
+        if (lane < NW) w = sm[lane]; else zero_acc(w);
+        warp_reduce_acc(w);
+        if (lane == 0) {
+            out.sum_v2 = w.sum_v2; out.sum_B = w.sum_B; out.evap_v2 = w.evap_v2; out.evap_B = w.evap_B;
+            out.n_alive = w.n_alive; out.n_maj = w.n_maj; out.n_knife = w.n_knife;
+            out.coll = w.coll; out.cand = w.cand; out.ovf_stayers = w.ovf_stayers;
+            out.pad1 = 0; out.pad2 = 0;
+        }
+    }
+}
+
 // reduce 4 i128 + 5 int64 over the block into p (thread 0 holds the result)
 template <int BLOCK>
 __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial* sm) {
@@ -205,6 +277,30 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
         }
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ void add_limbs(unsigned long long* dst, i128 v) {
+    const unsigned __int128 u = (unsigned __int128)v;
+    constexpr unsigned long long M42 = (1ull << 42) - 1ull;
+    if (u == 0) return;
+    atomicAdd(dst, (unsigned long long)u & M42);
+    atomicAdd(dst + 1, (unsigned long long)(u >> 42) & M42);
+    atomicAdd(dst + 2, (unsigned long long)(u >> 84));
+}
+// one tile's totals into its cloud's bucket (one thread)
+__device__ __forceinline__ void accum_tile(CloudAccum* bucket, const TilePartial& t) {
+    add_limbs(bucket->v2, t.sum_v2);
+    add_limbs(bucket->B, t.sum_B);
+    add_limbs(bucket->ev2, t.evap_v2);
+    add_limbs(bucket->eB, t.evap_B);
+    if (t.n_alive) atomicAdd(&bucket->n_alive, (unsigned long long)t.n_alive);
+    if (t.n_maj) atomicAdd(&bucket->n_maj, (unsigned long long)t.n_maj);
+    if (t.n_knife) atomicAdd(&bucket->n_knife, (unsigned long long)t.n_knife);
+    if (t.coll) atomicAdd(&bucket->coll, (unsigned long long)t.coll);
+    if (t.cand) atomicAdd(&bucket->cand, (unsigned long long)t.cand);
+}
+__device__ __forceinline__ i128 from_limbs(const unsigned long long* l) {
+    return (i128)((unsigned __int128)l[0] + ((unsigned __int128)l[1] << 42) + ((unsigned __int128)l[2] << 84));
 }
 
 __device__ __forceinline__ void zero_partial(TilePartial& t) {
@@ -282,189 +378,193 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     R4* s_psi = s_vel + CAP;
     int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
     __shared__ CloudPhys<R> P;
-    __shared__ TilePartial red[BLOCK / 32];
+    __shared__ StepAcc red[BLOCK / 32];
+    __shared__ R s_cut;
 
     const int p = A.parity;
-    const int b = blockIdx.x;
-    if (b >= A.ctl->ntiles[p]) return;
-    const int tb = A.tile_begin[b];
-    const int te = A.tile_begin[b + 1];
-    const int L = te - tb;
-    const int cloud = A.tile_cloud[b];
+    const int ntiles = A.ctl->ntiles[p];
     const int nprev = A.ctl->n[p];
-    const int lane = threadIdx.x & 31;
-    load_cloud(P, A.clouds + cloud);
-    __syncthreads();
-    const bool box = (P.trap == TRAP_BOX);
-
-    if (L > CAP || L < 0 || te > nprev) {
-        // cannot stage this tile: every atom in it leaves the simulation (flagged), so the cell
-        // counts stay consistent and every later kernel only touches indices it computed itself
-        if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_CELL_FULL);
-        for (int t = threadIdx.x; t < L && tb + t < nprev; t += BLOCK) {
-            int s = A.src_in[tb + t];
-            s = (s >= 0 && s < A.capacity) ? s : 0;
-            const R4 q = A.pos_in[s];
-            atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
-            A.keys[tb + t] = make_int2(-1, KIND_LOST);
-        }
-        if (threadIdx.x == 0) {
-            TilePartial z;
-            zero_partial(z);
-            A.partials[b] = z;
-            A.tile_ovf[b] = 0;
-        }
-        return;
-    }
     const int step = A.ctl->step[p];
-    const R cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
+    const int lane = threadIdx.x & 31;
+    const bool collide_now = (step % A.collide_every) == 0;
+    int cur_cloud = -1;
 
-    // phase 1: all storage indices, then all gathers in flight at once.  src values index the
-    // buffer the previous step wrote, which held the atoms before that step's losses: they are
-    // bounded by the capacity, not by the current count.
-    int sidx[PER];
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int t = threadIdx.x + k * BLOCK;
-        sidx[k] = t < L ? A.src_in[tb + t] : 0;
-    }
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int t = threadIdx.x + k * BLOCK;
-        if (t < L) {
-            int s = sidx[k];
-            if (s < 0 || s >= A.capacity) {
-                atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                s = 0;
-            }
-            stage(s_pos + t, A.pos_in + s);
-            stage(s_vel + t, A.vel_in + s);
-            stage(s_psi + t, A.psi_in + s);
+    // tiles in a grid-stride loop: the launch size only sets how many tiles run at once
+    for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        const int tb = A.tile_begin[b];
+        const int te = A.tile_begin[b + 1];
+        const int L = te - tb;
+        const int cloud = A.tile_cloud[b];
+        if (cloud != cur_cloud) {  // block-uniform: the cloud's parameters and knife cut
+            load_cloud(P, A.clouds + cloud);
+            __syncthreads();
+            if (threadIdx.x == 0) s_cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
+            __syncthreads();
+            cur_cloud = cloud;
         }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    for (int t = threadIdx.x; t < L; t += BLOCK) {
-        const R4 q = s_pos[t];
-        s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
-    }
-    __syncthreads();
+        const bool box = (P.trap == TRAP_BOX);
 
-    // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles)
-    long long my_coll = 0, my_cand = 0;
-    if ((P.flags & F_COLLIDE) && (step % A.collide_every) == 0) {
+        if (L > CAP || L < 0 || te > nprev) {
+            // cannot stage this tile: every atom in it leaves the simulation (flagged), so the cell
+            // counts stay consistent and every later kernel only touches indices it computed itself
+            if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_CELL_FULL);
+            for (int t = threadIdx.x; t < L && tb + t < nprev; t += BLOCK) {
+                int s = A.src_in[tb + t];
+                s = (s >= 0 && s < A.capacity) ? s : 0;
+                const R4 q = A.pos_in[s];
+                atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
+                A.keys[tb + t] = make_int2(-1, KIND_LOST);
+            }
+            if (threadIdx.x == 0) A.tile_ovf[b] = 0;
+            continue;
+        }
+        const R cut = s_cut;
+
+        // phase 1: all storage indices, then all gathers in flight at once.  src values index the
+        // buffer the previous step wrote, which held the atoms before that step's losses: they are
+        // bounded by the capacity, not by the current count.
+        int sidx[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int t = threadIdx.x + k * BLOCK;
+            sidx[k] = t < L ? A.src_in[tb + t] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int t = threadIdx.x + k * BLOCK;
+            if (t < L) {
+                int s = sidx[k];
+                if (s < 0 || s >= A.capacity) {
+                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                    s = 0;
+                }
+                stage(s_pos + t, A.pos_in + s);
+                stage(s_vel + t, A.vel_in + s);
+                stage(s_psi + t, A.psi_in + s);
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
         for (int t = threadIdx.x; t < L; t += BLOCK) {
-            const int c = s_cell[t];
-            if (c == P.ovf_cell) continue;
-            if (t > 0 && s_cell[t - 1] == c) continue;
-            const int n = A.old_start[c + 1] - A.old_start[c];
-            if (A.old_start[c] != tb + t || n > L - t) {  // cell not wholly inside this tile
-                atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                continue;
-            }
-            if (n < 2) continue;
-            R svm = A.sigvrmax[c];
-            CollideResult<R> cr;
-            if (A.clog_ij) {
-                TileCollisionLog<R> lg{s_pos + t, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
-                cr = collide_cell<R, R4, TileCollisionLog<R>>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                               (uint32_t)step, A.seed, &lg);
-            } else {
-                cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
-            }
-            A.sigvrmax[c] = svm;
-            my_coll += cr.accepted;
-            my_cand += cr.candidates;
+            const R4 q = s_pos[t];
+            s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
         }
         __syncthreads();
-    }
 
-    // phase 3: move, spin, evaporate and classify every atom once
-    TilePartial acc;
-    zero_partial(acc);
-    acc.coll = my_coll;
-    acc.cand = my_cand;
-    long long ovf_stayers = 0;
-    for (int base = 0; base < L; base += BLOCK) {
-        const int t = base + threadIdx.x;
-        const bool valid = t < L;
-        Atom<R> a;
-        AtomOut<R> o;
-        o.fate = FATE_ALIVE;
-        o.cell = 0;
-        bool stayer = false, mover = false;
-        int c_old = 0;
-        R4 q, v, s;
-        if (valid) {
-            q = s_pos[t];
-            v = s_vel[t];
-            s = s_psi[t];
-            a.x = q.x; a.y = q.y; a.z = q.z;
-            a.vx = v.x; a.vy = v.y; a.vz = v.z;
-            a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
-            a.flags = lane_to_u32(v.w);
-            advance_atom(P, cut, a, o);
-            c_old = s_cell[t];
-            const bool alive = (o.fate == FATE_ALIVE);
-            stayer = alive && (o.cell == c_old);
-            mover = alive && !stayer;
-            if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
+        StepAcc acc;
+        zero_acc(acc);
+        // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles)
+        if ((P.flags & F_COLLIDE) && collide_now) {
+            for (int t = threadIdx.x; t < L; t += BLOCK) {
+                const int c = s_cell[t];
+                if (c == P.ovf_cell) continue;
+                if (t > 0 && s_cell[t - 1] == c) continue;
+                const int n = A.old_start[c + 1] - A.old_start[c];
+                if (A.old_start[c] != tb + t || n > L - t) {  // cell not wholly inside this tile
+                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                    continue;
+                }
+                if (n < 2) continue;
+                R svm = A.sigvrmax[c];
+                CollideResult<R> cr;
+                if (A.clog_ij) {
+                    TileCollisionLog<R> lg{s_pos + t, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
+                    cr = collide_cell<R, R4, TileCollisionLog<R>>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                                   (uint32_t)step, A.seed, &lg);
+                } else {
+                    cr = collide_cell<R, R4>(s_vel + t, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step,
+                                             A.seed);
+                }
+                A.sigvrmax[c] = svm;
+                acc.coll += (unsigned)cr.accepted;
+                acc.cand += (unsigned)cr.candidates;
+            }
+            __syncthreads();
         }
-        // leavers of the old cell (movers and lost atoms), warp-aggregated
-        const bool leaver = valid && !stayer;
-        const unsigned lm = __ballot_sync(0xffffffffu, leaver);
-        if (leaver) {
-            const unsigned peers = __match_any_sync(lm, c_old);
-            if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
-        }
-        // movers: a slot in the step's mover list and a ticket in the target cell
-        const unsigned mm = __ballot_sync(0xffffffffu, mover);
-        int slot = 0;
-        if (mm) {
-            const int leader = __ffs(mm) - 1;
-            int sbase = 0;
-            if (lane == leader) sbase = atomicAdd(&A.ctl->movers, __popc(mm));
-            sbase = __shfl_sync(0xffffffffu, sbase, leader);
-            slot = sbase + __popc(mm & ((1u << lane) - 1u));
-        }
-        if (mover) {
-            const unsigned peers = __match_any_sync(mm, o.cell);
-            const int leader = __ffs(peers) - 1;
-            int tbase = 0;
-            if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
-            tbase = __shfl_sync(peers, tbase, leader);
-            const int ticket = tbase + __popc(peers & ((1u << lane) - 1u));
-            A.mrec[slot] = make_int4(o.cell, tb + t, ticket, 0);
-        }
-        if (valid) {
-            const int j = tb + t;
-            if (stayer || mover) {
-                R4 qo, vo, so;
-                qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
-                vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = v.w;
-                so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
-                A.pos_out[j] = qo;
-                A.vel_out[j] = vo;
-                A.psi_out[j] = so;
-                acc.n_alive += 1;
-                acc.sum_v2 += fx_from(o.v2);
-                acc.sum_B += fx_from(o.absB);
-                A.keys[j] = stayer ? make_int2(c_old, KIND_STAY) : make_int2(slot, KIND_MOVE);
-                if (stayer && c_old == P.ovf_cell) ovf_stayers += 1;
-            } else {
-                acc.evap_v2 += fx_from(o.v2);
-                acc.evap_B += fx_from(o.absB);
-                if (o.fate == FATE_MAJORANA) acc.n_maj += 1;
-                else acc.n_knife += 1;
-                A.keys[j] = make_int2(-1, KIND_LOST);
+
+        // phase 3: move, spin, evaporate and classify every atom once
+        for (int base = 0; base < L; base += BLOCK) {
+            const int t = base + threadIdx.x;
+            const bool valid = t < L;
+            Atom<R> a;
+            AtomOut<R> o;
+            o.fate = FATE_ALIVE;
+            o.cell = 0;
+            bool stayer = false, mover = false;
+            int c_old = 0;
+            R4 q, v, s;
+            if (valid) {
+                q = s_pos[t];
+                v = s_vel[t];
+                s = s_psi[t];
+                a.x = q.x; a.y = q.y; a.z = q.z;
+                a.vx = v.x; a.vy = v.y; a.vz = v.z;
+                a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
+                a.flags = lane_to_u32(v.w);
+                advance_atom(P, cut, a, o);
+                c_old = s_cell[t];
+                const bool alive = (o.fate == FATE_ALIVE);
+                stayer = alive && (o.cell == c_old);
+                mover = alive && !stayer;
+                if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
+            }
+            // leavers of the old cell (movers and lost atoms), warp-aggregated
+            const bool leaver = valid && !stayer;
+            const unsigned lm = __ballot_sync(0xffffffffu, leaver);
+            if (leaver) {
+                const unsigned peers = __match_any_sync(lm, c_old);
+                if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
+            }
+            // movers: a slot in the step's mover list and a ticket in the target cell
+            const unsigned mm = __ballot_sync(0xffffffffu, mover);
+            int slot = 0;
+            if (mm) {
+                const int leader = __ffs(mm) - 1;
+                int sbase = 0;
+                if (lane == leader) sbase = atomicAdd(&A.ctl->movers, __popc(mm));
+                sbase = __shfl_sync(0xffffffffu, sbase, leader);
+                slot = sbase + __popc(mm & ((1u << lane) - 1u));
+            }
+            if (mover) {
+                const unsigned peers = __match_any_sync(mm, o.cell);
+                const int leader = __ffs(peers) - 1;
+                int tbase = 0;
+                if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
+                tbase = __shfl_sync(peers, tbase, leader);
+                const int ticket = tbase + __popc(peers & ((1u << lane) - 1u));
+                A.mrec[slot] = make_int4(o.cell, tb + t, ticket, 0);
+            }
+            if (valid) {
+                const int j = tb + t;
+                if (stayer || mover) {
+                    R4 qo, vo, so;
+                    qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
+                    vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = v.w;
+                    so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
+                    A.pos_out[j] = qo;
+                    A.vel_out[j] = vo;
+                    A.psi_out[j] = so;
+                    acc.n_alive += 1u;
+                    acc.sum_v2 += fx_from(o.v2);
+                    acc.sum_B += fx_from(o.absB);
+                    A.keys[j] = stayer ? make_int2(c_old, KIND_STAY) : make_int2(slot, KIND_MOVE);
+                    if (stayer && c_old == P.ovf_cell) acc.ovf_stayers += 1u;
+                } else {
+                    acc.evap_v2 += fx_from(o.v2);
+                    acc.evap_B += fx_from(o.absB);
+                    if (o.fate == FATE_MAJORANA) acc.n_maj += 1u;
+                    else acc.n_knife += 1u;
+                    A.keys[j] = make_int2(-1, KIND_LOST);
+                }
             }
         }
-    }
-    acc.ovf_stayers = ovf_stayers;
-    block_reduce_partial<BLOCK>(acc, red);
-    if (threadIdx.x == 0) {
-        A.tile_ovf[b] = (int)acc.ovf_stayers;
-        A.partials[b] = acc;
+        TilePartial tot;
+        block_reduce_acc<BLOCK>(acc, red, tot);
+        if (threadIdx.x == 0) {
+            A.tile_ovf[b] = (int)tot.ovf_stayers;
+            accum_tile(A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1)), tot);
+        }
+        __syncthreads();  // the staging arrays and red are reused by the next tile
     }
 }
 
@@ -480,12 +580,12 @@ __global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
     __shared__ uint32_t s_pre[CAP];
     __shared__ uint32_t wsum[32];
     const int p = A.parity;
-    const int b = blockIdx.x;
-    if (b >= A.ctl->ntiles[p]) return;
+    const int ntiles = A.ctl->ntiles[p];
+    for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int tb = A.tile_begin[b];
     const int te = A.tile_begin[b + 1];
     const int L = te - tb;
-    if (L > CAP || L < 0) return;  // step_pass marked every atom of such a tile as lost
+    if (L > CAP || L < 0) continue;  // step_pass marked every atom of such a tile as lost
     const int cloud = A.tile_cloud[b];
     const int carry_base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
     const int t0 = threadIdx.x * K;
@@ -527,6 +627,8 @@ __global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
         }
         if (dest >= 0) A.src_out[dest] = tb + t;
         else if (dest == -2) atomicOr(&A.ctl->err, EB_INCONSISTENT);
+    }
+    __syncthreads();  // s_pre is reused by the next tile
     }
 }
 
@@ -748,28 +850,36 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
 
 // per-cloud diagnostics from the tile partials; block k handles cloud k
 template <class R, bool INIT>
-__global__ void __launch_bounds__(512) finalize(Args<R> A) {
-    __shared__ TilePartial red[32];
+__global__ void __launch_bounds__(32) finalize(Args<R> A) {
+    static_assert(ACC_BUCKETS <= 32, "one lane per bucket");
     const int p = A.parity;
     const int k = blockIdx.x;
     CloudDyn& d = A.cdyn[k];
-    const int t0 = d.tile_off[p], nt = d.ntiles[p];
     TilePartial acc;
     zero_partial(acc);
-#pragma unroll 4
-    for (int j = threadIdx.x; j < nt; j += 512) {
-        const TilePartial& t = A.partials[t0 + j];
-        acc.sum_v2 += t.sum_v2;
-        acc.sum_B += t.sum_B;
-        acc.evap_v2 += t.evap_v2;
-        acc.evap_B += t.evap_B;
-        acc.n_alive += t.n_alive;
-        acc.n_maj += t.n_maj;
-        acc.n_knife += t.n_knife;
-        acc.coll += t.coll;
-        acc.cand += t.cand;
+    if (threadIdx.x < ACC_BUCKETS) {
+        CloudAccum& g = A.accum[k * ACC_BUCKETS + threadIdx.x];
+        acc.sum_v2 = from_limbs(g.v2);
+        acc.sum_B = from_limbs(g.B);
+        acc.evap_v2 = from_limbs(g.ev2);
+        acc.evap_B = from_limbs(g.eB);
+        acc.n_alive = (long long)g.n_alive;
+        acc.n_maj = (long long)g.n_maj;
+        acc.n_knife = (long long)g.n_knife;
+        acc.coll = (long long)g.coll;
+        acc.cand = (long long)g.cand;
+        CloudAccum z = {};
+        g = z;  // cleared for the next step
     }
-    block_reduce_partial<512>(acc, red);
+    acc.sum_v2 = warp_sum_i128(acc.sum_v2);
+    acc.sum_B = warp_sum_i128(acc.sum_B);
+    acc.evap_v2 = warp_sum_i128(acc.evap_v2);
+    acc.evap_B = warp_sum_i128(acc.evap_B);
+    acc.n_alive = warp_sum_ll(acc.n_alive);
+    acc.n_maj = warp_sum_ll(acc.n_maj);
+    acc.n_knife = warp_sum_ll(acc.n_knife);
+    acc.coll = warp_sum_ll(acc.coll);
+    acc.cand = warp_sum_ll(acc.cand);
     if (threadIdx.x == 0) {
         const CloudPhys<R>& P = A.clouds[k];
         CloudDiagDev& g = A.cdiag[k];
@@ -807,15 +917,15 @@ __global__ void __launch_bounds__(512) finalize(Args<R> A) {
     }
 }
 
-// diagnostics of the current (sorted) state without moving it: tile partials for finalize<INIT>
+// diagnostics of the current (sorted) state without moving it: bucket totals for finalize<INIT>
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
     typedef typename V4T<R>::type R4;
     __shared__ TilePartial red[BLOCK / 32];
     __shared__ CloudPhys<R> P;
     const int p = A.parity;
-    const int b = blockIdx.x;
-    if (b >= A.ctl->ntiles[p]) return;
+    const int ntiles = A.ctl->ntiles[p];
+    for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int tb = A.tile_begin[b], te = A.tile_begin[b + 1];
     load_cloud(P, A.clouds + A.tile_cloud[b]);
     __syncthreads();
@@ -833,7 +943,8 @@ __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
         acc.sum_B += fx_from(f.absB);
     }
     block_reduce_partial<BLOCK>(acc, red);
-    if (threadIdx.x == 0) A.partials[b] = acc;
+    if (threadIdx.x == 0) accum_tile(A.accum + A.tile_cloud[b] * ACC_BUCKETS + (b & (ACC_BUCKETS - 1)), acc);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
