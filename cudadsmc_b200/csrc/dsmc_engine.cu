@@ -160,7 +160,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB>, BLOCK, smem_tile));
         resident_step = nsm * std::max(occ, 1);
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R, 256, CAP>, 256, 0));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R>, 256, 0));
         resident_permute = nsm * std::max(occ, 1);
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, measure_tiles<R, 256>, 256, 0));
         resident_measure = nsm * std::max(occ, 1);
@@ -287,7 +287,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 4: mover_place<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         case 5: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
-        case 6: permute_pass<R, 256, CAP><<<tile_grid(resident_permute), 256, 0, stream>>>(A); break;
+        case 6: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
         case 7: finalize<R, false><<<nclouds, 32, 0, stream>>>(A); break;
         }
     }

@@ -86,7 +86,12 @@ struct Ctl {
 };
 
 // sort keys written by step_pass for every current position j
-enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2 };
+// keys written by step_pass, one per atom position: .y = kind | (rank << 2)
+//   KIND_STAY  .x = cell, rank among the cell's stayers before it (the cell starts in this tile)
+//   KIND_OVF   .x = tile, rank among the tile's stayers of the cloud's overflow cell, which
+//              started in an earlier tile (the only cell that may be split across tiles)
+//   KIND_MOVE  .x = slot in the step's mover list;  KIND_LOST  .x = -1
+enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2, KIND_OVF = 3 };
 
 template <class R> struct Args {
     typedef typename V4T<R>::type R4;
@@ -379,6 +384,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
     __shared__ CloudPhys<R> P;
     __shared__ StepAcc red[BLOCK / 32];
+    __shared__ uint32_t wsum[32];
     __shared__ R s_cut;
 
     const int p = A.parity;
@@ -547,14 +553,57 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
                     acc.n_alive += 1u;
                     acc.sum_v2 += fx_from(o.v2);
                     acc.sum_B += fx_from(o.absB);
-                    A.keys[j] = stayer ? make_int2(c_old, KIND_STAY) : make_int2(slot, KIND_MOVE);
-                    if (stayer && c_old == P.ovf_cell) acc.ovf_stayers += 1u;
+                    if (stayer) {
+                        s_cell[t] = (int)((unsigned)c_old | 0x80000000u);  // ranked below
+                        if (c_old == P.ovf_cell) acc.ovf_stayers += 1u;
+                    } else {
+                        A.keys[j] = make_int2(slot, KIND_MOVE);
+                    }
                 } else {
                     acc.evap_v2 += fx_from(o.v2);
                     acc.evap_B += fx_from(o.absB);
                     if (o.fate == FATE_MAJORANA) acc.n_maj += 1u;
                     else acc.n_knife += 1u;
                     A.keys[j] = make_int2(-1, KIND_LOST);
+                }
+            }
+        }
+        // phase 4: rank of every stayer among the stayers of its cell (in old order), by one
+        // exclusive scan of the stayer marks over the tile; positions are blocked per thread
+        __syncthreads();
+        {
+            uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_pos);  // staging no longer needed
+            const int t0 = threadIdx.x * PER;
+            int cc[PER];
+            uint32_t mine = 0;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                cc[k] = t0 + k < L ? s_cell[t0 + k] : 0;
+                mine += cc[k] < 0 ? 1u : 0u;
+            }
+            uint32_t total;
+            uint32_t run = block_excl_scan_u32<BLOCK>(mine, wsum, total);
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                if (t0 + k < L) s_pre[t0 + k] = run;
+                run += cc[k] < 0 ? 1u : 0u;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int t = t0 + k;
+                if (t < L && cc[k] < 0) {
+                    const int c = cc[k] & 0x7fffffff;
+                    const int seg = A.old_start[c];
+                    const int sl = seg > tb ? seg - tb : 0;
+                    int2 key = make_int2(-1, KIND_LOST);
+                    if (sl <= t) {
+                        const int rank = (int)(s_pre[t] - s_pre[sl]);
+                        key = seg < tb ? make_int2(b, KIND_OVF | (rank << 2)) : make_int2(c, KIND_STAY | (rank << 2));
+                    } else {
+                        atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                    }
+                    A.keys[tb + t] = key;
                 }
             }
         }
@@ -569,66 +618,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// permute_pass: destination of every surviving atom in the new order, written as the next
-// permutation.  Stayers rank inside their old cell by a block-wide prefix count (a grid cell
-// never straddles tiles; the overflow cell adds the count of its stayers in earlier tiles),
-// movers take the slot mover_rank computed.
+// permute_pass: the stayers' part of the next step's gather permutation.  A stayer of cell c with
+// rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
+// KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Movers are placed by
+// mover_rank.  A flat stream over the keys, no shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
-template <class R, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) permute_pass(Args<R> A) {
-    constexpr int K = CAP / BLOCK;  // positions per thread, a contiguous run
-    __shared__ uint32_t s_pre[CAP];
-    __shared__ uint32_t wsum[32];
+template <class R>
+__global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
     const int p = A.parity;
+    const int n = A.ctl->n[p];
     const int ntiles = A.ctl->ntiles[p];
-    for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
-    const int tb = A.tile_begin[b];
-    const int te = A.tile_begin[b + 1];
-    const int L = te - tb;
-    if (L > CAP || L < 0) continue;  // step_pass marked every atom of such a tile as lost
-    const int cloud = A.tile_cloud[b];
-    const int carry_base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
-    const int t0 = threadIdx.x * K;
-    int2 key[K];
-    uint32_t mine = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        key[k] = (t0 + k < L) ? A.keys[tb + t0 + k] : make_int2(-1, KIND_LOST);
-        mine += (key[k].y == KIND_STAY) ? 1u : 0u;
-    }
-    uint32_t tot;
-    uint32_t run = block_excl_scan_u32<BLOCK>(mine, wsum, tot);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (t0 + k < L) s_pre[t0 + k] = run;
-        run += (key[k].y == KIND_STAY) ? 1u : 0u;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const int t = t0 + k;
-        if (t >= L) break;
-        int dest = -1;
-        if (key[k].y == KIND_STAY) {
-            const int c = key[k].x;
-            const int seg = A.old_start[c];
-            const int sl = seg > tb ? seg - tb : 0;
-            if (sl <= t) {
-                int rank = (int)(s_pre[t] - s_pre[sl]);
-                if (seg < tb) rank += carry_base;
-                dest = A.new_start[c] + rank;
-                if (dest < A.new_start[c] || dest >= A.new_start[c + 1]) dest = -2;
-            } else {
-                dest = -2;
-            }
-        } else if (key[k].y == KIND_MOVE) {
-            dest = (key[k].x >= 0 && key[k].x < A.capacity) ? A.mrec[key[k].x].w : -2;
-            if (dest < 0 || dest >= A.capacity) dest = -2;
+    for (int j = blockIdx.x * 256 + threadIdx.x; j < n; j += gridDim.x * 256) {
+        const int2 key = A.keys[j];
+        const int kind = key.y & 3;
+        if (kind == KIND_MOVE || kind == KIND_LOST) continue;
+        const int rank = key.y >> 2;
+        int c = key.x, base = 0;
+        if (kind == KIND_OVF) {
+            const int b = key.x;
+            if (b < 0 || b >= ntiles) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
+            const int cloud = A.tile_cloud[b];
+            c = A.clouds[cloud].ovf_cell;
+            base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
         }
-        if (dest >= 0) A.src_out[dest] = tb + t;
-        else if (dest == -2) atomicOr(&A.ctl->err, EB_INCONSISTENT);
-    }
-    __syncthreads();  // s_pre is reused by the next tile
+        if (c < 0 || c >= A.total_cells) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
+        const int lo = A.new_start[c];
+        const int dest = lo + base + rank;
+        if (dest >= lo && dest < A.new_start[c + 1]) A.src_out[dest] = j;
+        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
 
@@ -832,19 +849,17 @@ template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
     const int m = A.ctl->movers;
     for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
-        int4 r = A.mrec[i];
+        const int4 r = A.mrec[i];
         const int lo = A.mover_base[r.x];
         const int hi = A.new_start[r.x + 1];
         if (lo < 0 || hi > A.capacity || lo > hi) {
             atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            r.w = -1;
-            A.mrec[i] = r;
             continue;
         }
         int rank = 0;
         for (int k = lo; k < hi; ++k) rank += (A.in_list[k] < r.y) ? 1 : 0;
-        r.w = lo + rank;
-        A.mrec[i] = r;
+        if (lo + rank < hi && r.y >= 0 && r.y < A.capacity) A.src_out[lo + rank] = r.y;
+        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
 
