@@ -152,7 +152,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
-        smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int));
+        smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int) + sizeof(uint16_t));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         int dev = 0, nsm = 0, occ = 0;

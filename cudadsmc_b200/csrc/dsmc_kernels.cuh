@@ -205,28 +205,25 @@ __device__ __forceinline__ i128 warp_sum_u128_redux(i128 v) {
     return (i128)r;
 }
 
-// per-thread accumulators of step_pass and their block reduction into a TilePartial
+// per-thread accumulators of step_pass (the retained atoms and the collisions) and their block
+// reduction; lost atoms are rare and go straight into a block-shared LostAcc
 struct StepAcc {
-    i128 sum_v2, sum_B, evap_v2, evap_B;
-    unsigned n_alive, n_maj, n_knife, coll, cand, ovf_stayers;
+    i128 sum_v2, sum_B;
+    unsigned n_alive, coll, cand;
+};
+struct LostAcc {
+    unsigned long long ev2[3], eB[3], n_maj, n_knife;
 };
 __device__ __forceinline__ void zero_acc(StepAcc& a) {
-    a.sum_v2 = 0; a.sum_B = 0; a.evap_v2 = 0; a.evap_B = 0;
-    a.n_alive = 0; a.n_maj = 0; a.n_knife = 0; a.coll = 0; a.cand = 0; a.ovf_stayers = 0;
+    a.sum_v2 = 0; a.sum_B = 0;
+    a.n_alive = 0; a.coll = 0; a.cand = 0;
 }
 __device__ __forceinline__ void warp_reduce_acc(StepAcc& a) {
     a.sum_v2 = warp_sum_u128_redux(a.sum_v2);
     a.sum_B = warp_sum_u128_redux(a.sum_B);
-    if (__any_sync(0xffffffffu, (a.n_maj | a.n_knife) != 0u)) {  // only warps that lost atoms
-        a.evap_v2 = warp_sum_u128_redux(a.evap_v2);
-        a.evap_B = warp_sum_u128_redux(a.evap_B);
-    }
     a.n_alive = __reduce_add_sync(0xffffffffu, a.n_alive);
-    a.n_maj = __reduce_add_sync(0xffffffffu, a.n_maj);
-    a.n_knife = __reduce_add_sync(0xffffffffu, a.n_knife);
     a.coll = __reduce_add_sync(0xffffffffu, a.coll);
     a.cand = __reduce_add_sync(0xffffffffu, a.cand);
-    a.ovf_stayers = __reduce_add_sync(0xffffffffu, a.ovf_stayers);
 }
 // every thread of the block calls; thread 0 receives the block total in `out`
 template <int BLOCK>
@@ -242,9 +239,9 @@ __device__ __forceinline__ void block_reduce_acc(StepAcc& a, StepAcc* sm, TilePa
         if (lane < NW) w = sm[lane]; else zero_acc(w);
         warp_reduce_acc(w);
         if (lane == 0) {
-            out.sum_v2 = w.sum_v2; out.sum_B = w.sum_B; out.evap_v2 = w.evap_v2; out.evap_B = w.evap_B;
-            out.n_alive = w.n_alive; out.n_maj = w.n_maj; out.n_knife = w.n_knife;
-            out.coll = w.coll; out.cand = w.cand; out.ovf_stayers = w.ovf_stayers;
+            out.sum_v2 = w.sum_v2; out.sum_B = w.sum_B; out.evap_v2 = 0; out.evap_B = 0;
+            out.n_alive = w.n_alive; out.n_maj = 0; out.n_knife = 0;
+            out.coll = w.coll; out.cand = w.cand; out.ovf_stayers = 0;
             out.pad1 = 0; out.pad2 = 0;
         }
     }
@@ -303,6 +300,19 @@ __device__ __forceinline__ void accum_tile(CloudAccum* bucket, const TilePartial
     if (t.n_knife) atomicAdd(&bucket->n_knife, (unsigned long long)t.n_knife);
     if (t.coll) atomicAdd(&bucket->coll, (unsigned long long)t.coll);
     if (t.cand) atomicAdd(&bucket->cand, (unsigned long long)t.cand);
+}
+// a block's lost-atom totals into a bucket (one thread), then cleared
+__device__ __forceinline__ void accum_lost(CloudAccum* bucket, LostAcc& s) {
+    for (int i = 0; i < 3; ++i) {
+        if (s.ev2[i]) atomicAdd(&bucket->ev2[i], s.ev2[i]);
+        if (s.eB[i]) atomicAdd(&bucket->eB[i], s.eB[i]);
+        s.ev2[i] = 0;
+        s.eB[i] = 0;
+    }
+    if (s.n_maj) atomicAdd(&bucket->n_maj, s.n_maj);
+    if (s.n_knife) atomicAdd(&bucket->n_knife, s.n_knife);
+    s.n_maj = 0;
+    s.n_knife = 0;
 }
 __device__ __forceinline__ i128 from_limbs(const unsigned long long* l) {
     return (i128)((unsigned __int128)l[0] + ((unsigned __int128)l[1] << 42) + ((unsigned __int128)l[2] << 84));
@@ -382,10 +392,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     R4* s_vel = s_pos + CAP;
     R4* s_psi = s_vel + CAP;
     int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
+    uint16_t* s_head = reinterpret_cast<uint16_t*>(s_cell + CAP);  // first positions of cells to collide
+    static_assert(CAP <= 65536, "head positions are 16-bit");
     __shared__ CloudPhys<R> P;
     __shared__ StepAcc red[BLOCK / 32];
-    __shared__ uint32_t wsum[32];
     __shared__ R s_cut;
+    __shared__ int s_nhead;
+    __shared__ int s_split;  // the tile's first cell began in an earlier tile
+    // the last run of cells in each 32-position chunk: its cell, its stayers, whether it spans the chunk
+    constexpr int NCH = CAP / 32;
+    __shared__ int s_tcell[NCH];
+    __shared__ int s_tcnt[NCH];
+    __shared__ int s_twhole[NCH];
+    __shared__ int s_ovf;  // stayers of the overflow cell in the current tile
+    __shared__ LostAcc s_lost;
 
     const int p = A.parity;
     const int ntiles = A.ctl->ntiles[p];
@@ -394,6 +414,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     const int lane = threadIdx.x & 31;
     const bool collide_now = (step % A.collide_every) == 0;
     int cur_cloud = -1;
+    if (threadIdx.x == 0) {
+        LostAcc z = {};
+        s_lost = z;  // ordered before first use by the barrier after the first load_cloud
+    }
 
     // tiles in a grid-stride loop: the launch size only sets how many tiles run at once
     for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
@@ -449,22 +473,47 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
                 stage(s_psi + t, A.psi_in + s);
             }
         }
+        if (threadIdx.x == 0) {
+            s_nhead = 0;
+            s_ovf = 0;
+        }
         cp_async_wait_all();
         __syncthreads();
         for (int t = threadIdx.x; t < L; t += BLOCK) {
             const R4 q = s_pos[t];
-            s_cell[t] = cell_of(P, q.x, q.y, q.z, box);
+            const int c = cell_of(P, q.x, q.y, q.z, box);
+            s_cell[t] = c;
+            if (t == 0) s_split = A.old_start[c] < tb ? 1 : 0;
         }
         __syncthreads();
+        const int c_first = L > 0 ? s_cell[0] : -1;
+        const bool split = L > 0 && s_split != 0;
 
         StepAcc acc;
         zero_acc(acc);
-        // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles)
+        // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles).  The
+        // cells holding two or more atoms are listed first, so that every lane takes a cell.
         if ((P.flags & F_COLLIDE) && collide_now) {
-            for (int t = threadIdx.x; t < L; t += BLOCK) {
+            for (int base = 0; base < L; base += BLOCK) {
+                const int t = base + threadIdx.x;
+                bool head = false;
+                if (t + 1 < L) {
+                    const int c = s_cell[t];
+                    head = c != P.ovf_cell && (t == 0 || s_cell[t - 1] != c) && s_cell[t + 1] == c;
+                }
+                const unsigned hm = __ballot_sync(0xffffffffu, head);
+                if (hm) {
+                    int first = 0;
+                    if (lane == 0) first = atomicAdd(&s_nhead, __popc(hm));
+                    first = __shfl_sync(0xffffffffu, first, 0);
+                    if (head) s_head[first + __popc(hm & ((1u << lane) - 1u))] = (uint16_t)t;
+                }
+            }
+            __syncthreads();
+            const int nhead = s_nhead;
+            for (int h = threadIdx.x; h < nhead; h += BLOCK) {
+                const int t = s_head[h];
                 const int c = s_cell[t];
-                if (c == P.ovf_cell) continue;
-                if (t > 0 && s_cell[t - 1] == c) continue;
                 const int n = A.old_start[c + 1] - A.old_start[c];
                 if (A.old_start[c] != tb + t || n > L - t) {  // cell not wholly inside this tile
                     atomicOr(&A.ctl->err, EB_INCONSISTENT);
@@ -514,6 +563,39 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
                 mover = alive && !stayer;
                 if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
             }
+            // stayers are ranked among the stayers of their cell in old order: cells are runs of
+            // consecutive positions, so within this warp's 32 positions a stayer's rank is the number
+            // of stayers since the start of its run; a run that continues from the previous chunk
+            // gets that chunk's count after the block's next barrier
+            const unsigned FULL = 0xffffffffu;
+            const int cprev = __shfl_up_sync(FULL, c_old, 1);
+            const unsigned vmask = __ballot_sync(FULL, valid);
+            const unsigned hmask = __ballot_sync(FULL, valid && (lane == 0 || c_old != cprev));
+            const unsigned smask = __ballot_sync(FULL, stayer);
+            const int chunk = t >> 5;
+            if (vmask) {
+                const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
+                const int run0 = 31 - __clz(hmask & le);
+                const int tail0 = 31 - __clz(hmask);
+                const int tcell = __shfl_sync(FULL, c_old, 31 - __clz(vmask));
+                if (lane == 0) {
+                    s_tcell[chunk] = tcell;
+                    s_tcnt[chunk] = __popc(smask & (FULL << tail0));
+                    s_twhole[chunk] = tail0 == 0 ? 1 : 0;
+                }
+                if (stayer) {
+                    const int rank = __popc(smask & ((1u << lane) - 1u) & (FULL << run0));
+                    const int cstart = t - lane;
+                    const bool cont = run0 == 0 && cstart > 0 && (s_cell[cstart - 1] & 0x7fffffff) == c_old;
+                    if (cont) {  // finished after the barrier
+                        reinterpret_cast<int*>(s_pos + t)[0] = rank;
+                        s_cell[t] = (int)((unsigned)c_old | 0x80000000u);
+                    } else {
+                        A.keys[tb + t] = (split && c_old == c_first) ? make_int2(b, KIND_OVF | (rank << 2))
+                                                                      : make_int2(c_old, KIND_STAY | (rank << 2));
+                    }
+                }
+            }
             // leavers of the old cell (movers and lost atoms), warp-aggregated
             const bool leaver = valid && !stayer;
             const unsigned lm = __ballot_sync(0xffffffffu, leaver);
@@ -554,66 +636,40 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
                     acc.sum_v2 += fx_from(o.v2);
                     acc.sum_B += fx_from(o.absB);
                     if (stayer) {
-                        s_cell[t] = (int)((unsigned)c_old | 0x80000000u);  // ranked below
-                        if (c_old == P.ovf_cell) acc.ovf_stayers += 1u;
+                        if (c_old == P.ovf_cell) atomicAdd(&s_ovf, 1);
                     } else {
                         A.keys[j] = make_int2(slot, KIND_MOVE);
                     }
                 } else {
-                    acc.evap_v2 += fx_from(o.v2);
-                    acc.evap_B += fx_from(o.absB);
-                    if (o.fate == FATE_MAJORANA) acc.n_maj += 1u;
-                    else acc.n_knife += 1u;
+                    add_limbs(s_lost.ev2, fx_from(o.v2));
+                    add_limbs(s_lost.eB, fx_from(o.absB));
+                    atomicAdd(o.fate == FATE_MAJORANA ? &s_lost.n_maj : &s_lost.n_knife, 1ull);
                     A.keys[j] = make_int2(-1, KIND_LOST);
                 }
             }
         }
-        // phase 4: rank of every stayer among the stayers of its cell (in old order), by one
-        // exclusive scan of the stayer marks over the tile; positions are blocked per thread
-        __syncthreads();
-        {
-            uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_pos);  // staging no longer needed
-            const int t0 = threadIdx.x * PER;
-            int cc[PER];
-            uint32_t mine = 0;
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                cc[k] = t0 + k < L ? s_cell[t0 + k] : 0;
-                mine += cc[k] < 0 ? 1u : 0u;
-            }
-            uint32_t total;
-            uint32_t run = block_excl_scan_u32<BLOCK>(mine, wsum, total);
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                if (t0 + k < L) s_pre[t0 + k] = run;
-                run += cc[k] < 0 ? 1u : 0u;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int t = t0 + k;
-                if (t < L && cc[k] < 0) {
-                    const int c = cc[k] & 0x7fffffff;
-                    const int seg = A.old_start[c];
-                    const int sl = seg > tb ? seg - tb : 0;
-                    int2 key = make_int2(-1, KIND_LOST);
-                    if (sl <= t) {
-                        const int rank = (int)(s_pre[t] - s_pre[sl]);
-                        key = seg < tb ? make_int2(b, KIND_OVF | (rank << 2)) : make_int2(c, KIND_STAY | (rank << 2));
-                    } else {
-                        atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                    }
-                    A.keys[tb + t] = key;
-                }
-            }
-        }
         TilePartial tot;
-        block_reduce_acc<BLOCK>(acc, red, tot);
+        block_reduce_acc<BLOCK>(acc, red, tot);  // its barrier also orders the chunk records, s_ovf and s_lost
         if (threadIdx.x == 0) {
-            A.tile_ovf[b] = (int)tot.ovf_stayers;
-            accum_tile(A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1)), tot);
+            CloudAccum* bucket = A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1));
+            A.tile_ovf[b] = s_ovf;
+            accum_tile(bucket, tot);
+            accum_lost(bucket, s_lost);
         }
-        __syncthreads();  // the staging arrays and red are reused by the next tile
+        // stayers whose cell run began in an earlier chunk: add the stayers of that run there
+        for (int t = threadIdx.x; t < L; t += BLOCK) {
+            const int cm = s_cell[t];
+            if (cm >= 0) continue;
+            const int c = cm & 0x7fffffff;
+            int rank = reinterpret_cast<const int*>(s_pos + t)[0];
+            for (int qq = (t >> 5) - 1; qq >= 0 && s_tcell[qq] == c; --qq) {
+                rank += s_tcnt[qq];
+                if (!s_twhole[qq]) break;
+            }
+            A.keys[tb + t] = (split && c == c_first) ? make_int2(b, KIND_OVF | (rank << 2))
+                                                     : make_int2(c, KIND_STAY | (rank << 2));
+        }
+        __syncthreads();  // the staging arrays, red and s_lost are reused by the next tile
     }
 }
 
