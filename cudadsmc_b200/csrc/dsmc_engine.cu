@@ -153,12 +153,14 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
         smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int) + sizeof(uint16_t));
-        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_tile));
+        CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         int dev = 0, nsm = 0, occ = 0;
         CU(cudaGetDevice(&dev));
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB>, BLOCK, smem_tile));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB, false>, BLOCK, smem_tile));
         resident_step = nsm * std::max(occ, 1);
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R>, 256, 0));
         resident_permute = nsm * std::max(occ, 1);
@@ -267,6 +269,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
+            A.one = phys[0];
             A.block_sums = block_sums.p; A.block_off = block_off.p;
             A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
             A.cloud_first_blk = cloud_first_blk.p;
@@ -281,7 +284,12 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0: step_pass<R, BLOCK, CAP, MINB><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A); break;
+        case 0:
+            if (nclouds == 1)
+                step_pass<R, BLOCK, CAP, MINB, true><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
+            else
+                step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
+            break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
         case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
         case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;

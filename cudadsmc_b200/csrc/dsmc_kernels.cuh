@@ -120,6 +120,7 @@ template <class R> struct Args {
     int* tile_ovf_carry;
     CloudAccum* accum;  // nclouds x ACC_BUCKETS
     const CloudPhys<R>* clouds;
+    CloudPhys<R> one;   // the parameters of cloud 0, read from the kernel parameters by one-cloud runs
     CloudDyn* cdyn;
     CloudDiagDev* cdiag;
     Ctl* ctl;
@@ -383,8 +384,10 @@ template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src
 // every atom moves straight from shared memory; only the new state, the keys and the counters
 // go back to global memory.
 // ---------------------------------------------------------------------------------------------
-template <class R, int BLOCK, int CAP, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
+// ONE: the run has a single cloud, whose parameters are read from the kernel parameter block
+// (constant operands) instead of a shared-memory copy
+template <class R, int BLOCK, int CAP, int MINB, bool ONE>
+__global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__ Args<R> A) {
     typedef typename V4T<R>::type R4;
     constexpr int PER = CAP / BLOCK;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -394,7 +397,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
     int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
     uint16_t* s_head = reinterpret_cast<uint16_t*>(s_cell + CAP);  // first positions of cells to collide
     static_assert(CAP <= 65536, "head positions are 16-bit");
-    __shared__ CloudPhys<R> P;
+    __shared__ CloudPhys<R> P_sh;
+    const CloudPhys<R>& P = ONE ? A.one : P_sh;
     __shared__ StepAcc red[BLOCK / 32];
     __shared__ R s_cut;
     __shared__ int s_nhead;
@@ -426,7 +430,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(Args<R> A) {
         const int L = te - tb;
         const int cloud = A.tile_cloud[b];
         if (cloud != cur_cloud) {  // block-uniform: the cloud's parameters and knife cut
-            load_cloud(P, A.clouds + cloud);
+            if (!ONE) load_cloud(P_sh, A.clouds + cloud);
             __syncthreads();
             if (threadIdx.x == 0) s_cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
             __syncthreads();
