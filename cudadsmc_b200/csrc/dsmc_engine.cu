@@ -62,9 +62,8 @@ constexpr int kMinTile = 128;  // smallest tile the autotuner tries (sizes the t
 #define DSMC_FP32_MINB 4
 #endif
 
-const char* kKernelNames[] = {"step_pass",   "scan_reduce", "scan_top",     "scan_down",
-                              "mover_place", "mover_rank",  "permute_pass", "finalize"};
-constexpr int kNumStepKernels = 8;
+const char* kKernelNames[] = {"step_pass", "scan_reduce", "scan_down", "permute_pass", "mover_rank"};
+constexpr int kNumStepKernels = 5;
 
 }  // namespace
 
@@ -111,7 +110,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<R4> pos[2], vel[2], psi[2];
     DevBuf<int> start[2], tile_begin[2], tile_cloud[2];
     DevBuf<int> src[2];
-    DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry;
+    DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry, ovf_list;
     DevBuf<int4> mrec;
     DevBuf<int2> keys;
     DevBuf<R> sigvrmax;
@@ -224,7 +223,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         in_list.alloc(capacity);
         mrec.alloc(capacity);
         keys.alloc(capacity);
-        tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles);
+        tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles); ovf_list.alloc(max_tiles);
         sigvrmax.alloc(total_cells);
         accum.alloc((size_t)nclouds * ACC_BUCKETS);
         CU(cudaMemset(accum.p, 0, (size_t)nclouds * ACC_BUCKETS * sizeof(CloudAccum)));
@@ -266,7 +265,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.mrec = mrec.p; A.in_list = in_list.p;
             A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p;
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
-            A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p;
+            A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p; A.ovf_list = ovf_list.p;
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.one = phys[0];
@@ -291,12 +290,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
                 step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
             break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
-        case 2: scan_top<R><<<1, 1024, 0, stream>>>(A); break;
-        case 3: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
-        case 4: mover_place<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
-        case 5: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
-        case 6: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
-        case 7: finalize<R, false><<<nclouds, 32, 0, stream>>>(A); break;
+        case 2: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
+        case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
+        case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
     }
 
@@ -404,7 +400,6 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p, orank.p);
         }
         scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
-        scan_top<R><<<1, 1024, 0, stream>>>(A);
         scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
         if (n > 0) {
             fs_place<R><<<ab, 256, 0, stream>>>(S, A);

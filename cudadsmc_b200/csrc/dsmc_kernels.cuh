@@ -82,7 +82,9 @@ struct Ctl {
     int ntiles[2];
     int step[2];
     int err;
-    int movers;  // movers listed by the current step (reset by finalize)
+    int movers[2];  // movers listed by the step of each parity (the other parity's is cleared by the scan)
+    int novf[2];    // tiles with overflow-cell stayers listed by the step of each parity
+    int scan_done;  // scan_reduce blocks finished (the last one runs the top level and clears it)
 };
 
 // sort keys written by step_pass for every current position j
@@ -118,6 +120,7 @@ template <class R> struct Args {
     int* tile_cloud_next;
     int* tile_ovf;
     int* tile_ovf_carry;
+    int* ovf_list;  // tiles holding stayers of an overflow cell, in any order (ctl->novf[parity])
     CloudAccum* accum;  // nclouds x ACC_BUCKETS
     const CloudPhys<R>* clouds;
     CloudPhys<R> one;   // the parameters of cloud 0, read from the kernel parameters by one-cloud runs
@@ -613,7 +616,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             if (mm) {
                 const int leader = __ffs(mm) - 1;
                 int sbase = 0;
-                if (lane == leader) sbase = atomicAdd(&A.ctl->movers, __popc(mm));
+                if (lane == leader) sbase = atomicAdd(&A.ctl->movers[p], __popc(mm));
                 sbase = __shfl_sync(0xffffffffu, sbase, leader);
                 slot = sbase + __popc(mm & ((1u << lane) - 1u));
             }
@@ -657,6 +660,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         if (threadIdx.x == 0) {
             CloudAccum* bucket = A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1));
             A.tile_ovf[b] = s_ovf;
+            if (s_ovf > 0) {
+                const int i = atomicAdd(&A.ctl->novf[p], 1);
+                if (i < A.max_tiles) A.ovf_list[i] = b;
+            }
             accum_tile(bucket, tot);
             accum_lost(bucket, s_lost);
         }
@@ -681,7 +688,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 // permute_pass: the stayers' part of the next step's gather permutation.  A stayer of cell c with
 // rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
 // KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Movers are placed by
-// mover_rank.  A flat stream over the keys, no shared memory and no barriers.
+// mover_rank, after this kernel has listed each cell's incoming movers.  Flat streams over the
+// keys and the mover records, no shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
@@ -699,12 +707,20 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             if (b < 0 || b >= ntiles) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
             const int cloud = A.tile_cloud[b];
             c = A.clouds[cloud].ovf_cell;
-            base = A.tile_ovf_carry[b] - A.tile_ovf_carry[A.cdyn[cloud].tile_off[p]];
+            base = A.tile_ovf_carry[b];
         }
         if (c < 0 || c >= A.total_cells) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
         const int lo = A.new_start[c];
         const int dest = lo + base + rank;
         if (dest >= lo && dest < A.new_start[c + 1]) A.src_out[dest] = j;
+        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+    }
+    // incoming movers: each writes its old position into its cell's incoming slots (ticket order)
+    const int m = A.ctl->movers[p];
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
+        const int4 r = A.mrec[i];
+        const int slot = A.mover_base[r.x] + r.z;
+        if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
         else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
@@ -722,59 +738,126 @@ __device__ __forceinline__ int cloud_cell_end(const Args<R>& A, int cloud) {
     return A.clouds[cloud].ovf_cell + 1;
 }
 
-template <class R>
-__global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
-    __shared__ uint32_t wsum[32];
-    const int blk = blockIdx.x;
-    const int cloud = A.scan_blk_cloud[blk];
-    const int c0 = A.scan_blk_cell0[blk];
-    const int cend = cloud_cell_end(A, cloud);
-    uint32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
-        if (c < cend) s += (uint32_t)((A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c]);
+// Step totals of cloud k from its buckets (one warp; the buckets are cleared), the knife
+// temperature of the coming step, and on cloud 0 the step counter of the coming step.
+template <class R, bool INIT>
+__device__ __forceinline__ void finalize_cloud(const Args<R>& A, int k, int lane) {
+    static_assert(ACC_BUCKETS <= 32, "one lane per bucket");
+    const int p = A.parity;
+    CloudDyn& d = A.cdyn[k];
+    TilePartial acc;
+    zero_partial(acc);
+    if (lane < ACC_BUCKETS) {
+        CloudAccum& g = A.accum[k * ACC_BUCKETS + lane];
+        acc.sum_v2 = from_limbs(g.v2);
+        acc.sum_B = from_limbs(g.B);
+        acc.evap_v2 = from_limbs(g.ev2);
+        acc.evap_B = from_limbs(g.eB);
+        acc.n_alive = (long long)g.n_alive;
+        acc.n_maj = (long long)g.n_maj;
+        acc.n_knife = (long long)g.n_knife;
+        acc.coll = (long long)g.coll;
+        acc.cand = (long long)g.cand;
+        CloudAccum z = {};
+        g = z;  // cleared for the next step
     }
-    uint32_t tot;
-    block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
-    if (threadIdx.x == 0) A.block_sums[blk] = (int)tot;
+    acc.sum_v2 = warp_sum_i128(acc.sum_v2);
+    acc.sum_B = warp_sum_i128(acc.sum_B);
+    acc.evap_v2 = warp_sum_i128(acc.evap_v2);
+    acc.evap_B = warp_sum_i128(acc.evap_B);
+    acc.n_alive = warp_sum_ll(acc.n_alive);
+    acc.n_maj = warp_sum_ll(acc.n_maj);
+    acc.n_knife = warp_sum_ll(acc.n_knife);
+    acc.coll = warp_sum_ll(acc.coll);
+    acc.cand = warp_sum_ll(acc.cand);
+    if (lane == 0) {
+        const CloudPhys<R>& P = A.clouds[k];
+        CloudDiagDev& g = A.cdiag[k];
+        const int step_now = A.ctl->step[p];
+        if (INIT) {
+            g.step = step_now;
+            g.cum_evap = 0; g.cum_maj = 0; g.cum_knife = 0; g.cum_coll = 0; g.cum_cand = 0;
+            g.cum_evap_v2 = 0; g.cum_evap_B = 0; g.cum_atom_steps = 0;
+        } else {
+            g.step = step_now + 1;
+            g.cum_evap += acc.n_maj + acc.n_knife;
+            g.cum_maj += acc.n_maj;
+            g.cum_knife += acc.n_knife;
+            g.cum_coll += acc.coll;
+            g.cum_cand += acc.cand;
+            g.cum_evap_v2 += acc.evap_v2;
+            g.cum_evap_B += acc.evap_B;
+            g.cum_atom_steps += acc.n_alive + acc.n_maj + acc.n_knife;
+        }
+        g.n_alive = acc.n_alive;
+        g.sum_v2 = acc.sum_v2;
+        g.sum_B = acc.sum_B;
+        g.err = A.ctl->err;
+        d.T_knife = knife_temperature(P.mass, P.kB, P.T0, (P.flags & F_KNIFE_FIXED_T) != 0, acc.sum_v2,
+                                      acc.n_alive);
+        if (k == 0 && !INIT) {
+            A.ctl->step[1 - p] = step_now + 1;
+            if (A.clog_off) {
+                const int rel = step_now + 1 - A.clog_step0;
+                const int cnt = *A.clog_count;
+                if (rel >= 1 && rel <= A.clog_steps) A.clog_off[rel] = cnt < A.clog_cap ? cnt : A.clog_cap;
+            }
+        }
+    }
 }
 
-// single block: block offsets, per-cloud totals and tilings for the next step, overflow carries
-template <class R>
-__global__ void __launch_bounds__(1024) scan_top(Args<R> A) {
+// diagnostics of the sorted state after initialisation (one warp per cloud)
+template <class R, bool INIT>
+__global__ void __launch_bounds__(32) finalize(Args<R> A) {
+    finalize_cloud<R, INIT>(A, blockIdx.x, threadIdx.x);
+}
+
+// Top level of the cell scan, run by the last scan_reduce block: offsets of the scan blocks,
+// per-cloud counts, starts and tilings of the coming step, the overflow-cell carries of the
+// listed tiles, and the coming step's counters.
+template <class R, int BLOCK>
+__device__ void scan_top_block(const Args<R>& A) {
     __shared__ uint32_t wsum[32];
-    __shared__ int s_carry;
+    __shared__ int s_carry, s_tcarry;
     const int p = A.parity, q = 1 - p;
-    // 1. exclusive scan of block sums
+    // 1. exclusive scan of the block sums (written by the other blocks of this kernel: read from L2)
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
-    for (int base = 0; base < A.nscan_blocks; base += 1024) {
-        const int i = base + threadIdx.x;
-        const uint32_t v = i < A.nscan_blocks ? (uint32_t)A.block_sums[i] : 0u;
+    for (int base = 0; base < A.nscan_blocks; base += BLOCK * SCAN_ITEMS) {
+        const int i0 = base + threadIdx.x * SCAN_ITEMS;
+        int v[SCAN_ITEMS];
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            v[k] = i0 + k < A.nscan_blocks ? __ldcg(A.block_sums + i0 + k) : 0;
+            s += (uint32_t)v[k];
+        }
         uint32_t tot;
-        const uint32_t ex = block_excl_scan_u32<1024>(v, wsum, tot);
-        if (i < A.nscan_blocks) A.block_off[i] = (int)ex + s_carry;
+        uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            if (i0 + k < A.nscan_blocks) A.block_off[i0 + k] = (int)ex;
+            ex += (uint32_t)v[k];
+        }
         __syncthreads();
         if (threadIdx.x == 0) s_carry += (int)tot;
         __syncthreads();
     }
     const int total = s_carry;
-    // 2. per-cloud counts, starts, tile offsets (clouds in chunks of 1024)
-    __shared__ int s_tcarry;
+    // 2. per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK)
     if (threadIdx.x == 0) s_tcarry = 0;
     __syncthreads();
-    for (int base = 0; base < A.nclouds; base += 1024) {
+    for (int base = 0; base < A.nclouds; base += BLOCK) {
         const int k = base + threadIdx.x;
         int n = 0, st = 0, nt = 0;
         if (k < A.nclouds) {
             const int fb = A.cloud_first_blk[k], lb = A.cloud_first_blk[k + 1] - 1;
             st = A.block_off[fb];
-            n = A.block_off[lb] + A.block_sums[lb] - st;
+            n = A.block_off[lb] + __ldcg(A.block_sums + lb) - st;
             nt = (n + A.tile_nominal - 1) / A.tile_nominal;
         }
         uint32_t tot;
-        const uint32_t ex = block_excl_scan_u32<1024>((uint32_t)nt, wsum, tot);
+        const uint32_t ex = block_excl_scan_u32<BLOCK>((uint32_t)nt, wsum, tot);
         if (k < A.nclouds) {
             CloudDyn& d = A.cdyn[k];
             d.n[q] = n;
@@ -793,10 +876,12 @@ __global__ void __launch_bounds__(1024) scan_top(Args<R> A) {
         if (ntiles_next > A.max_tiles) atomicOr(&A.ctl->err, EB_TILE_OVERFLOW);
         A.new_start[A.total_cells] = total;
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
+        A.ctl->movers[q] = 0;
+        A.ctl->novf[q] = 0;
     }
     // 3. cloud of every next tile: binary search of the per-cloud first tiles (a one-cloud
     //    handle's table is all zeros from the start)
-    for (int t = threadIdx.x; A.nclouds > 1 && t < ntiles_next && t < A.max_tiles; t += 1024) {
+    for (int t = threadIdx.x; A.nclouds > 1 && t < ntiles_next && t < A.max_tiles; t += BLOCK) {
         int lo = 0, hi = A.nclouds;  // largest k with tile_off[k] <= t and ntiles[k] > 0
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -805,33 +890,53 @@ __global__ void __launch_bounds__(1024) scan_top(Args<R> A) {
         while (lo + 1 < A.nclouds && A.cdyn[lo + 1].tile_off[q] <= t) ++lo;
         A.tile_cloud_next[t] = lo;
     }
-    // 4. overflow-stayer prefix over the current tiles: tile_ovf_carry[b] = sum of tile_ovf over
-    //    tiles before b; the carry of a tile is this prefix minus the prefix at its cloud's first tile.
+    // 4. overflow-cell carry of each listed tile: the overflow-cell stayers of the listed tiles
+    //    of the same cloud before it (only tiles holding such stayers are listed)
     if (!A.init_mode) {
-        constexpr int IT = 16;
-        const int nt = A.ctl->ntiles[p];
-        if (threadIdx.x == 0) s_carry = 0;
-        __syncthreads();
-        for (int base = 0; base < nt; base += 1024 * IT) {
-            const int i0 = base + threadIdx.x * IT;
-            int v[IT];
-            uint32_t s = 0;
-#pragma unroll
-            for (int k = 0; k < IT; ++k) {
-                v[k] = (i0 + k < nt) ? A.tile_ovf[i0 + k] : 0;
-                s += (uint32_t)v[k];
+        const int m = min(A.ctl->novf[p], A.max_tiles);
+        for (int i = threadIdx.x; i < m; i += BLOCK) {
+            const int bi = A.ovf_list[i];
+            const int ci = A.tile_cloud[bi];
+            int carry = 0;
+            for (int j = 0; j < m; ++j) {
+                const int bj = A.ovf_list[j];
+                if (bj < bi && A.tile_cloud[bj] == ci) carry += A.tile_ovf[bj];
             }
-            uint32_t tot;
-            uint32_t ex = block_excl_scan_u32<1024>(s, wsum, tot) + (uint32_t)s_carry;
-#pragma unroll
-            for (int k = 0; k < IT; ++k) {
-                if (i0 + k < nt) A.tile_ovf_carry[i0 + k] = (int)ex;
-                ex += (uint32_t)v[k];
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) s_carry += (int)tot;
-            __syncthreads();
+            A.tile_ovf_carry[bi] = carry;
         }
+    }
+}
+
+// Block sums of the coming cell counts; the last block to finish runs the top level of the scan
+// and, for a physics step, the per-cloud step totals.
+template <class R>
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
+    __shared__ uint32_t wsum[32];
+    __shared__ int s_last;
+    const int blk = blockIdx.x;
+    const int cloud = A.scan_blk_cloud[blk];
+    const int c0 = A.scan_blk_cell0[blk];
+    const int cend = cloud_cell_end(A, cloud);
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
+        if (c < cend) s += (uint32_t)((A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c]);
+    }
+    uint32_t tot;
+    block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
+    if (threadIdx.x == 0) {
+        A.block_sums[blk] = (int)tot;
+        __threadfence();
+        s_last = atomicAdd(&A.ctl->scan_done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) A.ctl->scan_done = 0;
+    scan_top_block<R, SCAN_BLOCK>(A);
+    if (!A.init_mode) {
+        for (int k = threadIdx.x >> 5; k < A.nclouds; k += SCAN_BLOCK / 32) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
     }
 }
 
@@ -865,6 +970,8 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
     const int S = d.start[q];
     const int toff = d.tile_off[q];
     const int T = A.tile_nominal;
+    // nominal tile starts S + j*T: the first at or after this thread's first cell, then in order
+    int j = ((int)ex - S + T - 1) / T;
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
         const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
@@ -874,40 +981,22 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
             if (in[k] > 0) A.mover_base[c] = st + oldc[k] - lv[k];
             if (lv[k]) A.Lc[c] = 0;
             if (in[k]) A.Ic[c] = 0;
-            if (cnt[k] > 0) {
-                const int e = st + cnt[k];
-                // nominal tile starts S + j*T falling in [st, e)
-                int j = (st - S + T - 1) / T;
-                for (; S + j * T < e; ++j) {
-                    const int pnom = S + j * T;
-                    int tbeg;
-                    if (pnom == st) tbeg = st;
-                    else tbeg = (c == ovf) ? pnom : e;
-                    const int ti = toff + j;
-                    if (ti < A.max_tiles) A.tile_begin_next[ti] = tbeg;
-                }
+            const int e = st + cnt[k];
+            for (; S + j * T < e; ++j) {  // nominal starts inside this cell snap to its end
+                const int pnom = S + j * T;
+                const int tbeg = pnom == st ? st : (c == ovf ? pnom : e);
+                const int ti = toff + j;
+                if (ti < A.max_tiles) A.tile_begin_next[ti] = tbeg;
             }
             ex += (uint32_t)cnt[k];
         }
     }
 }
 
-// incoming movers: each writes its old position into its cell's incoming slots (ticket order)
-template <class R>
-__global__ void __launch_bounds__(256) mover_place(Args<R> A) {
-    const int m = A.ctl->movers;
-    for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
-        const int4 r = A.mrec[i];
-        const int slot = A.mover_base[r.x] + r.z;
-        if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
-        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
-    }
-}
-
 // rank = number of incoming movers of the same cell with a smaller old position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
-    const int m = A.ctl->movers;
+    const int m = A.ctl->movers[A.parity];
     for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
         const int4 r = A.mrec[i];
         const int lo = A.mover_base[r.x];
@@ -920,75 +1009,6 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
         for (int k = lo; k < hi; ++k) rank += (A.in_list[k] < r.y) ? 1 : 0;
         if (lo + rank < hi && r.y >= 0 && r.y < A.capacity) A.src_out[lo + rank] = r.y;
         else atomicOr(&A.ctl->err, EB_INCONSISTENT);
-    }
-}
-
-// per-cloud diagnostics from the tile partials; block k handles cloud k
-template <class R, bool INIT>
-__global__ void __launch_bounds__(32) finalize(Args<R> A) {
-    static_assert(ACC_BUCKETS <= 32, "one lane per bucket");
-    const int p = A.parity;
-    const int k = blockIdx.x;
-    CloudDyn& d = A.cdyn[k];
-    TilePartial acc;
-    zero_partial(acc);
-    if (threadIdx.x < ACC_BUCKETS) {
-        CloudAccum& g = A.accum[k * ACC_BUCKETS + threadIdx.x];
-        acc.sum_v2 = from_limbs(g.v2);
-        acc.sum_B = from_limbs(g.B);
-        acc.evap_v2 = from_limbs(g.ev2);
-        acc.evap_B = from_limbs(g.eB);
-        acc.n_alive = (long long)g.n_alive;
-        acc.n_maj = (long long)g.n_maj;
-        acc.n_knife = (long long)g.n_knife;
-        acc.coll = (long long)g.coll;
-        acc.cand = (long long)g.cand;
-        CloudAccum z = {};
-        g = z;  // cleared for the next step
-    }
-    acc.sum_v2 = warp_sum_i128(acc.sum_v2);
-    acc.sum_B = warp_sum_i128(acc.sum_B);
-    acc.evap_v2 = warp_sum_i128(acc.evap_v2);
-    acc.evap_B = warp_sum_i128(acc.evap_B);
-    acc.n_alive = warp_sum_ll(acc.n_alive);
-    acc.n_maj = warp_sum_ll(acc.n_maj);
-    acc.n_knife = warp_sum_ll(acc.n_knife);
-    acc.coll = warp_sum_ll(acc.coll);
-    acc.cand = warp_sum_ll(acc.cand);
-    if (threadIdx.x == 0) {
-        const CloudPhys<R>& P = A.clouds[k];
-        CloudDiagDev& g = A.cdiag[k];
-        const int step_now = A.ctl->step[p];
-        if (INIT) {
-            g.step = step_now;
-            g.cum_evap = 0; g.cum_maj = 0; g.cum_knife = 0; g.cum_coll = 0; g.cum_cand = 0;
-            g.cum_evap_v2 = 0; g.cum_evap_B = 0; g.cum_atom_steps = 0;
-        } else {
-            g.step = step_now + 1;
-            g.cum_evap += acc.n_maj + acc.n_knife;
-            g.cum_maj += acc.n_maj;
-            g.cum_knife += acc.n_knife;
-            g.cum_coll += acc.coll;
-            g.cum_cand += acc.cand;
-            g.cum_evap_v2 += acc.evap_v2;
-            g.cum_evap_B += acc.evap_B;
-            g.cum_atom_steps += acc.n_alive + acc.n_maj + acc.n_knife;
-        }
-        g.n_alive = acc.n_alive;
-        g.sum_v2 = acc.sum_v2;
-        g.sum_B = acc.sum_B;
-        g.err = A.ctl->err;
-        d.T_knife = knife_temperature(P.mass, P.kB, P.T0, (P.flags & F_KNIFE_FIXED_T) != 0, acc.sum_v2,
-                                      acc.n_alive);
-        if (k == 0 && !INIT) {
-            A.ctl->step[1 - p] = step_now + 1;
-            A.ctl->movers = 0;
-            if (A.clog_off) {
-                const int rel = step_now + 1 - A.clog_step0;
-                const int cnt = *A.clog_count;
-                if (rel >= 1 && rel <= A.clog_steps) A.clog_off[rel] = cnt < A.clog_cap ? cnt : A.clog_cap;
-            }
-        }
     }
 }
 

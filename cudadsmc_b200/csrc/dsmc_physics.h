@@ -320,27 +320,26 @@ DSMC_HD double xexp(double x) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Exact fixed-point accumulation for diagnostics: a non-negative double d (< 2^62) maps to
-// round-toward-zero(d * 2^64) as a 128-bit integer.  Sums of these are exact and therefore
-// independent of summation order (GPU tiles, CPU loop, batched or single clouds).
+// Exact fixed-point accumulation for diagnostics: a non-negative value d, clamped to 2^38
+// (no physical v^2 or |B| comes near; NaN clamps too), maps to floor(d * 2^64) as a 128-bit
+// integer.  Sums of these are exact and therefore independent of summation order (GPU tiles,
+// CPU loop, batched or single clouds).  The integer part and the fraction scaled by 2^64 are
+// both exact in the value's own precision, so the float and double forms agree bit for bit
+// on every float input.
 // ---------------------------------------------------------------------------------------
 DSMC_HD i128 fx_from(double d) {
-    double h = xfloor(d);
-    int64_t hi = (int64_t)h;
-    double fr = (d - h) * 0x1p64;
-    uint64_t lo = (uint64_t)fr;
+    if (!(d < 0x1p38)) d = 0x1p38;
+    const double h = xfloor(d);
+    const int64_t hi = (int64_t)h;
+    const uint64_t lo = (uint64_t)((d - h) * 0x1p64);
     return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
 }
-// the same value for a non-negative float, from its bits: f = M 2^(E-150) for the 24-bit
-// significand M, so f 2^64 = M 2^(E-86) -- a shift, no floating-point work
 DSMC_HD i128 fx_from(float f) {
-    const uint32_t u = f2u(f);
-    const int E = (int)(u >> 23);
-    if (E == 0) return 0;  // zero or subnormal: below 2^-64
-    const unsigned __int128 M = (unsigned __int128)((u & 0x7FFFFFu) | 0x800000u);
-    const int sh = E - 86;
-    if (sh > 100) return (i128)((unsigned __int128)1 << 124);  // beyond 2^38: not a physical v^2 or |B|
-    return (i128)(sh >= 0 ? (M << sh) : (sh > -24 ? (M >> -sh) : (unsigned __int128)0));
+    if (!(f < 0x1p38f)) f = 0x1p38f;
+    const float h = xfloor(f);
+    const int64_t hi = (int64_t)h;
+    const uint64_t lo = (uint64_t)((f - h) * 0x1p64f);
+    return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
 }
 DSMC_HD double fx_to_double(i128 q) {
     int64_t hi = (int64_t)(q >> 64);

@@ -46,6 +46,7 @@ def load() -> C.CDLL:
             "oracle_philox": (None, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
             "oracle_math_f": (None, [i32, C.POINTER(C.c_float), C.POINTER(C.c_float), i64]),
             "oracle_math_d": (None, [i32, C.POINTER(C.c_double), C.POINTER(C.c_double), i64]),
+            "oracle_fx": (None, [i32, C.c_void_p, C.POINTER(C.c_uint64), i64]),
             "oracle_field_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), i64]),
             "oracle_smooth_loss": (C.c_double, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
@@ -77,6 +78,20 @@ def philox4x32_10(ctr, key) -> np.ndarray:
     o = (C.c_uint32 * 4)()
     load().oracle_philox(c, k, o)
     return np.array(list(o), np.uint32)
+
+
+def fixed_point(x: np.ndarray) -> list:
+    """The diagnostics' exact fixed-point value floor(min(x, 2^38) * 2^64) of each element (float32
+    elements through the float form, float64 through the double form), as Python ints."""
+    x = np.ascontiguousarray(x)
+    out = np.zeros(2 * x.size, np.uint64)
+    prec = 0 if x.dtype == np.float32 else 1
+    load().oracle_fx(prec, x.ctypes.data, out.ctypes.data_as(C.POINTER(C.c_uint64)), x.size)
+    vals = []
+    for lo, hi in zip(out[0::2], out[1::2]):
+        v = int(lo) | (int(hi) << 64)
+        vals.append(v - (1 << 128) if v >> 127 else v)
+    return vals
 
 
 def math(which: str, x: np.ndarray) -> np.ndarray:

@@ -477,6 +477,15 @@ OAPI void oracle_math_f(int which, const float* x, float* y, int64_t n) {
         }
     }
 }
+// the diagnostics' fixed-point conversion of each value (prec DSMC_FP32: the float form, else
+// the double form), as (low 64 bits, high 64 bits) pairs
+OAPI void oracle_fx(int prec, const void* x, uint64_t* out, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        const i128 q = prec == DSMC_FP32 ? fx_from(((const float*)x)[i]) : fx_from(((const double*)x)[i]);
+        out[2 * i] = (uint64_t)q;
+        out[2 * i + 1] = (uint64_t)((unsigned __int128)q >> 64);
+    }
+}
 OAPI void oracle_math_d(int which, const double* x, double* y, int64_t n) {
     for (int64_t i = 0; i < n; ++i) {
         double s, c;

@@ -165,7 +165,7 @@ def test_profiling_mode_identical():
     orc.step(5)
     assert_same(a, orc)
     t = a.kernel_times()
-    assert len(t) == a.launches_per_step() == 8
+    assert len(t) == a.launches_per_step() == 5
     assert all(v[1] == 5 for v in t.values())
 
 
