@@ -286,7 +286,8 @@ def main():
         sim2.set_state(pin["pos"].numpy(), pin["vel"].numpy(), pin["psi"].numpy(), counts)
         sim2.step(args.warmup)
         sim2.synchronize()
-        out = {k: torch.empty_like(v).pin_memory() for k, v in pin.items()}
+        out = {k: torch.empty((c.capacity, 4), dtype=v.dtype).pin_memory() for k, v in pin.items()}
+        out_np = {k: v.numpy() for k, v in out.items()}
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -298,7 +299,7 @@ def main():
         for _ in range(args.steps):
             sim2.step(1)
             dd = sim2.diagnostics()
-        st2 = sim2.get_state()
+        st2 = sim2.get_state(out=out_np)
         ee1 = torch.cuda.Event(enable_timing=True)
         ee1.record(stream)
         ee1.synchronize()

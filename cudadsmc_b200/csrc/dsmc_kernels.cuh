@@ -84,6 +84,7 @@ struct Ctl {
     int err;
     int movers[2];  // movers listed by the step of each parity (the other parity's is cleared by the scan)
     int novf[2];    // tiles with overflow-cell stayers listed by the step of each parity
+    int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds prefixes from there on
     int scan_done;  // scan_reduce blocks finished (the last one runs the top level and clears it)
 };
 
@@ -707,7 +708,8 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             if (b < 0 || b >= ntiles) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
             const int cloud = A.tile_cloud[b];
             c = A.clouds[cloud].ovf_cell;
-            base = A.tile_ovf_carry[b];
+            const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
+            base = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
         }
         if (c < 0 || c >= A.total_cells) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
         const int lo = A.new_start[c];
@@ -813,7 +815,7 @@ __global__ void __launch_bounds__(32) finalize(Args<R> A) {
 }
 
 // Top level of the cell scan, run by the last scan_reduce block: offsets of the scan blocks,
-// per-cloud counts, starts and tilings of the coming step, the overflow-cell carries of the
+// per-cloud counts, starts and tile offsets of the coming step, the overflow-cell carries of the
 // listed tiles, and the coming step's counters.
 template <class R, int BLOCK>
 __device__ void scan_top_block(const Args<R>& A) {
@@ -879,36 +881,52 @@ __device__ void scan_top_block(const Args<R>& A) {
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
     }
-    // 3. cloud of every next tile: binary search of the per-cloud first tiles (a one-cloud
-    //    handle's table is all zeros from the start)
-    for (int t = threadIdx.x; A.nclouds > 1 && t < ntiles_next && t < A.max_tiles; t += BLOCK) {
-        int lo = 0, hi = A.nclouds;  // largest k with tile_off[k] <= t and ntiles[k] > 0
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (A.cdyn[mid].tile_off[q] <= t) lo = mid; else hi = mid;
-        }
-        while (lo + 1 < A.nclouds && A.cdyn[lo + 1].tile_off[q] <= t) ++lo;
-        A.tile_cloud_next[t] = lo;
-    }
-    // 4. overflow-cell carry of each listed tile: the overflow-cell stayers of the listed tiles
-    //    of the same cloud before it (only tiles holding such stayers are listed)
+    // 3. overflow-cell stayers: exclusive prefix of tile_ovf over the tiles from the lowest to the
+    //    highest listed one (tile_ovf is zero on every unlisted tile, so a listed tile's carry is
+    //    its prefix minus the prefix at its cloud's first tile, or at the lowest listed tile)
     if (!A.init_mode) {
+        __shared__ int s_lo, s_hi;
+        if (threadIdx.x == 0) {
+            s_lo = 0x7fffffff;
+            s_hi = -1;
+        }
+        __syncthreads();
         const int m = min(A.ctl->novf[p], A.max_tiles);
         for (int i = threadIdx.x; i < m; i += BLOCK) {
-            const int bi = A.ovf_list[i];
-            const int ci = A.tile_cloud[bi];
-            int carry = 0;
-            for (int j = 0; j < m; ++j) {
-                const int bj = A.ovf_list[j];
-                if (bj < bi && A.tile_cloud[bj] == ci) carry += A.tile_ovf[bj];
+            const int b = A.ovf_list[i];
+            atomicMin(&s_lo, b);
+            atomicMax(&s_hi, b);
+        }
+        __syncthreads();
+        const int lo = s_lo, hi = s_hi;
+        if (threadIdx.x == 0) A.ctl->ovf_lo[p] = lo;
+        constexpr int IT = 16;
+        if (threadIdx.x == 0) s_carry = 0;
+        __syncthreads();
+        for (int base = lo; base <= hi; base += BLOCK * IT) {
+            const int i0 = base + threadIdx.x * IT;
+            int v[IT];
+            uint32_t s = 0;
+#pragma unroll
+            for (int k = 0; k < IT; ++k) {
+                v[k] = (i0 + k <= hi) ? A.tile_ovf[i0 + k] : 0;
+                s += (uint32_t)v[k];
             }
-            A.tile_ovf_carry[bi] = carry;
+            uint32_t tot;
+            uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
+#pragma unroll
+            for (int k = 0; k < IT; ++k) {
+                if (i0 + k <= hi) A.tile_ovf_carry[i0 + k] = (int)ex;
+                ex += (uint32_t)v[k];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry += (int)tot;
+            __syncthreads();
         }
     }
 }
 
-// Block sums of the coming cell counts; the last block to finish runs the top level of the scan
-// and, for a physics step, the per-cloud step totals.
+// Block sums of the coming cell counts; the last block to finish runs the top level of the scan.
 template <class R>
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
     __shared__ uint32_t wsum[32];
@@ -935,16 +953,17 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
     __threadfence();
     if (threadIdx.x == 0) A.ctl->scan_done = 0;
     scan_top_block<R, SCAN_BLOCK>(A);
-    if (!A.init_mode) {
-        for (int k = threadIdx.x >> 5; k < A.nclouds; k += SCAN_BLOCK / 32) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
-    }
 }
 
+// New cell starts, the movers' base slots and the coming step's tiles (start and cloud); cleared
+// leaver / incoming counters.  In a physics step, block k < nclouds also closes cloud k's step
+// totals (every cloud has at least one scan block).
 template <class R>
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
     __shared__ uint32_t wsum[32];
     const int q = 1 - A.parity;
     const int blk = blockIdx.x;
+    if (!A.init_mode && blk < A.nclouds && threadIdx.x < 32) finalize_cloud<R, false>(A, blk, threadIdx.x);
     const int cloud = A.scan_blk_cloud[blk];
     const int c0 = A.scan_blk_cell0[blk];
     const int cend = cloud_cell_end(A, cloud);
@@ -986,7 +1005,10 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
                 const int pnom = S + j * T;
                 const int tbeg = pnom == st ? st : (c == ovf ? pnom : e);
                 const int ti = toff + j;
-                if (ti < A.max_tiles) A.tile_begin_next[ti] = tbeg;
+                if (ti < A.max_tiles) {
+                    A.tile_begin_next[ti] = tbeg;
+                    A.tile_cloud_next[ti] = cloud;
+                }
             }
             ex += (uint32_t)cnt[k];
         }

@@ -160,12 +160,21 @@ class Simulation:
     def n_alive(self) -> int:
         return int(self.diagnostics()["n_alive"])
 
-    def get_state(self) -> dict:
-        """Sorted state: pos/vel/psi as (n, 4) arrays, atom ids, cloud counts."""
+    def get_state(self, out: dict = None) -> dict:
+        """Sorted state: pos/vel/psi as (n, 4) arrays, atom ids, cloud counts.  `out` may give
+        C-contiguous (capacity, 4) arrays of the handle's precision for pos/vel/psi (pinned host
+        memory, say) to be filled instead of new ones."""
         cap = int(sum(max(c.capacity, c.n_atoms) for c in self.clouds))
-        pos = np.empty((cap, 4), self.dtype)
-        vel = np.empty((cap, 4), self.dtype)
-        psi = np.empty((cap, 4), self.dtype)
+        if out is not None:
+            pos, vel, psi = out["pos"], out["vel"], out["psi"]
+            for a in (pos, vel, psi):
+                if a.dtype != self.dtype or a.ndim != 2 or a.shape[1] != 4 or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError("out arrays must be C-contiguous (capacity, 4) of the handle's precision")
+            cap = min(a.shape[0] for a in (pos, vel, psi))
+        else:
+            pos = np.empty((cap, 4), self.dtype)
+            vel = np.empty((cap, 4), self.dtype)
+            psi = np.empty((cap, 4), self.dtype)
         counts = np.zeros(len(self.clouds), np.int64)
         b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, cap,
                          counts.ctypes.data_as(C.POINTER(C.c_int64)))
