@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=50)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -125,6 +127,44 @@ def cpu_baseline(run, cloud, steps: int, threads: int | None = None) -> dict:
     return {"value": atom_steps / (t1 - t0), "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{cloud.n_atoms:.0e} atoms, {steps} timed steps after init + 1 warm-up step "
                       f"({t1 - t0:.1f} s), OpenMP float build of oracle/dsmc_oracle.cpp"}
+
+
+def adjoint_vs_plain(stream, steps: int, checkpoint_every: int) -> dict:
+    """The adjoint workload (1e6 atoms, 0.1 mT bias, 30 uK, 8-segment knife ramp): device time of a
+    plain forward run of `steps` steps against the pathwise-adjoint call on the same cloud (the
+    recorded physical run + the smoothed forward + the checkpointed recomputation and adjoint), in
+    FP32; the FP64 adjoint's gradient gives the FP32 drift."""
+    import numpy as np
+    import torch
+    from cudadsmc_b200 import FP32, FP64, Simulation, preset
+    run, c = preset(4)
+    plain = Simulation(run, c)
+    plain.set_stream(stream.cuda_stream)
+    plain.init_cloud(4321)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    plain.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    plain.close()
+    grads = {}
+    for prec, name in ((FP32, "fp32"), (FP64, "fp64")):
+        s = Simulation(run, c)
+        s.set_stream(stream.cuda_stream)
+        s.init_cloud(4321)
+        grads[name] = s.adjoint_run(steps, checkpoint_every=checkpoint_every, precision=prec, sigmoid_width_kT=0.2)
+        s.close()
+    g = grads["fp32"]
+    vec = lambda d: np.array([d["dL_dBp"], d["dL_dB0"]] + list(d["dL_deta"]))
+    g32, g64 = vec(grads["fp32"]), vec(grads["fp64"])
+    scale = np.max(np.abs(g64))
+    return {"atoms": c.n_atoms, "steps": steps, "checkpoint_every": checkpoint_every, "precision": "fp32",
+            "ms_plain_forward": ms_plain, "ms_record": g["ms_record"], "ms_smoothed_forward": g["ms_forward"],
+            "ms_adjoint": g["ms_backward"],
+            "fwd_adjoint_over_plain": (g["ms_record"] + g["ms_forward"] + g["ms_backward"]) / ms_plain,
+            "collisions_recorded": g["collisions"], "loss": g["loss"],
+            "grad_fp32_vs_fp64_max_abs_over_max": float(np.max(np.abs(g32 - g64)) / scale) if scale > 0 else 0.0}
 
 
 def batched_vs_sequential(stream, steps: int) -> dict:
@@ -330,6 +370,11 @@ def main():
     if rank == 0 and ws == 1 and not args.no_batched:
         batched = batched_vs_sequential(stream, steps=args.batched_steps)
 
+    # ------------------------------------------------------------------ forward + adjoint vs plain
+    adjoint = None
+    if rank == 0 and ws == 1 and not args.no_adjoint:
+        adjoint = adjoint_vs_plain(stream, steps=args.adjoint_steps, checkpoint_every=100)
+
     # ------------------------------------------------------------------ CPU baseline
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -346,7 +391,7 @@ def main():
                            "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
                            "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"},
                 "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint,
                 "n_alive_end": d1["n_alive"]}
         print(json.dumps(line), flush=True)
     sim.close()

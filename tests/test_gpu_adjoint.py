@@ -90,3 +90,31 @@ def test_torch_autograd_function():
     assert loss.item() == g["loss"]
     ref = np.array([g["dL_dBp"], g["dL_dB0"]] + g["dL_deta"])
     np.testing.assert_allclose(th.grad.numpy(), ref, rtol=1e-9, atol=1e-14)
+
+
+def test_adjoint_workload_scale_finite_differences():
+    # the adjoint workload as configured (1e6 atoms, 0.1 mT bias, 30 uK, 8-segment ramp over 2000
+    # steps, K = 100, sigmoid width 0.2 kT): FP64 adjoint against common-random-number central
+    # differences (h = 1e-4 relative) of the smoothed loss, 1e-3 relative on every parameter the
+    # run is sensitive to
+    run, c = preset(4)
+    sim = Simulation(run, c)
+    sim.init_cloud(4321)
+    g = sim.adjoint_run(2000, checkpoint_every=100, precision=FP64, sigmoid_width_kT=0.2)
+    assert g["collisions"] > 0
+    th = theta_of(c)
+    assert sim.adjoint_loss(th) == g["loss"]
+    grad = np.array([g["dL_dBp"], g["dL_dB0"]] + g["dL_deta"])
+    scale = np.max(np.abs(grad * th))
+    checked = 0
+    for p in range(11):
+        h = 1e-4 * abs(th[p])
+        tp, tm = th.copy(), th.copy()
+        tp[p] += h
+        tm[p] -= h
+        fd = (sim.adjoint_loss(tp) - sim.adjoint_loss(tm)) / (2 * h)
+        if abs(fd * th[p]) < 1e-6 * scale:
+            continue  # a knot whose weight no atom feels
+        assert abs(grad[p] - fd) <= 1e-3 * abs(fd), (p, grad[p], fd)
+        checked += 1
+    assert checked >= 8
