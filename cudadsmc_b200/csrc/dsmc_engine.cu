@@ -964,6 +964,11 @@ DSMC_API dsmc_status dsmc_step(dsmc_handle* h, int32_t n) {
     NEED_H;
     return guard(h, [&] { h->step(n); });
 }
+DSMC_API dsmc_status dsmc_batch_create(const dsmc_params* run, const dsmc_cloud_params* clouds, int32_t nclouds,
+                                       dsmc_handle** out) {
+    return dsmc_create(run, clouds, nclouds, out);
+}
+DSMC_API dsmc_status dsmc_batch_step(dsmc_handle* h, int32_t n) { return dsmc_step(h, n); }
 DSMC_API dsmc_status dsmc_synchronize(dsmc_handle* h) {
     NEED_H;
     return guard(h, [&] { h->sync(); });

@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdsmc_b20
 EXPORTED_SYMBOLS = (
     "dsmc_abi_version", "dsmc_status_string", "dsmc_last_error", "dsmc_preset", "dsmc_create",
     "dsmc_destroy", "dsmc_set_stream", "dsmc_init_cloud", "dsmc_step", "dsmc_synchronize",
+    "dsmc_batch_create", "dsmc_batch_step",
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
     "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_export",
@@ -57,6 +58,8 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_set_stream": (i32, [vp, vp]),
         "dsmc_init_cloud": (i32, [vp, u64]),
         "dsmc_step": (i32, [vp, i32]),
+        "dsmc_batch_create": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), i32, C.POINTER(vp)]),
+        "dsmc_batch_step": (i32, [vp, i32]),
         "dsmc_synchronize": (i32, [vp]),
         "dsmc_diagnostics": (i32, [vp, i32, C.POINTER(Diag)]),
         "dsmc_get_state": (i32, [vp, C.POINTER(StateBuffers)]),

@@ -169,6 +169,13 @@ DSMC_API dsmc_status dsmc_preset(int32_t which, dsmc_params* run, dsmc_cloud_par
 
 DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params* clouds,
                                  int32_t nclouds, dsmc_handle** out);
+/* Batched names: many independent clouds in one handle, stepped together by one graph launch per
+ * two steps.  The same calls as dsmc_create / dsmc_step (a handle always holds 1..n clouds);
+ * spelled out for callers that keep batched and single-cloud code apart.  No counterpart in the
+ * reference, which runs one cloud per process. */
+DSMC_API dsmc_status dsmc_batch_create(const dsmc_params* run, const dsmc_cloud_params* clouds,
+                                       int32_t nclouds, dsmc_handle** out);
+DSMC_API dsmc_status dsmc_batch_step(dsmc_handle* h, int32_t nsteps);
 DSMC_API dsmc_status dsmc_destroy(dsmc_handle* h);
 DSMC_API dsmc_status dsmc_set_stream(dsmc_handle* h, void* cuda_stream);
 

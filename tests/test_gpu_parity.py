@@ -197,6 +197,22 @@ def test_batched_clouds_match_oracle_and_single_runs():
         ds, db = single.diagnostics(), sim.diagnostics(k)
         for f in ("n_alive", "sum_v2", "sum_absB", "collisions", "n_evaporated"):
             assert ds[f] == db[f], (k, f)
+    # the batched entry points are the same engine: dsmc_batch_create + dsmc_batch_step
+    import ctypes as C
+    from cudadsmc_b200 import _abi
+    from cudadsmc_b200.engine import load_library
+    lib = load_library()
+    arr = (_abi.CloudParams * len(clouds))(*clouds)
+    h = C.c_void_p()
+    assert lib.dsmc_batch_create(C.byref(run), arr, len(clouds), C.byref(h)) == 0
+    try:
+        assert lib.dsmc_init_cloud(h, C.c_uint64(1234)) == 0
+        assert lib.dsmc_batch_step(h, 25) == 0
+        d = _abi.Diag()
+        assert lib.dsmc_diagnostics(h, -1, C.byref(d)) == 0
+        assert d.n_alive == sim.diagnostics()["n_alive"] and d.sum_v2 == sim.diagnostics()["sum_v2"]
+    finally:
+        lib.dsmc_destroy(h)
 
 
 def test_set_state_unsorted_input():
