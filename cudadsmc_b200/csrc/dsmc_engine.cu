@@ -143,7 +143,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         nclouds = n;
         cp.assign(clouds, clouds + n);
         use_graphs = r.use_graphs != 0;
-        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP / 2;
+        // default nominal tile: a little under two passes of the block, since a tile snapped to
+        // cell boundaries overshoots its nominal size by part of a cell
+        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP / 2 - 16;
         if (tile_nominal > CAP / 2) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP / 2)};
         if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
@@ -600,7 +602,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
         if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
-        const int cands[] = {128, 192, 256, 384, 512, 768, 1024};
+        const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, 768, 960, 1024};
         int best = tile_nominal;
         double best_ms = 1e300;
         const bool prof = profiling;

@@ -485,8 +485,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             s_nhead = 0;
             s_ovf = 0;
         }
+        // each thread's cell pass reads only the positions it staged itself: its own copies
+        // suffice, the barrier after the pass publishes the cells and the staged tile
         cp_async_wait_all();
-        __syncthreads();
         for (int t = threadIdx.x; t < L; t += BLOCK) {
             const R4 q = s_pos[t];
             const int c = cell_of(P, q.x, q.y, q.z, box);
