@@ -48,7 +48,7 @@ template <class T> struct DevBuf {
     ~DevBuf() { free(); }
 };
 
-constexpr int kMinTile = 128;  // smallest tile the autotuner tries (sizes the tile tables)
+constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes the tile tables)
 
 // launch shape of the FP32 step_pass: threads per tile, atoms staged per tile (48 B + 4 B of
 // shared memory each), blocks per SM requested from the compiler
@@ -145,8 +145,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         use_graphs = r.use_graphs != 0;
         // default nominal tile: a little under two passes of the block, since a tile snapped to
         // cell boundaries overshoots its nominal size by part of a cell
-        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP / 2 - 16;
-        if (tile_nominal > CAP / 2) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP / 2)};
+        // preferred nominal tile: three passes of the block, less a part of a cell for the snap
+        // to cell boundaries (each step's scan lowers it where a cell is fuller than CAP - T + 1)
+        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP - BLOCK - 16;
+        // a grid cell holds at most CAP - T + 1 atoms (DSMC_ERR_CELL_FULL beyond): T <= CAP - 128
+        if (tile_nominal > CAP - 128) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP - 128)};
         if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
         allocate();
@@ -275,7 +278,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
-            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal;
+            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal; A.tile_cap = CAP;
             A.collide_every = run.collide_every; A.parity = p; A.init_mode = 0;
             A.seed = run.seed;
             A.capacity = capacity;
@@ -602,13 +605,13 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
         if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
-        const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, 768, 960, 1024};
+        const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, CAP - BLOCK - 16, 768, 960, 1024};
         int best = tile_nominal;
         double best_ms = 1e300;
         const bool prof = profiling;
         profiling = false;
         for (int T : cands) {
-            if (T > CAP / 2) continue;
+            if (T > CAP - 128) continue;
             set_tile(T);
             step(1);  // builds the tiling of size T
             CU(cudaEventRecord(ev[0], stream));

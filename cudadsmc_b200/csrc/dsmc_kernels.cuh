@@ -58,6 +58,9 @@ struct __align__(16) TilePartial {
 // them non-negative, below 2^126) is split into three 42-bit limbs, so a bucket's limb sum cannot
 // wrap before 2^21 tiles.  finalize recombines and clears the buckets.
 constexpr int ACC_BUCKETS = 16;
+
+// smallest nominal tile (sizes the tile tables: at most capacity / MIN_TILE + clouds + 2 tiles)
+constexpr int MIN_TILE = 128;
 struct __align__(16) CloudAccum {
     unsigned long long v2[3], B[3], ev2[3], eB[3];
     unsigned long long n_alive, n_maj, n_knife, coll, cand, pad[3];
@@ -86,6 +89,8 @@ struct Ctl {
     int novf[2];    // tiles with overflow-cell stayers listed by the step of each parity
     int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds prefixes from there on
     int scan_done;  // scan_reduce blocks finished (the last one runs the top level and clears it)
+    int max_cell;   // largest coming grid-cell count, gathered by scan_reduce (cleared by its top level)
+    int tile_T[2];  // nominal tile size of the tiling built for each parity
 };
 
 // sort keys written by step_pass for every current position j
@@ -134,6 +139,7 @@ template <class R> struct Args {
     const int* scan_blk_cell0;
     const int* cloud_first_blk;  // nclouds + 1
     int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
+    int tile_cap;  // atoms a tile can stage (CAP): a tiling of nominal size T fits cells of CAP - T + 1
     int capacity;
     // collision record (adjoint runs): pairs by atom id, directions, per-step offsets
     int2* clog_ij;
@@ -847,6 +853,10 @@ __device__ void scan_top_block(const Args<R>& A) {
         __syncthreads();
     }
     const int total = s_carry;
+    // the coming tiling's nominal size: the preferred size, or less where a cell holds so many
+    // atoms that a tile snapped to cell boundaries could outgrow the staging capacity
+    const int mc = __ldcg(&A.ctl->max_cell);
+    const int T = max(min(A.tile_nominal, A.tile_cap + 1 - mc), MIN_TILE);
     // 2. per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK)
     if (threadIdx.x == 0) s_tcarry = 0;
     __syncthreads();
@@ -857,7 +867,7 @@ __device__ void scan_top_block(const Args<R>& A) {
             const int fb = A.cloud_first_blk[k], lb = A.cloud_first_blk[k + 1] - 1;
             st = A.block_off[fb];
             n = A.block_off[lb] + __ldcg(A.block_sums + lb) - st;
-            nt = (n + A.tile_nominal - 1) / A.tile_nominal;
+            nt = (n + T - 1) / T;
         }
         uint32_t tot;
         const uint32_t ex = block_excl_scan_u32<BLOCK>((uint32_t)nt, wsum, tot);
@@ -881,6 +891,8 @@ __device__ void scan_top_block(const Args<R>& A) {
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
+        A.ctl->tile_T[q] = T;
+        A.ctl->max_cell = 0;
     }
     // 3. overflow-cell stayers: exclusive prefix of tile_ovf over the tiles from the lowest to the
     //    highest listed one (tile_ovf is zero on every unlisted tile, so a listed tile's carry is
@@ -936,16 +948,26 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
     const int cloud = A.scan_blk_cloud[blk];
     const int c0 = A.scan_blk_cell0[blk];
     const int cend = cloud_cell_end(A, cloud);
+    __shared__ int s_max;
+    if (threadIdx.x == 0) s_max = 0;
     uint32_t s = 0;
+    int m = 0;  // largest grid-cell count (the cloud's overflow cell, its last, is split across tiles)
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
         const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
-        if (c < cend) s += (uint32_t)((A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c]);
+        if (c < cend) {
+            const int cnt = (A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c];
+            s += (uint32_t)cnt;
+            if (c < cend - 1) m = max(m, cnt);
+        }
     }
+    m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
     uint32_t tot;
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
     block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
     if (threadIdx.x == 0) {
         A.block_sums[blk] = (int)tot;
+        if (s_max > 0) atomicMax(&A.ctl->max_cell, s_max);
         __threadfence();
         s_last = atomicAdd(&A.ctl->scan_done, 1) == (int)gridDim.x - 1;
     }
@@ -989,7 +1011,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
     const CloudDyn& d = A.cdyn[cloud];
     const int S = d.start[q];
     const int toff = d.tile_off[q];
-    const int T = A.tile_nominal;
+    const int T = A.ctl->tile_T[q];
     // nominal tile starts S + j*T: the first at or after this thread's first cell, then in order
     int j = ((int)ex - S + T - 1) / T;
 #pragma unroll

@@ -51,6 +51,46 @@ DSMC_HD double xceil(double x) { return ceil(x); }
 DSMC_HD float xrint(float x) { return rintf(x); }
 DSMC_HD double xrint(double x) { return rint(x); }
 
+// ---------------------------------------------------------------------------------------
+// Two independent lanes of arithmetic.  On sm_100 a float pair is one paired FP32 instruction
+// (FADD2 / FMUL2 / FFMA2), each lane an ordinary round-to-nearest IEEE operation; elsewhere
+// (double, the host) it is two scalar operations with the same results.
+// ---------------------------------------------------------------------------------------
+template <class R> struct V2 {
+    R x, y;
+};
+template <class R> DSMC_HD V2<R> v2(R a, R b) {
+    V2<R> r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+template <class R> DSMC_HD V2<R> v2s(R a) { return v2(a, a); }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+DSMC_HD V2<float> add2(V2<float> a, V2<float> b) {
+    const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+    return v2(r.x, r.y);
+}
+DSMC_HD V2<float> mul2(V2<float> a, V2<float> b) {
+    const float2 r = __fmul2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+    return v2(r.x, r.y);
+}
+DSMC_HD V2<float> fma2(V2<float> a, V2<float> b, V2<float> c) {
+    const float2 r = __ffma2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y), make_float2(c.x, c.y));
+    return v2(r.x, r.y);
+}
+#else
+DSMC_HD V2<float> add2(V2<float> a, V2<float> b) { return v2(a.x + b.x, a.y + b.y); }
+DSMC_HD V2<float> mul2(V2<float> a, V2<float> b) { return v2(a.x * b.x, a.y * b.y); }
+DSMC_HD V2<float> fma2(V2<float> a, V2<float> b, V2<float> c) { return v2(xfma(a.x, b.x, c.x), xfma(a.y, b.y, c.y)); }
+#endif
+DSMC_HD V2<double> add2(V2<double> a, V2<double> b) { return v2(a.x + b.x, a.y + b.y); }
+DSMC_HD V2<double> mul2(V2<double> a, V2<double> b) { return v2(a.x * b.x, a.y * b.y); }
+DSMC_HD V2<double> fma2(V2<double> a, V2<double> b, V2<double> c) {
+    return v2(xfma(a.x, b.x, c.x), xfma(a.y, b.y, c.y));
+}
+template <class R> DSMC_HD V2<R> sub2(V2<R> a, V2<R> b) { return add2(a, v2(-b.x, -b.y)); }
+
 DSMC_HD uint32_t f2u(float f) {
 #if defined(__CUDA_ARCH__)
     return __float_as_uint(f);
@@ -165,16 +205,15 @@ DSMC_HD void xsincos(float x, float* s, float* c) {
     r = xfma(-k, p3, r);
     float r2 = r * r;
     // sin r = r + r^3 (-1/3! + r^2 (1/5! + r^2 (-1/7! + r^2/9!)))
-    float ps = xfma(r2, 2.75573192e-6f, -1.98412698e-4f);
-    ps = xfma(r2, ps, 8.33333333e-3f);
-    ps = xfma(r2, ps, -1.66666667e-1f);
-    float sr = xfma(r * r2, ps, r);
     // cos r = 1 + r^2 (-1/2 + r^2 (1/4! + r^2 (-1/6! + r^2 (1/8! - r^2/10!))))
-    float pc = xfma(r2, -2.75573192e-7f, 2.48015873e-5f);
-    pc = xfma(r2, pc, -1.38888889e-3f);
-    pc = xfma(r2, pc, 4.16666667e-2f);
-    pc = xfma(r2, pc, -0.5f);
-    float cr = xfma(r2, pc, 1.0f);
+    // evaluated as one two-lane Horner chain (sin lane, cos lane)
+    const V2<float> rr = v2s(r2);
+    const float pc0 = xfma(r2, -2.75573192e-7f, 2.48015873e-5f);
+    V2<float> p = fma2(rr, v2(2.75573192e-6f, pc0), v2(-1.98412698e-4f, -1.38888889e-3f));
+    p = fma2(rr, p, v2(8.33333333e-3f, 4.16666667e-2f));
+    p = fma2(rr, p, v2(-1.66666667e-1f, -0.5f));
+    const V2<float> sc = fma2(v2(r * r2, r2), p, v2(r, 1.0f));
+    const float sr = sc.x, cr = sc.y;
     int q = ((int)k) & 3;
     float ss = (q & 1) ? cr : sr;
     float cc = (q & 1) ? sr : cr;
@@ -372,6 +411,7 @@ template <class R> struct CloudPhys {
     R inv_dx, inv_dy, inv_dz;
     R box_x, box_y, box_z;       // grid box edge lengths (periodic wrap)
     R inv_box_x, inv_box_y, inv_box_z;
+    R fnx, fny, fnz;              // nx, ny, nz as reals (the grid's extent in cell units)
     R Bp, Bpp, B0, B_floor;       // gradient, curvature, bias, trap-bottom |B|
     R dt, half_dt;
     R accel_scale;                // mu / m
@@ -423,18 +463,21 @@ DSMC_HD void trap_field(const CloudPhys<R>& P, R x, R y, R z, Field<R>& f) {
     if (P.trap == TRAP_QUADRUPOLE) {
         // B = (h x, h y, B0 - B' z), h = B'/2;  grad|B| = (h B^x, h B^y, -B' B^z)
         const R h = R(0.5) * P.Bp;
-        const R Bx = h * x, By = h * y, Bz = P.B0 - P.Bp * z;
-        const R b2 = Bx * Bx + By * By + Bz * Bz;
+        const V2<R> Bxy = mul2(v2s(h), v2(x, y));
+        const R Bz = xfma(-P.Bp, z, P.B0);
+        const R b2 = xfma(Bz, Bz, xfma(Bxy.y, Bxy.y, Bxy.x * Bxy.x));
         if (b2 > R(0)) {
             const R inv = xrsqrt(b2);
             f.absB = b2 * inv;
-            f.bx = Bx * inv; f.by = By * inv; f.bz = Bz * inv;
+            const V2<R> bxy = mul2(Bxy, v2s(inv));
+            f.bx = bxy.x; f.by = bxy.y; f.bz = Bz * inv;
         } else {
             f.absB = R(0);
             f.bx = R(0); f.by = R(0); f.bz = R(1);
         }
-        f.gx = h * f.bx;
-        f.gy = h * f.by;
+        const V2<R> gxy = mul2(v2s(h), v2(f.bx, f.by));
+        f.gx = gxy.x;
+        f.gy = gxy.y;
         f.gz = -(P.Bp * f.bz);
         return;
     }
@@ -474,8 +517,9 @@ DSMC_HD void trap_field(const CloudPhys<R>& P, R x, R y, R z, Field<R>& f) {
 // ---------------------------------------------------------------------------------------
 template <class R>
 DSMC_HD int32_t cell_of(const CloudPhys<R>& P, R x, R y, R z, bool periodic) {
-    R fx = (x - P.gmin_x) * P.inv_dx;
-    R fy = (y - P.gmin_y) * P.inv_dy;
+    const V2<R> fxy = mul2(sub2(v2(x, y), v2(P.gmin_x, P.gmin_y)), v2(P.inv_dx, P.inv_dy));
+    R fx = fxy.x;
+    R fy = fxy.y;
     R fz = (z - P.gmin_z) * P.inv_dz;
     if (periodic) {
         int ix = (fx >= R(0)) ? (int)fx : 0;
@@ -487,8 +531,7 @@ DSMC_HD int32_t cell_of(const CloudPhys<R>& P, R x, R y, R z, bool periodic) {
         iz = iz < P.nz ? iz : P.nz - 1;
         return P.cell_base + (iz * P.ny + iy) * P.nx + ix;
     }
-    if (!(fx >= R(0) && fx < (R)P.nx && fy >= R(0) && fy < (R)P.ny && fz >= R(0) &&
-          fz < (R)P.nz))
+    if (!(fx >= R(0) && fx < P.fnx && fy >= R(0) && fy < P.fny && fz >= R(0) && fz < P.fnz))
         return P.ovf_cell;
     int ix = (int)fx, iy = (int)fy, iz = (int)fz;
     return P.cell_base + (iz * P.ny + iy) * P.nx + ix;
@@ -523,32 +566,38 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
     trap_field(P, a.x, a.y, a.z, f0);
 
     if ((P.flags & F_LARMOR) && !box) {
-        // psi <- [cos t - i sin t (s.B^)] psi, t = mu |B| dt / hbar   (wavefunction.cu:39-73)
+        // psi <- [cos t - i sin t (s.B^)] psi, t = mu |B| dt / hbar   (wavefunction.cu:39-73):
+        //   ur' = ur c + ( bx di - by dr + bz ui) s     ui' = ui c + (-bx dr - by di - bz ur) s
+        //   dr' = dr c + ( bx ui + by ur - bz di) s     di' = di c + (-bx ur + by ui + bz dr) s
+        // with the (up, down) rows as two-lane pairs
         R th = P.theta_per_B * f0.absB;
         R s, c;
         xsincos(th, &s, &c);
-        R nur = a.ur * c + (f0.bx * a.di - f0.by * a.dr + f0.bz * a.ui) * s;
-        R nui = a.ui * c + (-(f0.bx * a.dr) - f0.by * a.di - f0.bz * a.ur) * s;
-        R ndr = a.dr * c + (f0.bx * a.ui + f0.by * a.ur - f0.bz * a.di) * s;
-        R ndi = a.di * c + (-(f0.bx * a.ur) + f0.by * a.ui + f0.bz * a.dr) * s;
-        a.ur = nur; a.ui = nui; a.dr = ndr; a.di = ndi;
+        const V2<R> u = v2(a.ur, a.ui), d = v2(a.dr, a.di);
+        const V2<R> tu = fma2(v2(f0.bz, -f0.bz), v2(a.ui, a.ur),
+                              fma2(v2s(-f0.by), d, mul2(v2(f0.bx, -f0.bx), v2(a.di, a.dr))));
+        const V2<R> td = fma2(v2(-f0.bz, f0.bz), v2(a.di, a.dr),
+                              fma2(v2s(f0.by), v2(a.ur, a.ui), mul2(v2(f0.bx, -f0.bx), v2(a.ui, a.ur))));
+        V2<R> nu = fma2(tu, v2s(s), mul2(u, v2s(c)));
+        V2<R> nd = fma2(td, v2s(s), mul2(d, v2s(c)));
         if (P.flags & F_NORMALISE) {
-            R n2 = a.ur * a.ur + a.ui * a.ui + a.dr * a.dr + a.di * a.di;
-            R inv = xrsqrt(n2);
-            a.ur = a.ur * inv; a.ui = a.ui * inv; a.dr = a.dr * inv; a.di = a.di * inv;
+            const V2<R> q = fma2(nd, nd, mul2(nu, nu));
+            const R inv = xrsqrt(q.x + q.y);
+            nu = mul2(nu, v2s(inv));
+            nd = mul2(nd, v2s(inv));
         }
+        a.ur = nu.x; a.ui = nu.y; a.dr = nd.x; a.di = nd.y;
     }
 
     // velocity Verlet (moveAtoms.cu:51-65); anti-trapped atoms feel +grad|B|
     const R sgn = (a.flags & 1u) ? R(1) : R(-1);
-    const R as = sgn * P.accel_scale;
-    const R hdt = P.half_dt;
-    a.vx = a.vx + hdt * (as * f0.gx);
-    a.vy = a.vy + hdt * (as * f0.gy);
-    a.vz = a.vz + hdt * (as * f0.gz);
-    a.x = a.x + P.dt * a.vx;
-    a.y = a.y + P.dt * a.vy;
-    a.z = a.z + P.dt * a.vz;
+    const R kick = P.half_dt * (sgn * P.accel_scale);
+    V2<R> vxy = fma2(v2s(kick), v2(f0.gx, f0.gy), v2(a.vx, a.vy));
+    a.vz = xfma(kick, f0.gz, a.vz);
+    const V2<R> xy = fma2(v2s(P.dt), vxy, v2(a.x, a.y));
+    a.x = xy.x;
+    a.y = xy.y;
+    a.z = xfma(P.dt, a.vz, a.z);
     if (box) {
         a.x = a.x - P.box_x * xfloor((a.x - P.gmin_x) * P.inv_box_x);
         a.y = a.y - P.box_y * xfloor((a.y - P.gmin_y) * P.inv_box_y);
@@ -556,23 +605,24 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
     }
     Field<R> f1;
     trap_field(P, a.x, a.y, a.z, f1);
-    a.vx = a.vx + hdt * (as * f1.gx);
-    a.vy = a.vy + hdt * (as * f1.gy);
-    a.vz = a.vz + hdt * (as * f1.gz);
+    vxy = fma2(v2s(kick), v2(f1.gx, f1.gy), vxy);
+    a.vx = vxy.x;
+    a.vy = vxy.y;
+    a.vz = xfma(kick, f1.gz, a.vz);
 
-    o.v2 = a.vx * a.vx + a.vy * a.vy + a.vz * a.vz;
+    o.v2 = xfma(a.vz, a.vz, xfma(a.vy, a.vy, a.vx * a.vx));
     o.absB = f1.absB;
     o.fate = FATE_ALIVE;
     if ((P.flags & F_MAJORANA) && !box) {
         // <s.B^> = 2 Bx Re(u* d) + 2 By Im(u* d) + Bz (|u|^2 - |d|^2)   (evaporation.cu:88-90)
-        R re = a.ur * a.dr + a.ui * a.di;
-        R im = a.ur * a.di - a.ui * a.dr;
-        R sz = (a.ur * a.ur + a.ui * a.ui) - (a.dr * a.dr + a.di * a.di);
-        R proj = R(2) * (f1.bx * re) + R(2) * (f1.by * im) + f1.bz * sz;
+        const V2<R> ri = fma2(v2(a.ui, -a.ui), v2(a.di, a.dr), mul2(v2s(a.ur), v2(a.dr, a.di)));  // Re, Im
+        const V2<R> nn = fma2(v2(a.ui, a.di), v2(a.ui, a.di), mul2(v2(a.ur, a.dr), v2(a.ur, a.dr)));
+        const R sz = nn.x - nn.y;
+        const R proj = xfma(f1.bz, sz, R(2) * xfma(f1.bx, ri.x, f1.by * ri.y));
         if (proj < R(0)) o.fate = FATE_MAJORANA;
     }
     if ((P.flags & F_KNIFE) && o.fate == FATE_ALIVE) {
-        R e = o.v2 + P.kappa * (f1.absB - P.B_floor);
+        R e = xfma(P.kappa, f1.absB - P.B_floor, o.v2);
         if (e > cut_v2) o.fate = FATE_KNIFE;
     }
     o.cell = cell_of(P, a.x, a.y, a.z, box);

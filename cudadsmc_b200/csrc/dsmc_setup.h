@@ -64,6 +64,7 @@ inline void make_cloud_phys(const dsmc_params& run, const dsmc_cloud_params& c, 
     const double dx = Lx / c.cells[0], dy = Ly / c.cells[1], dz = Lz / c.cells[2];
     P.gmin_x = (R)c.grid_min[0]; P.gmin_y = (R)c.grid_min[1]; P.gmin_z = (R)c.grid_min[2];
     P.inv_dx = (R)(1.0 / dx); P.inv_dy = (R)(1.0 / dy); P.inv_dz = (R)(1.0 / dz);
+    P.fnx = (R)P.nx; P.fny = (R)P.ny; P.fnz = (R)P.nz;
     P.box_x = (R)Lx; P.box_y = (R)Ly; P.box_z = (R)Lz;
     P.inv_box_x = (R)(1.0 / Lx); P.inv_box_y = (R)(1.0 / Ly); P.inv_box_z = (R)(1.0 / Lz);
     P.Bp = (R)c.dBdz; P.Bpp = (R)c.d2Bdz2; P.B0 = (R)c.B0;
