@@ -108,7 +108,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     std::vector<int> cloud_cell_base;
     // device memory
     DevBuf<R4> pos[2], vel[2], psi[2];
-    DevBuf<int> start[2], tile_begin[2], tile_cloud[2];
+    DevBuf<int> start[2], tile_begin[2], tile_cloud[2], tile_split[2];
     DevBuf<int> src[2];
     DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry, ovf_list;
     DevBuf<int4> mrec;
@@ -218,9 +218,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             start[i].alloc(total_cells + 1);
             tile_begin[i].alloc(max_tiles + 1);
             tile_cloud[i].alloc(max_tiles);
+            tile_split[i].alloc(max_tiles);
             CU(cudaMemset(start[i].p, 0, (total_cells + 1) * sizeof(int)));
             CU(cudaMemset(tile_begin[i].p, 0, (max_tiles + 1) * sizeof(int)));
             CU(cudaMemset(tile_cloud[i].p, 0, max_tiles * sizeof(int)));
+            CU(cudaMemset(tile_split[i].p, 0, max_tiles * sizeof(int)));
         }
         Lc.alloc(total_cells); Ic.alloc(total_cells); mover_base.alloc(total_cells);
         CU(cudaMemset(Lc.p, 0, total_cells * sizeof(int)));
@@ -268,8 +270,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.Lc = Lc.p; A.Ic = Ic.p; A.mover_base = mover_base.p;
             A.sigvrmax = sigvrmax.p;
             A.mrec = mrec.p; A.in_list = in_list.p;
-            A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p;
+            A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p; A.tile_split = tile_split[p].p;
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
+            A.tile_split_next = tile_split[q].p;
             A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p; A.ovf_list = ovf_list.p;
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
@@ -295,7 +298,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
                 step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
             break;
         case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
-        case 2: scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
+        case 2: scan_down<R><<<nscan_blocks + (nclouds + SCAN_BLOCK / 32 - 1) / (SCAN_BLOCK / 32), SCAN_BLOCK, 0, stream>>>(A); break;
         case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
         case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }

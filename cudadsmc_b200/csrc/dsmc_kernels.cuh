@@ -122,8 +122,10 @@ template <class R> struct Args {
     int* in_list;
     const int* tile_begin;
     const int* tile_cloud;
+    const int* tile_split;  // 1: the tile begins inside a cell (the overflow cell) that began earlier
     int* tile_begin_next;
     int* tile_cloud_next;
+    int* tile_split_next;
     int* tile_ovf;
     int* tile_ovf_carry;
     int* ovf_list;  // tiles holding stayers of an overflow cell, in any order (ctl->novf[parity])
@@ -412,7 +414,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     __shared__ StepAcc red[BLOCK / 32];
     __shared__ R s_cut;
     __shared__ int s_nhead;
-    __shared__ int s_split;  // the tile's first cell began in an earlier tile
     // the last run of cells in each 32-position chunk: its cell, its stayers, whether it spans the chunk
     constexpr int NCH = CAP / 32;
     __shared__ int s_tcell[NCH];
@@ -498,11 +499,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             const R4 q = s_pos[t];
             const int c = cell_of(P, q.x, q.y, q.z, box);
             s_cell[t] = c;
-            if (t == 0) s_split = A.old_start[c] < tb ? 1 : 0;
         }
         __syncthreads();
         const int c_first = L > 0 ? s_cell[0] : -1;
-        const bool split = L > 0 && s_split != 0;
+        const bool split = L > 0 && A.tile_split[b] != 0;
 
         StepAcc acc;
         zero_acc(acc);
@@ -529,13 +529,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             for (int h = threadIdx.x; h < nhead; h += BLOCK) {
                 const int t = s_head[h];
                 const int c = s_cell[t];
-                const int n = A.old_start[c + 1] - A.old_start[c];
-                if (A.old_start[c] != tb + t || n > L - t) {  // cell not wholly inside this tile
+                // three independent loads in one round trip (c is a grid cell of this cloud)
+                const int c_beg = A.old_start[c], c_end = A.old_start[c + 1];
+                R svm = A.sigvrmax[c];
+                const int n = c_end - c_beg;
+                if (c_beg != tb + t || n > L - t) {  // cell not wholly inside this tile
                     atomicOr(&A.ctl->err, EB_INCONSISTENT);
                     continue;
                 }
                 if (n < 2) continue;
-                R svm = A.sigvrmax[c];
                 CollideResult<R> cr;
                 if (A.clog_ij) {
                     TileCollisionLog<R> lg{s_pos + t, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap, &A.ctl->err};
@@ -704,25 +706,58 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
     const int p = A.parity;
     const int n = A.ctl->n[p];
     const int ntiles = A.ctl->ntiles[p];
-    for (int j = blockIdx.x * 256 + threadIdx.x; j < n; j += gridDim.x * 256) {
-        const int2 key = A.keys[j];
-        const int kind = key.y & 3;
-        if (kind == KIND_MOVE || kind == KIND_LOST) continue;
-        const int rank = key.y >> 2;
-        int c = key.x, base = 0;
-        if (kind == KIND_OVF) {
-            const int b = key.x;
-            if (b < 0 || b >= ntiles) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
-            const int cloud = A.tile_cloud[b];
-            c = A.clouds[cloud].ovf_cell;
-            const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
-            base = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
+    // four consecutive positions per thread and pass: two 16-byte key loads, then the cell
+    // starts of all four, then the stores (the loads of one pass are independent)
+    constexpr int G = 4;
+    for (int j0 = (blockIdx.x * 256 + threadIdx.x) * G; j0 < n; j0 += gridDim.x * 256 * G) {
+        int2 key[G];
+        if (j0 + G <= n) {
+            const int4 a = reinterpret_cast<const int4*>(A.keys + j0)[0];
+            const int4 b = reinterpret_cast<const int4*>(A.keys + j0)[1];
+            key[0] = make_int2(a.x, a.y); key[1] = make_int2(a.z, a.w);
+            key[2] = make_int2(b.x, b.y); key[3] = make_int2(b.z, b.w);
+        } else {
+#pragma unroll
+            for (int i = 0; i < G; ++i) key[i] = j0 + i < n ? A.keys[j0 + i] : make_int2(-1, KIND_LOST);
         }
-        if (c < 0 || c >= A.total_cells) { atomicOr(&A.ctl->err, EB_INCONSISTENT); continue; }
-        const int lo = A.new_start[c];
-        const int dest = lo + base + rank;
-        if (dest >= lo && dest < A.new_start[c + 1]) A.src_out[dest] = j;
-        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        int c[G], base[G];
+        bool ok[G];
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const int kind = key[i].y & 3;
+            ok[i] = kind == KIND_STAY || kind == KIND_OVF;
+            c[i] = key[i].x;
+            base[i] = 0;
+            if (kind == KIND_OVF) {
+                const int b = key[i].x;
+                if (b < 0 || b >= ntiles) {
+                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                    ok[i] = false;
+                    continue;
+                }
+                const int cloud = A.tile_cloud[b];
+                c[i] = A.clouds[cloud].ovf_cell;
+                const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
+                base[i] = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
+            }
+            if (ok[i] && (c[i] < 0 || c[i] >= A.total_cells)) {
+                atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                ok[i] = false;
+            }
+        }
+        int lo[G], hi[G];
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            lo[i] = ok[i] ? A.new_start[c[i]] : 0;
+            hi[i] = ok[i] ? A.new_start[c[i] + 1] : 0;
+        }
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            if (!ok[i]) continue;
+            const int dest = lo[i] + base[i] + (key[i].y >> 2);
+            if (dest >= lo[i] && dest < hi[i]) A.src_out[dest] = j0 + i;
+            else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        }
     }
     // incoming movers: each writes its old position into its cell's incoming slots (ticket order)
     const int m = A.ctl->movers[p];
@@ -979,14 +1014,18 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
 }
 
 // New cell starts, the movers' base slots and the coming step's tiles (start and cloud); cleared
-// leaver / incoming counters.  In a physics step, block k < nclouds also closes cloud k's step
-// totals (every cloud has at least one scan block).
+// leaver / incoming counters.  The launch carries one extra block per SCAN_BLOCK / 32 clouds, whose
+// warps close the clouds' step totals (in a physics step) beside the scan blocks.
 template <class R>
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
     __shared__ uint32_t wsum[32];
     const int q = 1 - A.parity;
     const int blk = blockIdx.x;
-    if (!A.init_mode && blk < A.nclouds && threadIdx.x < 32) finalize_cloud<R, false>(A, blk, threadIdx.x);
+    if (blk >= A.nscan_blocks) {
+        const int k = (blk - A.nscan_blocks) * (SCAN_BLOCK / 32) + (threadIdx.x >> 5);
+        if (!A.init_mode && k < A.nclouds) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
+        return;
+    }
     const int cloud = A.scan_blk_cloud[blk];
     const int c0 = A.scan_blk_cell0[blk];
     const int cend = cloud_cell_end(A, cloud);
@@ -1031,6 +1070,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
                 if (ti < A.max_tiles) {
                     A.tile_begin_next[ti] = tbeg;
                     A.tile_cloud_next[ti] = cloud;
+                    A.tile_split_next[ti] = (tbeg != st && tbeg != e) ? 1 : 0;
                 }
             }
             ex += (uint32_t)cnt[k];
