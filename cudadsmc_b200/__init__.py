@@ -9,12 +9,12 @@
 """
 from ._abi import (CloudParams, Diag, RunParams, StateBuffers, FP32, FP64, TRAP_QUADRUPOLE,
                    TRAP_IOFFE_PRITCHARD, TRAP_BOX, F_COLLIDE, F_LARMOR, F_MAJORANA, F_KNIFE,
-                   F_NORMALISE, F_KNIFE_FIXED_T, INIT_THERMAL, INIT_UNIFORM)
+                   F_NORMALISE, F_KNIFE_FIXED_T, F_MCWF, INIT_THERMAL, INIT_UNIFORM)
 from .engine import DSMCError, Simulation, load_library, preset, EXPORTED_SYMBOLS
 
 __all__ = [
     "CloudParams", "Diag", "RunParams", "StateBuffers", "Simulation", "DSMCError", "load_library",
     "preset", "EXPORTED_SYMBOLS", "FP32", "FP64", "TRAP_QUADRUPOLE", "TRAP_IOFFE_PRITCHARD",
-    "TRAP_BOX", "F_COLLIDE", "F_LARMOR", "F_MAJORANA", "F_KNIFE", "F_NORMALISE", "F_KNIFE_FIXED_T",
+    "TRAP_BOX", "F_COLLIDE", "F_LARMOR", "F_MAJORANA", "F_KNIFE", "F_NORMALISE", "F_KNIFE_FIXED_T", "F_MCWF",
     "INIT_THERMAL", "INIT_UNIFORM",
 ]

@@ -428,6 +428,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     const int step = A.ctl->step[p];
     const int lane = threadIdx.x & 31;
     const bool collide_now = (step % A.collide_every) == 0;
+    // MCWF phase of this step: bit 0 at the start of a collision period, bit 1 at its end
+    const uint32_t mcwf_phase = (collide_now ? 1u : 0u) | (((step + 1) % A.collide_every) == 0 ? 2u : 0u);
     int cur_cloud = -1;
     if (threadIdx.x == 0) {
         LostAcc z = {};
@@ -573,7 +575,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 a.vx = v.x; a.vy = v.y; a.vz = v.z;
                 a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
                 a.flags = lane_to_u32(v.w);
-                advance_atom(P, cut, a, o);
+                StepCtx sc;
+                sc.id = lane_to_u32(q.w);
+                sc.step = (uint32_t)step;
+                sc.cloud = (uint32_t)P.cloud_id;
+                sc.mcwf = mcwf_phase;
+                sc.seed = A.seed;
+                advance_atom(P, cut, a, o, sc);
                 c_old = s_cell[t];
                 const bool alive = (o.fate == FATE_ALIVE);
                 stayer = alive && (o.cell == c_old);
@@ -644,7 +652,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 if (stayer || mover) {
                     R4 qo, vo, so;
                     qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
-                    vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = v.w;
+                    vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = lane_from_u32(a.flags, R(0));
                     so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
                     A.pos_out[j] = qo;
                     A.vel_out[j] = vo;
@@ -1120,7 +1128,7 @@ __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
         const R v2 = v.x * v.x + v.y * v.y + v.z * v.z;
         acc.n_alive += 1;
         acc.sum_v2 += fx_from(v2);
-        acc.sum_B += fx_from(f.absB);
+        acc.sum_B += fx_from((lane_to_u32(v.w) & 1u) ? -f.absB : f.absB);  // anti-trapped: -|B|
     }
     block_reduce_partial<BLOCK>(acc, red);
     if (threadIdx.x == 0) accum_tile(A.accum + A.tile_cloud[b] * ACC_BUCKETS + (b & (ACC_BUCKETS - 1)), acc);

@@ -359,27 +359,22 @@ DSMC_HD double xexp(double x) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Exact fixed-point accumulation for diagnostics: a non-negative value d, clamped to 2^38
-// (no physical v^2 or |B| comes near; NaN clamps too), maps to floor(d * 2^64) as a 128-bit
+// Exact fixed-point accumulation for diagnostics: a value d, its magnitude clamped to 2^38 (no
+// physical v^2 or |B| comes near; NaN clamps too), maps to sign(d) floor(|d| 2^64) as a 128-bit
 // integer.  Sums of these are exact and therefore independent of summation order (GPU tiles,
-// CPU loop, batched or single clouds).  The integer part and the fraction scaled by 2^64 are
-// both exact in the value's own precision, so the float and double forms agree bit for bit
+// CPU loop, batched or single clouds).  The integer part of |d| and its fraction scaled by 2^64
+// are both exact in the value's own precision, so the float and double forms agree bit for bit
 // on every float input.
 // ---------------------------------------------------------------------------------------
-DSMC_HD i128 fx_from(double d) {
-    if (!(d < 0x1p38)) d = 0x1p38;
-    const double h = xfloor(d);
+template <class R> DSMC_HD i128 fx_from_magnitude(R m) {
+    if (!(m < R(0x1p38))) m = R(0x1p38);
+    const R h = xfloor(m);
     const int64_t hi = (int64_t)h;
-    const uint64_t lo = (uint64_t)((d - h) * 0x1p64);
+    const uint64_t lo = (uint64_t)((m - h) * R(0x1p64));
     return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
 }
-DSMC_HD i128 fx_from(float f) {
-    if (!(f < 0x1p38f)) f = 0x1p38f;
-    const float h = xfloor(f);
-    const int64_t hi = (int64_t)h;
-    const uint64_t lo = (uint64_t)((f - h) * 0x1p64f);
-    return (i128)(((unsigned __int128)(uint64_t)hi << 64) | (unsigned __int128)lo);
-}
+DSMC_HD i128 fx_from(double d) { return d < 0.0 ? -fx_from_magnitude(-d) : fx_from_magnitude(d); }
+DSMC_HD i128 fx_from(float f) { return f < 0.0f ? -fx_from_magnitude(-f) : fx_from_magnitude(f); }
 DSMC_HD double fx_to_double(i128 q) {
     int64_t hi = (int64_t)(q >> 64);
     uint64_t lo = (uint64_t)q;
@@ -398,7 +393,8 @@ DSMC_HD double knife_temperature(double mass, double kB, double T0, bool fixed_T
 // ---------------------------------------------------------------------------------------
 enum { TRAP_QUADRUPOLE = 0, TRAP_IOFFE_PRITCHARD = 1, TRAP_BOX = 2 };
 enum {
-    F_COLLIDE = 1, F_LARMOR = 2, F_MAJORANA = 4, F_KNIFE = 8, F_NORMALISE = 16, F_KNIFE_FIXED_T = 32
+    F_COLLIDE = 1, F_LARMOR = 2, F_MAJORANA = 4, F_KNIFE = 8, F_NORMALISE = 16, F_KNIFE_FIXED_T = 32,
+    F_MCWF = 64
 };
 
 template <class R> struct CloudPhys {
@@ -422,6 +418,9 @@ template <class R> struct CloudPhys {
     R v_init;                     // sqrt(kB T0 / m)
     R r0_init;                    // kB T0 / mu  (quadrupole thermal length)
     R inv_kT_over_mu;             // mu / (kB T0) for rejection sampling
+    R mcwf_cp;                    // 1.163 sqrt(sigma): tau_pos = mcwf_cp / sqrt(2 |a|)
+    R mcwf_cv;                    // sqrt(2/pi) hbar / (m sigma): tau_vel = mcwf_cv / (2 |a|)
+    R dt_period;                  // collide_every * dt: the MCWF period
     R prop_min_x, prop_min_y, prop_min_z;  // proposal box of the rejection sampler
     R prop_len_x, prop_len_y, prop_len_z;
     int32_t knife_nknots;
@@ -547,7 +546,17 @@ DSMC_HD int32_t cell_of(const CloudPhys<R>& P, R x, R y, R z, bool periodic) {
 template <class R> struct Atom {
     R x, y, z, vx, vy, vz;
     R ur, ui, dr, di;  // psi_up, psi_dn
-    uint32_t flags;    // bit 0: anti-trapped
+    uint32_t flags;    // bit 0: anti-trapped; bits 2..31: MCWF period-start population (mcwf_store)
+};
+
+// Per-atom context of a step: the atom id, the step number and seed for the spin-flip random
+// number, and the MCWF phase (bit 0: record the trapped population, bit 1: flip and decay)
+struct StepCtx {
+    uint32_t id;
+    uint32_t step;
+    uint32_t cloud;
+    uint32_t mcwf;
+    uint64_t seed;
 };
 
 enum { FATE_ALIVE = 0, FATE_MAJORANA = 1, FATE_KNIFE = 2 };
@@ -556,14 +565,82 @@ template <class R> struct AtomOut {
     int32_t cell;
     int32_t fate;
     R v2;     // |v|^2 after the step
-    R absB;   // |B| after the step
+    R absB;   // s |B| after the step: s = +1 trapped, -1 anti-trapped (potential energy / mu)
 };
 
+// ---------------------------------------------------------------------------------------
+// MCWF spin flips and decoherence (wavefunction.cu:75-237; scheduled by main.cu:457-520: the
+// populations are taken after the collisions, the flip and the decay follow the last motion
+// step of the collision period).
+// ---------------------------------------------------------------------------------------
+// trapped-state population (1 + <s.B^>)/2 in the reference's form for a normalised spinor:
+// 1/2 + Bx Re(u* d) + By Im(u* d) - Bz (1/2 - |u|^2)   (projectLocalPopulations, :162-170)
+template <class R> DSMC_HD R trapped_population(const Field<R>& f, const Atom<R>& a) {
+    const R re = a.ur * a.dr + a.ui * a.di;
+    const R im = a.ur * a.di - a.ui * a.dr;
+    const R u2 = a.ur * a.ur + a.ui * a.ui;
+    return R(0.5) + f.bx * re + f.by * im - f.bz * (R(0.5) - u2);
+}
+// the period-start population kept in flag bits 2..31 as floor(x 2^30), x clamped to [0, 1)
+template <class R> DSMC_HD uint32_t mcwf_store(uint32_t flags, R x) {
+    const R xc = x >= R(0) ? (x < R(1) ? x : R(1) - R(1) / R(1 << 24)) : R(0);  // NaN -> 0
+    uint32_t q = (uint32_t)(xc * R(1 << 30));
+    q = q < (1u << 30) ? q : (1u << 30) - 1u;
+    return (flags & 3u) | (q << 2);
+}
+template <class R> DSMC_HD R mcwf_load(uint32_t flags) { return (R)(flags >> 2) * (R(1) / R(1 << 30)); }
+
+// End of a collision period: the jump to the other state with probability (y1 - y0)/x0 for a
+// trapped atom, (x1 - x0)/y0 for an anti-trapped one (y = 1 - x), taken when the kinetic
+// energy stays positive after the change 2 mu |B| of potential energy, the speed rescaled to
+// conserve energy (flipAtoms, :99-156); then decoherence towards the eigenstates of s.B^ over
+// the period, psi <- [(1 - e) (s.B^) psi + (1 + e) psi] / 2 with e = exp(-dt_c / tau), tau from the
+// local acceleration (exponentialDecay + calculateTau, :175-223), and renormalisation.
 template <class R>
-DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R>& o) {
+DSMC_HD void mcwf_end(const CloudPhys<R>& P, const Field<R>& f, Atom<R>& a, const StepCtx& sc) {
+    const R x0 = mcwf_load<R>(a.flags);
+    const R x1 = trapped_population(f, a);
+    const bool trapped = !(a.flags & 1u);
+    const R pflip = trapped ? ((R(1) - x1) - (R(1) - x0)) / x0 : (x1 - x0) / (R(1) - x0);
+    const R dv2 = trapped ? R(2) * P.kappa * f.absB : -(R(2) * P.kappa * f.absB);  // dE / (m/2)
+    const R vv = xfma(a.vz, a.vz, xfma(a.vy, a.vy, a.vx * a.vx));
+    const u32x4 w = draw(sc.id, sc.step, PURPOSE_FLIP, sc.cloud, 0u, sc.seed);
+    const R u = u01<R>(w.x, w.y);
+    if (pflip > u && vv + dv2 > R(0) && vv > R(0)) {
+        a.flags ^= 1u;
+        const R s = xsqrt(vv + dv2) / xsqrt(vv);
+        const V2<R> vxy = mul2(v2(a.vx, a.vy), v2s(s));
+        a.vx = vxy.x;
+        a.vy = vxy.y;
+        a.vz = a.vz * s;
+    }
+    // decoherence: 1/tau = (tau_pos^-3 + tau_vel^-3)^(1/3), relative acceleration 2 |a|
+    const R g = xsqrt(xfma(f.gz, f.gz, xfma(f.gy, f.gy, f.gx * f.gx)));
+    const R rel = R(2) * P.accel_scale * g;
+    R e = R(1);
+    if (rel > R(0)) {
+        const R ip = xsqrt(rel) / P.mcwf_cp;  // 1 / tau_pos
+        const R iv = rel / P.mcwf_cv;         // 1 / tau_vel
+        const R s3 = ip * ip * ip + iv * iv * iv;
+        const R rate = xexp(xlog(s3) * (R(1) / R(3)));
+        e = xexp(-(P.dt_period * rate));
+    }
+    const R om = R(1) - e, op = R(1) + e;
+    const R ur = R(0.5) * ((f.bx * a.dr + f.by * a.di + f.bz * a.ur) * om + a.ur * op);
+    const R ui = R(0.5) * ((f.bx * a.di - f.by * a.dr + f.bz * a.ui) * om + a.ui * op);
+    const R dr = R(0.5) * ((f.bx * a.ur - f.by * a.ui - f.bz * a.dr) * om + a.dr * op);
+    const R di = R(0.5) * ((f.bx * a.ui + f.by * a.ur - f.bz * a.di) * om + a.di * op);
+    const R n2 = ur * ur + ui * ui + dr * dr + di * di;
+    const R inv = xrsqrt(n2);
+    a.ur = ur * inv; a.ui = ui * inv; a.dr = dr * inv; a.di = di * inv;
+}
+
+template <class R>
+DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R>& o, const StepCtx& sc) {
     const bool box = (P.trap == TRAP_BOX);
     Field<R> f0;
     trap_field(P, a.x, a.y, a.z, f0);
+    if ((P.flags & F_MCWF) && !box && (sc.mcwf & 1u)) a.flags = mcwf_store(a.flags, trapped_population(f0, a));
 
     if ((P.flags & F_LARMOR) && !box) {
         // psi <- [cos t - i sin t (s.B^)] psi, t = mu |B| dt / hbar   (wavefunction.cu:39-73):
@@ -625,6 +702,11 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
         R e = xfma(P.kappa, f1.absB - P.B_floor, o.v2);
         if (e > cut_v2) o.fate = FATE_KNIFE;
     }
+    if ((P.flags & F_MCWF) && !box && (sc.mcwf & 2u) && o.fate == FATE_ALIVE) {
+        mcwf_end(P, f1, a, sc);
+        o.v2 = xfma(a.vz, a.vz, xfma(a.vy, a.vy, a.vx * a.vx));
+    }
+    if (a.flags & 1u) o.absB = -o.absB;
     o.cell = cell_of(P, a.x, a.y, a.z, box);
 }
 

@@ -74,6 +74,9 @@ inline void make_cloud_phys(const dsmc_params& run, const dsmc_cloud_params& c, 
     P.theta_per_B = (R)(c.moment * run.dt / hbar);
     P.kappa = (R)(2.0 * c.moment / c.mass);
     P.sigma = (R)c.sigma;
+    P.mcwf_cp = (R)(1.163 * std::sqrt(c.sigma));
+    P.mcwf_cv = (R)(std::sqrt(2.0 / 3.14159265358979323846) * hbar / (c.mass * c.sigma));
+    P.dt_period = (R)(run.collide_every * run.dt);
     P.cand_pref = (R)(c.alpha * run.dt * run.collide_every / (dx * dy * dz));
     P.v_init = (R)std::sqrt(kB * c.temperature / c.mass);
     P.r0_init = (R)((c.moment > 0 && c.dBdz != 0) ? kB * c.temperature / (c.moment * std::fabs(c.dBdz)) : 0.0);

@@ -71,7 +71,9 @@ enum {
     DSMC_F_MAJORANA = 1 << 2,     /* remove atoms with <sigma.B^> < 0 (evaporation.cu:90-95) */
     DSMC_F_KNIFE = 1 << 3,        /* remove atoms with E > eta(step) kB T */
     DSMC_F_NORMALISE = 1 << 4,    /* renormalise the spinor after every rotation */
-    DSMC_F_KNIFE_FIXED_T = 1 << 5 /* knife uses the initial T instead of the running T */
+    DSMC_F_KNIFE_FIXED_T = 1 << 5, /* knife uses the initial T instead of the running T */
+    DSMC_F_MCWF = 1 << 6           /* spin flips and decoherence once per collision period
+                                      (flipAtoms + exponentialDecay + normalise, wavefunction.cu:99-237) */
 };
 
 /* Initial distributions. */
@@ -127,7 +129,7 @@ typedef struct dsmc_diag {
     double e_pot;          /* total potential energy mu |B| (J) */
     double temperature;    /* m <v^2> / (3 kB) (K) */
     double sum_v2;         /* sum of v^2 (m^2/s^2), exact fixed-point sum */
-    double sum_absB;       /* sum of |B| (T), exact fixed-point sum */
+    double sum_absB;       /* sum of s |B| (T), s = +1 trapped, -1 anti-trapped: E_pot / mu; exact fixed-point sum */
     int64_t n_evaporated;  /* cumulative atoms removed (Majorana + knife) */
     int64_t n_majorana;    /* cumulative Majorana losses */
     int64_t n_knife;       /* cumulative knife losses */

@@ -53,6 +53,9 @@ def load() -> C.CDLL:
                                                 C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, i32,
                                                 C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                                 C.POINTER(C.c_double), i32]),
+            "oracle_mcwf_end_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), i32, i64]),
             "oracle_advance_atoms_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                              i64, i32]),
@@ -113,6 +116,20 @@ def field(run: RunParams, cloud: CloudParams, xyz: np.ndarray) -> np.ndarray:
     load().oracle_field_d(C.byref(run), C.byref(cloud), xyz.ctypes.data_as(C.POINTER(C.c_double)),
                           out.ctypes.data_as(C.POINTER(C.c_double)), xyz.shape[0])
     return out
+
+
+def mcwf_end(run: RunParams, cloud: CloudParams, pos, vel, psi, x0, flags, ids, step: int):
+    """The MCWF period end (spin flip, decoherence, renormalisation) of each atom, FP64: pos/vel
+    (n, 3), psi (n, 4), x0 the trapped population at the period start, flags bit 0 anti-trapped.
+    Returns (vel, psi, flags) after the period end."""
+    pos = np.ascontiguousarray(pos, np.float64); vel = np.array(vel, np.float64, order="C")
+    psi = np.array(psi, np.float64, order="C"); x0 = np.ascontiguousarray(x0, np.float64)
+    fl = np.array(flags, np.uint32, order="C"); ids = np.ascontiguousarray(ids, np.uint32)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    up = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+    load().oracle_mcwf_end_d(C.byref(run), C.byref(cloud), dp(pos), dp(vel), dp(psi), dp(x0), up(fl), up(ids),
+                             int(step), pos.shape[0])
+    return vel, psi, fl
 
 
 def advance_atoms(run: RunParams, cloud: CloudParams, pos, vel, psi, nsteps: int):

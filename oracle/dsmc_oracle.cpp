@@ -139,7 +139,8 @@ template <class R> struct Oracle final : OracleBase {
                 trap_field(C, pos[i].x, pos[i].y, pos[i].z, f);
                 const R v2 = vel[i].x * vel[i].x + vel[i].y * vel[i].y + vel[i].z * vel[i].z;
                 a.sum_v2 += fx_from((double)v2);
-                a.sum_B += fx_from((double)f.absB);
+                const R sb = (lane_to_u32(vel[i].w) & 1u) ? -f.absB : f.absB;  // anti-trapped: -|B|
+                a.sum_B += fx_from((double)sb);
             }
             a.n_alive = natoms[k];
             a.T_knife = knife_temperature(C.mass, C.kB, C.T0, (C.flags & F_KNIFE_FIXED_T) != 0, a.sum_v2, a.n_alive);
@@ -233,9 +234,16 @@ template <class R> struct Oracle final : OracleBase {
                 a.ur = psi[i].x; a.ui = psi[i].y; a.dr = psi[i].z; a.di = psi[i].w;
                 a.flags = lane_to_u32(vel[i].w);
                 AtomOut<R> o;
-                advance_atom(C, cut, a, o);
+                StepCtx sc;
+                sc.id = lane_to_u32(pos[i].w);
+                sc.step = (uint32_t)step_no;
+                sc.cloud = (uint32_t)C.cloud_id;
+                sc.mcwf = ((step_no % run.collide_every) == 0 ? 1u : 0u) |
+                          (((step_no + 1) % run.collide_every) == 0 ? 2u : 0u);
+                sc.seed = run.seed;
+                advance_atom(C, cut, a, o, sc);
                 pos[i].x = a.x; pos[i].y = a.y; pos[i].z = a.z;
-                vel[i].x = a.vx; vel[i].y = a.vy; vel[i].z = a.vz;
+                vel[i].x = a.vx; vel[i].y = a.vy; vel[i].z = a.vz; vel[i].w = lane_from_u32(a.flags, R(0));
                 psi[i].x = a.ur; psi[i].y = a.ui; psi[i].z = a.dr; psi[i].w = a.di;
                 newcell[i] = o.cell;
                 fate[i] = o.fate;
@@ -525,11 +533,38 @@ OAPI int oracle_advance_atoms_d(const dsmc_params* run, const dsmc_cloud_params*
         a.flags = lane_to_u32(vel[4 * i + 3]);
         AtomOut<double> o;
         o.fate = FATE_ALIVE;
-        for (int s = 0; s < nsteps; ++s) advance_atom(P, 0.0, a, o);
+        StepCtx sc = {};
+        for (int s = 0; s < nsteps; ++s) advance_atom(P, 0.0, a, o, sc);
         pos[4 * i] = a.x; pos[4 * i + 1] = a.y; pos[4 * i + 2] = a.z;
         vel[4 * i] = a.vx; vel[4 * i + 1] = a.vy; vel[4 * i + 2] = a.vz;
         psi[4 * i] = a.ur; psi[4 * i + 1] = a.ui; psi[4 * i + 2] = a.dr; psi[4 * i + 3] = a.di;
         if (fate) fate[i] = o.fate;
+    }
+    return 0;
+}
+
+// MCWF period end (flip + decoherence + renormalisation) of each atom at its position, in FP64:
+// x0 = the trapped population recorded at the period start; flags bit 0 = anti-trapped on input
+// and output; ids and step key the flip's random number.
+OAPI int oracle_mcwf_end_d(const dsmc_params* run, const dsmc_cloud_params* c, const double* pos, double* vel,
+                           double* psi, const double* x0, uint32_t* flags, const uint32_t* ids, int32_t step,
+                           int64_t n) {
+    CloudPhys<double> P;
+    make_cloud_phys<double>(*run, *c, 0, 0, P);
+    for (int64_t i = 0; i < n; ++i) {
+        Atom<double> a;
+        a.x = pos[3 * i]; a.y = pos[3 * i + 1]; a.z = pos[3 * i + 2];
+        a.vx = vel[3 * i]; a.vy = vel[3 * i + 1]; a.vz = vel[3 * i + 2];
+        a.ur = psi[4 * i]; a.ui = psi[4 * i + 1]; a.dr = psi[4 * i + 2]; a.di = psi[4 * i + 3];
+        a.flags = mcwf_store(flags[i] & 1u, x0[i]);
+        Field<double> f;
+        trap_field(P, a.x, a.y, a.z, f);
+        StepCtx sc;
+        sc.id = ids[i]; sc.step = (uint32_t)step; sc.cloud = (uint32_t)P.cloud_id; sc.mcwf = 2u; sc.seed = run->seed;
+        mcwf_end(P, f, a, sc);
+        vel[3 * i] = a.vx; vel[3 * i + 1] = a.vy; vel[3 * i + 2] = a.vz;
+        psi[4 * i] = a.ur; psi[4 * i + 1] = a.ui; psi[4 * i + 2] = a.dr; psi[4 * i + 3] = a.di;
+        flags[i] = a.flags & 1u;
     }
     return 0;
 }

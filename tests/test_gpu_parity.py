@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from cudadsmc_b200 import (FP32, FP64, F_COLLIDE, F_KNIFE, F_KNIFE_FIXED_T, F_LARMOR, F_MAJORANA,
+from cudadsmc_b200 import (FP32, FP64, F_COLLIDE, F_KNIFE, F_KNIFE_FIXED_T, F_LARMOR, F_MAJORANA, F_MCWF,
                            F_NORMALISE, TRAP_BOX, TRAP_IOFFE_PRITCHARD, INIT_THERMAL, Simulation, preset)
 from cudadsmc_b200.engine import DSMCError
 
@@ -285,3 +285,37 @@ def test_autotune_changes_speed_not_results():
     sim.step(3)
     orc.step(3)
     assert_same(sim, orc)
+
+
+@pytest.mark.parametrize("precision,period", [(FP32, 1), (FP32, 3), (FP64, 3)])
+def test_mcwf_flips_and_decoherence_bit_exact(precision, period):
+    # MCWF (flip + decoherence + renormalisation once per collision period) with collisions,
+    # starting from half-population spinors, half the atoms anti-trapped: flips happen, and the
+    # GPU state, order and diagnostics equal the oracle's bit for bit
+    run, c = scaled(2, n=30000, cells=24, precision=precision, flags=ALL | F_MCWF, alpha=4000.0)
+    run.collide_every = period
+    src = Simulation(run, c)
+    src.init_cloud(5)
+    st = src.get_state()
+    pos, vel = st["pos"].astype(np.float64), st["vel"].copy()
+    B = np.stack([0.5 * c.dBdz * pos[:, 0], 0.5 * c.dBdz * pos[:, 1], c.B0 - c.dBdz * pos[:, 2]], 1)
+    b = B / np.linalg.norm(B, axis=1)[:, None]
+    nrm = np.sqrt(2.0 * (1.0 + b[:, 2]))
+    up_p, dn_p = (1.0 + b[:, 2]) / nrm, (b[:, 0] + 1j * b[:, 1]) / nrm
+    up_m, dn_m = -(b[:, 0] - 1j * b[:, 1]) / nrm, (1.0 + b[:, 2]) / nrm
+    u, d = np.sqrt(0.5) * (up_p + up_m), np.sqrt(0.5) * (dn_p + dn_m)
+    psi = np.stack([u.real, u.imag, d.real, d.imag], 1).astype(st["psi"].dtype)
+    w = vel[:, 3].view(np.uint32 if vel.dtype == np.float32 else np.uint64)
+    w[::2] |= 1  # anti-trapped
+    sim = Simulation(run, c)
+    orc = oracle.Oracle(run, c)
+    for s in (sim, orc):
+        s.set_state(st["pos"], vel, psi, st["cloud_counts"])
+    assert_same(sim, orc)
+    flags0 = bits(sim.get_state()["vel"])[:, 3] & 1
+    for n in (period, 2 * period + 1, 12):
+        sim.step(n)
+        orc.step(n)
+        assert_same(sim, orc)
+    g = sim.get_state()
+    assert int(np.sum(bits(g["vel"])[:, 3] & 1)) != int(np.sum(flags0))  # spins flipped

@@ -20,7 +20,7 @@ import pytest
 from scipy import stats
 
 import oracle
-from cudadsmc_b200._abi import (FP32, FP64, F_COLLIDE, F_LARMOR, F_MAJORANA, F_KNIFE, F_NORMALISE,
+from cudadsmc_b200._abi import (FP32, FP64, F_COLLIDE, F_LARMOR, F_MAJORANA, F_KNIFE, F_NORMALISE, F_MCWF,
                                 TRAP_BOX, TRAP_IOFFE_PRITCHARD, INIT_UNIFORM)
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -261,3 +261,89 @@ def test_knife_removes_hot_atoms_and_tallies_energy():
     f = oracle.field(run, c, s["pos"][:, :3].astype(np.float64))
     e = 0.5 * c.mass * v2 + c.moment * f[:, 3]
     assert np.all(e <= 4.0 * KB * d0["temperature"] * (1 + 1e-5))
+
+
+# ---------------------------------------------------------------------------------------------
+# MCWF spin flips and decoherence (wavefunction.cu:99-237)
+# ---------------------------------------------------------------------------------------------
+def quad_unit_field(pos, Bp, B0=0.0):
+    B = np.stack([0.5 * Bp * pos[:, 0], 0.5 * Bp * pos[:, 1], B0 - Bp * pos[:, 2]], 1)
+    absB = np.linalg.norm(B, axis=1)
+    return B / absB[:, None], absB
+
+
+def spinor_with_population(b, x):
+    """psi = sqrt(x)|+> + sqrt(1-x)|->, |+-> the eigenvectors of s.b (|+> trapped)."""
+    bx, by, bz = b[:, 0], b[:, 1], b[:, 2]
+    nrm = np.sqrt(2.0 * (1.0 + bz))
+    up_p, dn_p = (1.0 + bz) / nrm, (bx + 1j * by) / nrm            # s.b |+> = +|+>
+    up_m, dn_m = -(bx - 1j * by) / nrm, (1.0 + bz) / nrm           # s.b |-> = -|->
+    u = np.sqrt(x) * up_p + np.sqrt(1.0 - x) * up_m
+    d = np.sqrt(x) * dn_p + np.sqrt(1.0 - x) * dn_m
+    return np.stack([u.real, u.imag, d.real, d.imag], 1)
+
+
+def trapped_pop(b, psi):
+    u = psi[:, 0] + 1j * psi[:, 1]
+    d = psi[:, 2] + 1j * psi[:, 3]
+    sb = 2 * b[:, 0] * (np.conj(u) * d).real + 2 * b[:, 1] * (np.conj(u) * d).imag + b[:, 2] * (abs(u) ** 2 - abs(d) ** 2)
+    return 0.5 * (1 + sb)
+
+
+@pytest.mark.parametrize("anti,x0,x1", [(0, 0.8, 0.6), (1, 0.3, 0.5)])
+def test_mcwf_flip_probability_and_energy(anti, x0, x1):
+    # flipAtoms (wavefunction.cu:99-156): a trapped atom jumps with probability (y1 - y0)/x0, an
+    # anti-trapped one with (x1 - x0)/y0; the speed changes by the potential step 2 mu |B|
+    run, c = small(0, flags=F_LARMOR | F_NORMALISE | F_MCWF)
+    n = 40000
+    rng = np.random.default_rng(11)
+    pos = rng.normal(0, 40e-6, (n, 3))
+    vel = rng.normal(0, 0.1, (n, 3))
+    b, absB = quad_unit_field(pos, c.dBdz)
+    psi = spinor_with_population(b, np.full(n, x1))
+    assert np.allclose(trapped_pop(b, psi), x1, atol=1e-12)
+    flags = np.full(n, anti, np.uint32)
+    v2, psi2, fl = oracle.mcwf_end(run, c, pos, vel, psi, np.full(n, x0), flags, np.arange(n), 7)
+    flipped = fl != flags
+    p = ((1 - x1) - (1 - x0)) / x0 if anti == 0 else (x1 - x0) / (1 - x0)
+    mu = c.moment
+    dE = 2 * mu * absB * (1 if anti == 0 else -1)
+    ok = 0.5 * M_RB * np.sum(vel ** 2, 1) + dE > 0
+    expect = p * ok.mean()
+    assert abs(flipped.mean() - expect) < 5 * math.sqrt(expect * (1 - expect) / n), (flipped.mean(), expect)
+    sgn = np.where(flags == 1, -1.0, 1.0)
+    sgn2 = np.where(fl == 1, -1.0, 1.0)
+    e_before = 0.5 * M_RB * np.sum(vel ** 2, 1) + sgn * mu * absB
+    e_after = 0.5 * M_RB * np.sum(v2 ** 2, 1) + sgn2 * mu * absB
+    np.testing.assert_allclose(e_after, e_before, rtol=1e-12, atol=1e-12 * np.abs(e_before).max())
+    assert np.array_equal(v2[~flipped], vel[~flipped])
+    # exponentialDecay over the period then normalise: the spinor is projected onto the trapped
+    # eigenstate (e = exp(-dt_c / tau) underflows for this trap), unit norm
+    assert np.allclose(np.sum(psi2 ** 2, 1), 1.0, atol=1e-14)
+    assert np.allclose(trapped_pop(b, psi2), 1.0, atol=1e-12)
+
+
+def test_mcwf_step_decoheres_each_period_and_conserves_energy():
+    # the MCWF path inside the oracle's step, collision period of 4 steps: spinors set to half
+    # trapped population relax onto the trapped eigenstate at the period's end (not before), and
+    # the total energy with the signed potential is conserved to Verlet accuracy
+    run, c = small(0, n=4000, flags=F_LARMOR | F_NORMALISE | F_MCWF)
+    run.collide_every = 4
+    o = oracle.Oracle(run, c)
+    o.init_cloud(1234)
+    st = o.get_state()
+    pos = st["pos"]
+    b, _ = quad_unit_field(pos[:, :3], c.dBdz, c.B0)
+    psi = spinor_with_population(b, np.full(pos.shape[0], 0.5))
+    o.set_state(st["pos"], st["vel"], psi, st["cloud_counts"])
+    e0 = total_energy(o.diagnostics())
+    o.step(3)
+    s3 = o.get_state()
+    b3, _ = quad_unit_field(s3["pos"][:, :3], c.dBdz, c.B0)
+    assert np.max(np.abs(trapped_pop(b3, s3["psi"]) - 0.5)) < 0.1  # precession only so far
+    o.step(1)
+    s4 = o.get_state()
+    b4, _ = quad_unit_field(s4["pos"][:, :3], c.dBdz, c.B0)
+    assert np.allclose(trapped_pop(b4, s4["psi"]), 1.0, atol=1e-9)
+    o.step(96)
+    assert abs(total_energy(o.diagnostics()) - e0) / e0 < 1e-5

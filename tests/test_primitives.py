@@ -88,19 +88,23 @@ def test_fixed_point_sums_are_order_independent():
 
 
 def test_fixed_point_float_and_double_forms_agree():
-    # floor(min(x, 2^38) * 2^64) from the float form equals the double form on the same value
+    # sign(x) floor(min(|x|, 2^38) * 2^64) from the float form equals the double form on the same
+    # value, negative values (anti-trapped atoms' -|B|) included
     rng = np.random.default_rng(5)
-    x = np.concatenate([
+    pos = np.concatenate([
         np.exp2(rng.uniform(-80, 40, 20000)),            # subnormal-adjacent to beyond the clamp
         rng.uniform(0, 4, 5000),
         [0.0, 2.0 ** -64, 2.0 ** -65, 1.0, 2.0 ** 38, 2.0 ** 38 * 0.999, np.inf, np.nan, 1e-45, 3e38],
-    ]).astype(np.float32)
+    ])
+    x = np.concatenate([pos, -pos[:25000], [-0.3, -1.7, -1e-3]]).astype(np.float32)
     f = oracle.fixed_point(x)
     d = oracle.fixed_point(x.astype(np.float64))
     assert f == d
     for xi, v in zip(x[:3000].astype(np.float64), f[:3000]):
         assert v == int(math.floor(min(xi, 2.0 ** 38) * 2.0 ** 64))
-    assert f[-3] == f[-4] == 2 ** 102  # inf and NaN clamp to 2^38
+    for xi, v in zip(x[25010:28000].astype(np.float64), f[25010:28000]):
+        assert v == -int(math.floor(min(-xi, 2.0 ** 38) * 2.0 ** 64))
+    assert f[25006] == f[25007] == 2 ** 102  # inf and NaN clamp to 2^38
 
 
 def field_reference(kind, p, B0, Bp, Bpp):
