@@ -124,9 +124,18 @@ def cpu_baseline(run, cloud, steps: int, threads: int | None = None) -> dict:
     t1 = time.perf_counter()
     d1 = o.diagnostics()
     atom_steps = d1["atom_steps"] - d0["atom_steps"]
+    # the same restatement on one host thread, one more step of the same cloud
+    oracle.set_threads(1)
+    t2 = time.perf_counter()
+    o.step(1)
+    t3 = time.perf_counter()
+    one = o.diagnostics()["atom_steps"] - d1["atom_steps"]
+    oracle.set_threads(nthreads)
     return {"value": atom_steps / (t1 - t0), "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{cloud.n_atoms:.0e} atoms, {steps} timed steps after init + 1 warm-up step "
-                      f"({t1 - t0:.1f} s), OpenMP float build of oracle/dsmc_oracle.cpp"}
+                      f"({t1 - t0:.1f} s), OpenMP float build of oracle/dsmc_oracle.cpp",
+            "single_thread": {"value": one / (t3 - t2), "unit": UNIT, "cores": 1,
+                              "sample": f"1 further step of the same cloud on one thread ({t3 - t2:.1f} s)"}}
 
 
 def adjoint_vs_plain(stream, steps: int, checkpoint_every: int) -> dict:
