@@ -7,18 +7,21 @@
 //   sorted order groups atoms by global cell (clouds one after another, each cloud's grid cells
 //   then its overflow cell), so every cell is a contiguous range [start[c], start[c+1]) of j.
 //
-// One step = 8 launches with static grids, captured in a CUDA graph:
+// One step = 5 launches with static grids, captured in a CUDA graph of two steps:
 //   step_pass        per tile of ~T sorted positions: gather the atoms through src, collide the
 //                    tile's cells in shared memory, then move + spin + evaporate every atom once,
 //                    write the new state at its current position j (coalesced) with an 8-byte
-//                    sort key, count leavers L[c] / incoming movers I[c], list movers, and reduce
-//                    exact diagnostics.  The only heavy pass: the step is computed once.
-//   scan_reduce/top/down   per-cell counts n_c - L_c + I_c -> new start[], next tiling, movers'
-//                    base slot, overflow prefix over tiles
-//   mover_place/rank deterministic rank of each incoming mover by its old position
-//   permute_pass     per tile: rank the stayers inside their old cell and write the next
-//                    permutation src'[dest] = j (4 B per atom instead of moving 48 B)
-//   finalize         per-cloud diagnostics, knife temperature, step counter
+//                    sort key (stayers ranked in their cell by warp ballots), count leavers L[c] /
+//                    incoming movers I[c], list movers, and add exact totals into per-cloud
+//                    buckets.  The only heavy pass: the step is computed once.
+//   scan_reduce      per-cell counts n_c - L_c + I_c, block sums, largest cell; its last block
+//                    runs the top level (block offsets, next tile size, per-cloud starts and tile
+//                    offsets, overflow-cell carries)
+//   scan_down        new start[], movers' base slots, next tiling; extra blocks close each
+//                    cloud's step totals (diagnostics, knife temperature, step counter)
+//   permute_pass     the next permutation src'[dest] = j for the stayers (4 B per atom instead of
+//                    moving 48 B), and each incoming mover's slot in its cell's incoming list
+//   mover_rank       deterministic rank of each incoming mover by its old position -> src'
 // The new order is the stable sort by (new cell, moved?, old position): in each new cell the atoms
 // that stayed keep their order, followed by the atoms that entered it, by old position.  Tiles are
 // contiguous, cloud-pure ranges of sorted positions whose boundaries snap to cell starts (the
