@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=50)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-drift", action="store_true")
+    ap.add_argument("--drift-steps", type=int, default=200)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
@@ -174,6 +176,41 @@ def adjoint_vs_plain(stream, steps: int, checkpoint_every: int) -> dict:
             "fwd_adjoint_over_plain": (g["ms_record"] + g["ms_forward"] + g["ms_backward"]) / ms_plain,
             "collisions_recorded": g["collisions"], "loss": g["loss"],
             "grad_fp32_vs_fp64_max_abs_over_max": float(np.max(np.abs(g32 - g64)) / scale) if scale > 0 else 0.0}
+
+
+def fp32_drift(stream, atoms: int, steps: int) -> dict:
+    """The measured workload in FP32 against an FP64 run of the same cloud: the FP64 initial state,
+    rounded to FP32, advanced `steps` steps in both precisions (same seeds, same random numbers);
+    the relative difference of every diagnostic."""
+    import numpy as np
+    from cudadsmc_b200 import FP64, Simulation
+    run, c = workload(atoms)
+    run64 = run.copy()
+    run64.precision = FP64
+    s64 = Simulation(run64, c)
+    s64.set_stream(stream.cuda_stream)
+    s64.init_cloud(run.seed)
+    st = s64.get_state()
+
+    def lanes32(a):
+        out = a.astype(np.float32)
+        out[:, 3] = a[:, 3].view(np.uint64).astype(np.uint32).view(np.float32)  # id / flag bits
+        return out
+
+    s32 = Simulation(run, c)
+    s32.set_stream(stream.cuda_stream)
+    s32.set_state(lanes32(st["pos"]), lanes32(st["vel"]), st["psi"].astype(np.float32), st["cloud_counts"])
+    del st
+    s64.step(steps)
+    s32.step(steps)
+    a, b = s32.diagnostics(), s64.diagnostics()
+    keys = ("n_alive", "temperature", "e_kin", "e_pot", "e_evaporated", "n_evaporated", "n_majorana",
+            "n_knife", "collisions", "candidates", "sum_v2", "sum_absB")
+    rel = {k: (abs(a[k] - b[k]) / abs(b[k]) if b[k] else float(abs(a[k]))) for k in keys}
+    s32.close()
+    s64.close()
+    return {"atoms": atoms, "steps": steps, "relative_drift": rel,
+            "definition": "|FP32 - FP64| / |FP64| per diagnostic after the same steps from the same state"}
 
 
 def batched_vs_sequential(stream, steps: int) -> dict:
@@ -379,6 +416,11 @@ def main():
     if rank == 0 and ws == 1 and not args.no_batched:
         batched = batched_vs_sequential(stream, steps=args.batched_steps)
 
+    # ------------------------------------------------------------------ FP32 against FP64
+    drift = None
+    if rank == 0 and ws == 1 and not args.no_drift:
+        drift = fp32_drift(stream, args.atoms, args.drift_steps)
+
     # ------------------------------------------------------------------ forward + adjoint vs plain
     adjoint = None
     if rank == 0 and ws == 1 and not args.no_adjoint:
@@ -400,7 +442,7 @@ def main():
                            "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
                            "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"},
                 "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint, "fp32_drift": drift,
                 "n_alive_end": d1["n_alive"]}
         print(json.dumps(line), flush=True)
     sim.close()
