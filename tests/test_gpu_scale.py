@@ -3,7 +3,7 @@ the drift of the FP32 engine's diagnostics against an FP64 run of the same cloud
 import numpy as np
 import pytest
 
-from cudadsmc_b200 import FP64, Simulation, preset
+from cudadsmc_b200 import FP32, FP64, Simulation, preset
 
 pytestmark = pytest.mark.gpu
 
@@ -63,3 +63,29 @@ def test_fp32_drift_against_fp64():
     print("FP32 vs FP64 relative drift after 200 steps:", rel,
           "collisions", a["collisions"], b["collisions"])
     assert rel["n_alive"] < 1e-3 and rel["temperature"] < 1e-3 and rel["e_kin"] < 2e-3
+
+
+def test_homogeneous_box_full_config():
+    # the homogeneous-gas check as configured (homogeneousGasCollisions.py / collisionComparison.py
+    # setting): 1e6 test atoms standing for 1e10 (alpha = 1e4) in a periodic 1 mm^3 box at 10 uK,
+    # 100^3 cells (one atom per cell on average), dt = 5 us, 2000 steps, FP32.  The collision rate
+    # per atom equals 1/2 n sigma <v_r>, <v_r> = sqrt(16 kT / (pi m)), within four statistical
+    # errors and 1 %, and elastic collisions keep the temperature constant.
+    run, c = preset(1)
+    assert run.precision == FP32 and c.n_atoms == 1_000_000 and c.cells[0] == 100
+    sim = Simulation(run, c)
+    sim.init_cloud(11)
+    d0 = sim.diagnostics()
+    steps = 2000
+    sim.step(steps)
+    d = sim.diagnostics()
+    assert d["error"] == 0 and d["n_alive"] == c.n_atoms
+    kb, m = 1.3806503e-23, 1.443160648e-25
+    volume = np.prod([c.grid_max[a] - c.grid_min[a] for a in range(3)])
+    n_real = c.alpha * c.n_atoms / volume
+    sigma = 8 * np.pi * (5.3e-9) ** 2
+    analytic = 0.5 * n_real * sigma * np.sqrt(16 * kb * c.temperature / (np.pi * m))
+    events = d["collisions"] - d0["collisions"]
+    rate = events / (steps * run.dt) / c.n_atoms
+    assert abs(rate - analytic) < 4 * rate / np.sqrt(events) + 0.01 * analytic, (rate, analytic, events)
+    assert abs(d["temperature"] - d0["temperature"]) / d0["temperature"] < 0.01
