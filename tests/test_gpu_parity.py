@@ -96,6 +96,22 @@ def test_small_trap_steps_bit_exact(precision):
     run_pair(run, c, 120, check_every=[1, 1, 18, 100])
 
 
+def test_small_configuration_as_specified_bit_exact():
+    # the small trapped configuration exactly as specified: 1e4 atoms, 50^3 cells, FP64, 1000
+    # steps with collisions, run by the serial C++ step and by the GPU: identical after every decade
+    run, c = scaled(0, precision=FP64)
+    assert c.n_atoms == 10000 and c.cells[0] == 50
+    run_pair(run, c, 1000, check_every=[1, 9, 90, 900])
+
+
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_motion_and_spin_over_ten_thousand_steps_bit_exact(precision):
+    # motion + Larmor precession + renormalisation over 10^4 steps (no collisions): the GPU state
+    # equals the serial oracle's bit for bit at 10^2, 10^3 and 10^4 steps
+    run, c = scaled(0, n=2000, precision=precision, flags=F_LARMOR | F_NORMALISE)
+    run_pair(run, c, 10000, check_every=[100, 900, 9000])
+
+
 @pytest.mark.parametrize("precision", [FP32, FP64])
 def test_full_step_with_evaporation_bit_exact(precision):
     # Larmor + Majorana + knife ramp; a hotter cloud and a tight knife so atoms are removed
