@@ -89,3 +89,25 @@ def test_homogeneous_box_full_config():
     rate = events / (steps * run.dt) / c.n_atoms
     assert abs(rate - analytic) < 4 * rate / np.sqrt(events) + 0.01 * analytic, (rate, analytic, events)
     assert abs(d["temperature"] - d0["temperature"]) / d0["temperature"] < 0.01
+
+
+def test_batched_ensemble_5000_steps_matches_single_runs():
+    # the batched workload as specified: 256 clouds (atoms log-uniform in [1e3, 1e5], B' in
+    # [1.5, 4] T/m, T in [5, 50] uK, grids 20^3-64^3), autotuned tiles, 5000 steps in one handle;
+    # every cloud's diagnostics equal those of the same cloud run alone for 5000 steps
+    from cudadsmc_b200.workloads import batched_ensemble
+    run, clouds = batched_ensemble()
+    batch = Simulation(run, clouds)
+    batch.init_cloud(run.seed)
+    tile, _ = batch.autotune(3)
+    done = batch.diagnostics()["step"]
+    batch.step(5000 - done)
+    assert batch.diagnostics()["error"] == 0
+    for k, c in enumerate(clouds):
+        s = Simulation(run, c)
+        s.init_cloud(run.seed)
+        s.step(5000)
+        a, b = s.diagnostics(), batch.diagnostics(k)
+        for f in ("step", "n_alive", "sum_v2", "sum_absB", "collisions", "candidates", "n_evaporated"):
+            assert a[f] == b[f], (k, f, a[f], b[f])
+        s.close()
