@@ -1,15 +1,19 @@
 // driver.cpp -- command-line driver with the call structure of CUDADSMC's main()
 // (CUDADSMC/src/main.cu:36-619), running the B200 engine through the C ABI (include/dsmc.h).
 //
-//   dsmc_driver [Nc N] [--preset K] [--steps-per-print S] [--prints P] [--fp64] [--out DIR] [--seed X]
+//   dsmc_driver [Nc N] [--preset K] [--steps-per-print S] [--prints P] [--loops-per-collision L]
+//               [--mcwf] [--fp64] [--out DIR] [--seed X]
 //
 // As in the reference: argv "Nc N" picks Nc^3 cells and N test atoms (main.cu:45-69), alpha is
 // 3e6 / N real atoms per test atom (main.cu:53, initialSystemParameters.cuh:27), the cloud is
 // initialised (main.cu:176-198), then numberOfPrints times the loop body runs
 // collisionsPerPrint x loopsPerCollision motion steps (main.cu:410-524) and a snapshot is
 // written (main.cu:526-577).  Snapshots replace the HDF5 file /atomData/* with one .npy file
-// per dataset and frame in DIR (positions, velocities, psiUp, psiDn, atomID, cellID,
-// atomCount, atomNumber, simuatedTime) -- the names of the reference datasets.
+// per dataset and frame in DIR (positions, velocities, psiUp, psiDn, atomID, atomIsSpinUp,
+// cellID, atomCount, atomNumber, simuatedTime) -- the names of the reference datasets.
+// --loops-per-collision is the reference's loopsPerCollision (main.cu:168: motion steps per
+// collision step, the engine's collide_every); --mcwf turns on the spin-flip and decoherence
+// path that the reference runs once per collision step (main.cu:501-520).
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -62,6 +66,7 @@ void snapshot(dsmc_handle* h, const std::string& dir, int frame, int64_t cap, co
     dsmc_get_cell_starts(h, start.data(), ncells + 1, &ncells);
     std::vector<double> p3(3 * n), v3(3 * n), up(2 * n), dn(2 * n);
     std::vector<int32_t> id(n), cell(n), count(ncells);
+    std::vector<uint8_t> spin_up(n);
     for (long i = 0; i < n; ++i) {
         for (int a = 0; a < 3; ++a) {
             p3[3 * i + a] = pos[4 * i + a];
@@ -72,6 +77,9 @@ void snapshot(dsmc_handle* h, const std::string& dir, int frame, int64_t cap, co
         uint64_t bits = 0;
         std::memcpy(&bits, &pos[4 * i + 3], sizeof(R));
         id[i] = (int32_t)(uint32_t)bits;
+        bits = 0;
+        std::memcpy(&bits, &vel[4 * i + 3], sizeof(R));
+        spin_up[i] = (bits & 1u) ? 0 : 1;  // flag bit 0: anti-trapped
     }
     for (int64_t c = 0; c < ncells; ++c) {
         count[c] = start[c + 1] - start[c];
@@ -83,6 +91,7 @@ void snapshot(dsmc_handle* h, const std::string& dir, int frame, int64_t cap, co
     write_npy(dir + "/psiUp" + f, "<f8", {n, 2}, up.data(), up.size() * 8);
     write_npy(dir + "/psiDn" + f, "<f8", {n, 2}, dn.data(), dn.size() * 8);
     write_npy(dir + "/atomID" + f, "<i4", {n}, id.data(), id.size() * 4);
+    write_npy(dir + "/atomIsSpinUp" + f, "|u1", {n}, spin_up.data(), spin_up.size());
     write_npy(dir + "/cellID" + f, "<i4", {n}, cell.data(), cell.size() * 4);
     write_npy(dir + "/atomCount" + f, "<i4", {(long)ncells}, count.data(), count.size() * 4);
     int32_t number = (int32_t)n;
@@ -95,8 +104,8 @@ void snapshot(dsmc_handle* h, const std::string& dir, int frame, int64_t cap, co
 int main(int argc, char** argv) {
     int Nc = -1;
     long N = -1;
-    int preset = 0, prints = 10, steps_per_print = 100;
-    bool fp64 = false;
+    int preset = 0, prints = 10, steps_per_print = 100, loops_per_collision = 0;
+    bool fp64 = false, mcwf = false;
     std::string out;
     uint64_t seed = 1234;
     std::vector<std::string> pos_args;
@@ -106,6 +115,8 @@ int main(int argc, char** argv) {
         else if (a == "--prints" && i + 1 < argc) prints = std::atoi(argv[++i]);
         else if (a == "--steps-per-print" && i + 1 < argc) steps_per_print = std::atoi(argv[++i]);
         else if (a == "--fp64") fp64 = true;
+        else if (a == "--mcwf") mcwf = true;
+        else if (a == "--loops-per-collision" && i + 1 < argc) loops_per_collision = std::atoi(argv[++i]);
         else if (a == "--out" && i + 1 < argc) out = argv[++i];
         else if (a == "--seed" && i + 1 < argc) seed = std::strtoull(argv[++i], nullptr, 10);
         else pos_args.push_back(a);
@@ -129,6 +140,8 @@ int main(int argc, char** argv) {
         cloud.alpha = N > 0 ? 3e6 / (double)N : 1.0;  // alpha = h_N / N (main.cu:53)
     }
     if (fp64) run.precision = DSMC_FP64;
+    if (loops_per_collision > 0) run.collide_every = loops_per_collision;
+    if (mcwf) cloud.flags |= DSMC_F_MCWF;
     dsmc_handle* h = nullptr;
     if (!check(dsmc_create(&run, &cloud, 1, &h), nullptr, "dsmc_create")) return 1;
     if (!check(dsmc_init_cloud(h, seed), h, "dsmc_init_cloud")) return 1;
