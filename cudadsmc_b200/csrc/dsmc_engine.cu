@@ -50,13 +50,14 @@ template <class T> struct DevBuf {
 
 constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes the tile tables)
 
-// launch shape of the FP32 step_pass: threads per tile, atoms staged per tile (48 B + 4 B of
-// shared memory each), blocks per SM requested from the compiler
+// launch shape of the FP32 step_pass: threads per tile, atoms staged per tile (42 B of shared
+// memory each: position and velocity, storage index, cell, head), blocks per SM requested from
+// the compiler
 #ifndef DSMC_FP32_BLOCK
 #define DSMC_FP32_BLOCK 256
 #endif
 #ifndef DSMC_FP32_CAP
-#define DSMC_FP32_CAP 1024
+#define DSMC_FP32_CAP 1280
 #endif
 #ifndef DSMC_FP32_MINB
 #define DSMC_FP32_MINB 4
@@ -156,7 +157,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
-        smem_tile = (size_t)CAP * (3 * sizeof(R4) + sizeof(int) + sizeof(uint16_t));
+        smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int) + sizeof(uint16_t));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

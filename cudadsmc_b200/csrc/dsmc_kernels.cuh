@@ -394,10 +394,11 @@ template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src
 
 // ---------------------------------------------------------------------------------------------
 // step_pass: the timestep of one tile.
-// The tile's atoms are gathered through src into shared memory with asynchronous 16-byte copies
-// issued all at once (positions, velocities, spinors: CAP x 3 x R4), then the cells collide and
-// every atom moves straight from shared memory; only the new state, the keys and the counters
-// go back to global memory.
+// The tile's positions and velocities are gathered through src into shared memory with
+// asynchronous 16-byte copies issued all at once (CAP x 2 x R4), with each atom's storage index
+// beside them; the cells collide from shared memory, then every atom moves, its spinor loaded
+// through the kept index (only the motion phase reads it, so it takes no staging space and the
+// tiles are larger); only the new state, the keys and the counters go back to global memory.
 // ---------------------------------------------------------------------------------------------
 // ONE: the run has a single cloud, whose parameters are read from the kernel parameter block
 // (constant operands) instead of a shared-memory copy
@@ -408,8 +409,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R4* s_pos = reinterpret_cast<R4*>(smem_raw);
     R4* s_vel = s_pos + CAP;
-    R4* s_psi = s_vel + CAP;
-    int* s_cell = reinterpret_cast<int*>(s_psi + CAP);
+    int* s_src = reinterpret_cast<int*>(s_vel + CAP);  // storage index of each staged atom
+    int* s_cell = s_src + CAP;
     uint16_t* s_head = reinterpret_cast<uint16_t*>(s_cell + CAP);  // first positions of cells to collide
     static_assert(CAP <= 65536, "head positions are 16-bit");
     __shared__ CloudPhys<R> P_sh;
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 }
                 stage(s_pos + t, A.pos_in + s);
                 stage(s_vel + t, A.vel_in + s);
-                stage(s_psi + t, A.psi_in + s);
+                s_src[t] = s;
             }
         }
         if (threadIdx.x == 0) {
@@ -571,9 +572,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             int c_old = 0;
             R4 q, v, s;
             if (valid) {
+                s = A.psi_in[s_src[t]];
                 q = s_pos[t];
                 v = s_vel[t];
-                s = s_psi[t];
                 a.x = q.x; a.y = q.y; a.z = q.z;
                 a.vx = v.x; a.vy = v.y; a.vz = v.z;
                 a.ur = s.x; a.ui = s.y; a.dr = s.z; a.di = s.w;
