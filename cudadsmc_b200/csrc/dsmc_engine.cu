@@ -63,8 +63,8 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #define DSMC_FP32_MINB 4
 #endif
 
-const char* kKernelNames[] = {"step_pass", "scan_reduce", "scan_down", "permute_pass", "mover_rank"};
-constexpr int kNumStepKernels = 5;
+const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
+constexpr int kNumStepKernels = 4;
 
 }  // namespace
 
@@ -120,7 +120,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<CloudDyn> cdyn;
     DevBuf<CloudDiagDev> cdiag;
     DevBuf<Ctl> ctl;
-    DevBuf<int> block_sums, block_off, scan_blk_cloud, scan_blk_cell0, cloud_first_blk;
+    DevBuf<unsigned long long> scan_desc;  // LB_STRIDE words per scan block
+    DevBuf<int> scan_blk_cloud, scan_blk_cell0, cloud_first_blk, d_cell_base;
     // runtime
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -241,11 +242,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(cdyn.p, 0, nclouds * sizeof(CloudDyn)));
         CU(cudaMemset(cdiag.p, 0, nclouds * sizeof(CloudDiagDev)));
         CU(cudaMemset(ctl.p, 0, sizeof(Ctl)));
-        // scan blocks: each covers up to SCAN_CHUNK cells of a single cloud
+        // scan blocks: each covers up to CELL_CHUNK cells of a single cloud
         std::vector<int> bc, b0, first(nclouds + 1);
         for (int k = 0; k < nclouds; ++k) {
             first[k] = (int)bc.size();
-            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += SCAN_CHUNK) {
+            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += CELL_CHUNK) {
                 bc.push_back(k);
                 b0.push_back(c);
             }
@@ -253,7 +254,10 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         first[nclouds] = (int)bc.size();
         nscan_blocks = (int)bc.size();
         scan_blk_cloud.alloc(nscan_blocks); scan_blk_cell0.alloc(nscan_blocks); cloud_first_blk.alloc(nclouds + 1);
-        block_sums.alloc(nscan_blocks); block_off.alloc(nscan_blocks);
+        scan_desc.alloc((size_t)nscan_blocks * LB_STRIDE);
+        CU(cudaMemset(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long)));
+        d_cell_base.alloc(nclouds + 1);
+        CU(cudaMemcpy(d_cell_base.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(scan_blk_cloud.p, bc.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(scan_blk_cell0.p, b0.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(cloud_first_blk.p, first.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
@@ -278,7 +282,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.one = phys[0];
-            A.block_sums = block_sums.p; A.block_off = block_off.p;
+            A.scan_desc = scan_desc.p; A.cloud_cell_base = d_cell_base.p;
             A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
@@ -298,10 +302,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 1: scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A); break;
-        case 2: scan_down<R><<<nscan_blocks + (nclouds + SCAN_BLOCK / 32 - 1) / (SCAN_BLOCK / 32), SCAN_BLOCK, 0, stream>>>(A); break;
-        case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
-        case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 1: scan_cells<R><<<scan_extra_blocks(nclouds) + nscan_blocks, CELL_BLOCK, 0, stream>>>(A); break;
+        case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
+        case 3: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
     }
 
@@ -393,6 +396,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemsetAsync(start[1].p, 0, (total_cells + 1) * sizeof(int), stream));
         CU(cudaMemsetAsync(Lc.p, 0, total_cells * sizeof(int), stream));
         CU(cudaMemsetAsync(Ic.p, 0, total_cells * sizeof(int), stream));
+        // the scan's epoch restarts at 0 with the cleared control block: clear its descriptors too
+        CU(cudaMemsetAsync(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long), stream));
         Args<R> A = args[1];
         A.init_mode = 1;
         SortArgs<R> S;
@@ -408,8 +413,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             gscan_top<<<1, 1024, 0, stream>>>(gb.p, gblocks, nullptr);
             gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p, orank.p);
         }
-        scan_reduce<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
-        scan_down<R><<<nscan_blocks, SCAN_BLOCK, 0, stream>>>(A);
+        scan_cells<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
+        init_tiles<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
         if (n > 0) {
             fs_place<R><<<ab, 256, 0, stream>>>(S, A);
             fs_scatter<R><<<ab, 256, 0, stream>>>(S, A);
@@ -472,6 +477,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             if (h.err & EB_NAN) { m += " non-finite velocity;"; st = DSMC_ERR_NAN; }
             if (h.err & EB_INIT_REJECT) { m += " initial rejection sampling gave up;"; st = DSMC_ERR_INVALID; }
             if (h.err & EB_TILE_OVERFLOW) { m += " tile table overflow;"; st = DSMC_ERR_CAPACITY; }
+            if (h.err & EB_TIMEOUT) { m += " a bounded device-side wait gave up;"; st = DSMC_ERR_TIMEOUT; }
             if (h.err & EB_INCONSISTENT) { m += " inconsistent cell bookkeeping (after an earlier error);"; }
             throw Fail{st, m};
         }

@@ -7,20 +7,21 @@
 //   sorted order groups atoms by global cell (clouds one after another, each cloud's grid cells
 //   then its overflow cell), so every cell is a contiguous range [start[c], start[c+1]) of j.
 //
-// One step = 5 launches with static grids, captured in a CUDA graph of two steps:
+// One step = 4 launches with static grids, captured in a CUDA graph of two steps:
 //   step_pass        per tile of ~T sorted positions: gather the atoms through src, collide the
 //                    tile's cells in shared memory, then move + spin + evaporate every atom once,
 //                    write the new state at its current position j (coalesced) with an 8-byte
 //                    sort key (stayers ranked in their cell by warp ballots), count leavers L[c] /
 //                    incoming movers I[c], list movers, and add exact totals into per-cloud
 //                    buckets.  The only heavy pass: the step is computed once.
-//   scan_reduce      per-cell counts n_c - L_c + I_c, block sums, largest cell; its last block
-//                    runs the top level (block offsets, next tile size, per-cloud starts and tile
-//                    offsets, overflow-cell carries)
-//   scan_down        new start[], movers' base slots, next tiling; extra blocks close each
-//                    cloud's step totals (diagnostics, knife temperature, step counter)
+//   scan_cells       one-pass scan (decoupled look-back) of the per-cell counts n_c - L_c + I_c:
+//                    new start[], movers' base slots, largest cell; its last block runs the top
+//                    level (next tile size, per-cloud starts and tile offsets); extra blocks
+//                    compute the overflow-cell carries and close each cloud's step totals
+//                    (diagnostics, knife temperature, step counter)
 //   permute_pass     the next permutation src'[dest] = j for the stayers (4 B per atom instead of
-//                    moving 48 B), and each incoming mover's slot in its cell's incoming list
+//                    moving 48 B), each incoming mover's slot in its cell's incoming list, and the
+//                    next tiling's starts from the atoms placed at cell starts
 //   mover_rank       deterministic rank of each incoming mover by its old position -> src'
 // The new order is the stable sort by (new cell, moved?, old position): in each new cell the atoms
 // that stayed keep their order, followed by the atoms that entered it, by old position.  Tiles are
@@ -91,18 +92,30 @@ struct Ctl {
     int movers[2];  // movers listed by the step of each parity (the other parity's is cleared by the scan)
     int novf[2];    // tiles with overflow-cell stayers listed by the step of each parity
     int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds prefixes from there on
-    int scan_done;  // scan_reduce blocks finished (the last one runs the top level and clears it)
-    int max_cell;   // largest coming grid-cell count, gathered by scan_reduce (cleared by its top level)
-    int tile_T[2];  // nominal tile size of the tiling built for each parity
+    int scan_done;    // scan_cells blocks finished (the last one runs the top level and clears it)
+    int max_cell;     // largest coming grid-cell count, gathered by scan_cells (cleared by its top level)
+    int tile_T[2];    // nominal tile size of the tiling built for each parity
+    int scan_ticket;  // scan_cells blocks started: a block's ticket is the scan block it processes
+    unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
 };
 
-// sort keys written by step_pass for every current position j
-// keys written by step_pass, one per atom position: .y = kind | (rank << 2)
+// keys written by step_pass, one per atom position: .y = kind | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT)
 //   KIND_STAY  .x = cell, rank among the cell's stayers before it (the cell starts in this tile)
 //   KIND_OVF   .x = tile, rank among the tile's stayers of the cloud's overflow cell, which
 //              started in an earlier tile (the only cell that may be split across tiles)
 //   KIND_MOVE  .x = slot in the step's mover list;  KIND_LOST  .x = -1
+//   KEY_OVF_CELL: the stayer's cell is its cloud's overflow cell (always set with KIND_OVF)
 enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2, KIND_OVF = 3 };
+constexpr int KEY_OVF_CELL = 4;
+constexpr int KEY_RANK_SHIFT = 3;
+// mover records written by step_pass: .x = target cell, .y = old position, .z = ticket in the
+// target cell, .w = cloud | MREC_OVF_CELL when the target is the cloud's overflow cell
+constexpr int MREC_OVF_CELL = 1 << 30;
+
+__device__ __forceinline__ int2 stayer_key(bool split_ovf, int tile, int cell, int rank, bool ovf_cell) {
+    return split_ovf ? make_int2(tile, KIND_OVF | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT))
+                     : make_int2(cell, KIND_STAY | (ovf_cell ? KEY_OVF_CELL : 0) | (rank << KEY_RANK_SHIFT));
+}
 
 template <class R> struct Args {
     typedef typename V4T<R>::type R4;
@@ -138,8 +151,8 @@ template <class R> struct Args {
     CloudDyn* cdyn;
     CloudDiagDev* cdiag;
     Ctl* ctl;
-    int* block_sums;
-    int* block_off;
+    unsigned long long* scan_desc;  // look-back descriptor of each scan block (LB_STRIDE apart)
+    const int* cloud_cell_base;     // first cell of each cloud, nclouds + 1
     const int* scan_blk_cloud;
     const int* scan_blk_cell0;
     const int* cloud_first_blk;  // nclouds + 1
@@ -620,8 +633,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                         reinterpret_cast<int*>(s_pos + t)[0] = rank;
                         s_cell[t] = (int)((unsigned)c_old | 0x80000000u);
                     } else {
-                        A.keys[tb + t] = (split && c_old == c_first) ? make_int2(b, KIND_OVF | (rank << 2))
-                                                                      : make_int2(c_old, KIND_STAY | (rank << 2));
+                        A.keys[tb + t] = stayer_key(split && c_old == c_first, b, c_old, rank, c_old == P.ovf_cell);
                     }
                 }
             }
@@ -649,7 +661,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
                 tbase = __shfl_sync(peers, tbase, leader);
                 const int ticket = tbase + __popc(peers & ((1u << lane) - 1u));
-                A.mrec[slot] = make_int4(o.cell, tb + t, ticket, 0);
+                A.mrec[slot] = make_int4(o.cell, tb + t, ticket, cloud | (o.cell == P.ovf_cell ? MREC_OVF_CELL : 0));
             }
             if (valid) {
                 const int j = tb + t;
@@ -699,19 +711,77 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 rank += s_tcnt[qq];
                 if (!s_twhole[qq]) break;
             }
-            A.keys[tb + t] = (split && c == c_first) ? make_int2(b, KIND_OVF | (rank << 2))
-                                                     : make_int2(c, KIND_STAY | (rank << 2));
+            A.keys[tb + t] = stayer_key(split && c == c_first, b, c, rank, c == P.ovf_cell);
         }
         __syncthreads();  // the staging arrays, red and s_lost are reused by the next tile
     }
 }
 
 // ---------------------------------------------------------------------------------------------
+// Tile starts of the coming step, written where the atoms are placed (permute_pass, mover_rank,
+// and init_tiles after a full sort).  The nominal starts S + j*T of cloud k (S its first sorted
+// position, T the coming nominal size) that fall inside a grid cell [st, e) snap to the cell's end,
+// except one exactly at st; the overflow cell, which never collides, begins a tile at each
+// nominal start inside it (the only cell split across tiles).
+// ---------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ int cloud_of_cell(const Args<R>& A, int c) {
+    if (A.nclouds == 1) return 0;
+    int lo = 0, hi = A.nclouds - 1;  // the last cloud whose first cell is <= c
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (A.cloud_cell_base[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// every tile start in the non-empty cell [st, e) of cloud k
+template <class R>
+__device__ void cell_tile_starts(const Args<R>& A, int k, int st, int e, bool ovf) {
+    const int q = 1 - A.parity;
+    const int S = A.cdyn[k].start[q], toff = A.cdyn[k].tile_off[q];
+    const int T = A.ctl->tile_T[q];
+    if (T <= 0 || st < S) {
+        atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        return;
+    }
+    for (int j = (st - S + T - 1) / T; S + j * T < e; ++j) {
+        const int pnom = S + j * T;
+        const int tbeg = pnom == st ? st : (ovf ? pnom : e);
+        const int ti = toff + j;
+        if (ti < A.max_tiles) {
+            A.tile_begin_next[ti] = tbeg;
+            A.tile_cloud_next[ti] = k;
+            A.tile_split_next[ti] = (tbeg != st && tbeg != e) ? 1 : 0;
+        }
+    }
+}
+
+// the tile start at position x of cloud k's overflow cell (which begins at st), if x is a nominal start
+template <class R>
+__device__ __forceinline__ void ovf_tile_start(const Args<R>& A, int k, int st, int x) {
+    const int q = 1 - A.parity;
+    const int S = A.cdyn[k].start[q];
+    const int T = A.ctl->tile_T[q];
+    const int r = x - S;
+    if (T <= 0 || r < 0 || r % T != 0) return;
+    const int ti = A.cdyn[k].tile_off[q] + r / T;
+    if (ti < A.max_tiles) {
+        A.tile_begin_next[ti] = x;
+        A.tile_cloud_next[ti] = k;
+        A.tile_split_next[ti] = x != st ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // permute_pass: the stayers' part of the next step's gather permutation.  A stayer of cell c with
 // rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
-// KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Movers are placed by
-// mover_rank, after this kernel has listed each cell's incoming movers.  Flat streams over the
-// keys and the mover records, no shared memory and no barriers.
+// KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  The stayer placed at a
+// grid cell's first position writes the cell's tile starts of the coming step; every stayer of an
+// overflow cell checks its own position.  Movers are placed by mover_rank, after this kernel has
+// listed each cell's incoming movers.  Flat streams over the keys and the mover records, no
+// shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
@@ -732,7 +802,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 #pragma unroll
             for (int i = 0; i < G; ++i) key[i] = j0 + i < n ? A.keys[j0 + i] : make_int2(-1, KIND_LOST);
         }
-        int c[G], base[G];
+        int c[G], base[G], kc[G];
         bool ok[G];
 #pragma unroll
         for (int i = 0; i < G; ++i) {
@@ -740,6 +810,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             ok[i] = kind == KIND_STAY || kind == KIND_OVF;
             c[i] = key[i].x;
             base[i] = 0;
+            kc[i] = -1;
             if (kind == KIND_OVF) {
                 const int b = key[i].x;
                 if (b < 0 || b >= ntiles) {
@@ -748,6 +819,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
                     continue;
                 }
                 const int cloud = A.tile_cloud[b];
+                kc[i] = cloud;
                 c[i] = A.clouds[cloud].ovf_cell;
                 const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
                 base[i] = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
@@ -766,9 +838,15 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 #pragma unroll
         for (int i = 0; i < G; ++i) {
             if (!ok[i]) continue;
-            const int dest = lo[i] + base[i] + (key[i].y >> 2);
-            if (dest >= lo[i] && dest < hi[i]) A.src_out[dest] = j0 + i;
-            else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            const int r = base[i] + (key[i].y >> KEY_RANK_SHIFT);
+            const int dest = lo[i] + r;
+            if (dest >= lo[i] && dest < hi[i]) {
+                A.src_out[dest] = j0 + i;
+                if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kc[i] >= 0 ? kc[i] : cloud_of_cell(A, c[i]), lo[i], dest);
+                else if (r == 0) cell_tile_starts(A, cloud_of_cell(A, c[i]), lo[i], hi[i], false);
+            } else {
+                atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            }
         }
     }
     // incoming movers: each writes its old position into its cell's incoming slots (ticket order)
@@ -782,16 +860,116 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// per-cell scans. Each scan block covers <= SCAN_ITEMS*SCAN_BLOCK cells of one cloud.
-// count of cell c after the step: (old_start[c+1] - old_start[c]) - L[c] + I[c]
+// The cell scan of a step, in one pass (scan_cells).  Each scan block covers <= CELL_CHUNK cells of
+// one cloud; the count of cell c after the step is (old_start[c+1] - old_start[c]) - L[c] + I[c].
+// A block takes its scan block from a ticket (so blocks start in scan order), publishes its sum,
+// and finds its offset by looking back over the descriptors of the scan blocks before it: it only
+// ever waits on blocks that started before it, and every wait is bounded in time.
 // ---------------------------------------------------------------------------------------------
 constexpr int SCAN_BLOCK = 256;
-constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_ITEMS = 8;  // items per thread of the generic scans (gscan_*)
 constexpr int SCAN_CHUNK = SCAN_BLOCK * SCAN_ITEMS;
+#ifndef DSMC_CELL_BLOCK
+#define DSMC_CELL_BLOCK 512
+#endif
+#ifndef DSMC_LB_STRIDE
+#define DSMC_LB_STRIDE 32
+#endif
+constexpr int CELL_BLOCK = DSMC_CELL_BLOCK;  // threads of a scan_cells block
+constexpr int CELL_ITEMS = 16;               // cells per thread: the launch fits the device at once
+constexpr int CELL_CHUNK = CELL_BLOCK * CELL_ITEMS;
+// descriptors lie LB_STRIDE words apart (one per 256 bytes), so that the look-back reads of all
+// blocks spread over the L2 slices instead of queueing on the few that hold a dense array
+constexpr int LB_STRIDE = DSMC_LB_STRIDE;
+
+// blocks of a physics-step scan_cells launch ahead of its scan blocks: one for the overflow-cell
+// carries, then one per CELL_BLOCK / 32 clouds for the clouds' step totals
+__host__ __device__ constexpr int scan_extra_blocks(int nclouds) {
+    return 1 + (nclouds + CELL_BLOCK / 32 - 1) / (CELL_BLOCK / 32);
+}
 
 template <class R>
 __device__ __forceinline__ int cloud_cell_end(const Args<R>& A, int cloud) {
     return A.clouds[cloud].ovf_cell + 1;
+}
+
+// descriptor of a scan block, one 64-bit word: (epoch << 34) | (status << 32) | value, where the
+// epoch numbers the scan launch that wrote it (a word left by an earlier launch reads as not ready)
+// and the value is the block's sum (LB_AGG) or its inclusive prefix (LB_INC)
+enum : unsigned { LB_NONE = 0, LB_AGG = 1, LB_INC = 2 };
+constexpr unsigned LB_EPOCH_MASK = 0x3fffffffu;
+// a look-back that sees no progress for this long gives up with EB_TIMEOUT instead of hanging
+constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned status, unsigned v) {
+    return ((unsigned long long)(epoch & LB_EPOCH_MASK) << 34) | ((unsigned long long)status << 32) | v;
+}
+__device__ __forceinline__ unsigned lb_status(unsigned long long w, unsigned epoch) {
+    return (unsigned)(w >> 34) == (epoch & LB_EPOCH_MASK) ? (unsigned)(w >> 32) & 3u : LB_NONE;
+}
+// the descriptor word carries all its data, so device-scope relaxed accesses suffice
+__device__ __forceinline__ void lb_store(unsigned long long* desc, int b, unsigned long long w) {
+    unsigned long long* p = desc + (size_t)b * LB_STRIDE;
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ unsigned long long lb_load(const unsigned long long* desc, int b) {
+    const unsigned long long* p = desc + (size_t)b * LB_STRIDE;
+    unsigned long long w;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Exclusive prefix of scan block blk (one full warp; the result is the same in every lane).  The
+// warp reads the LB_WINDOW descriptors before it (lane l holds distances 8l .. 8l+7, nearest
+// first) and adds the values up to the nearest inclusive prefix once all of them are published;
+// with none in the window it adds them all and moves on.
+constexpr int LB_PER_LANE = 8;
+constexpr int LB_WINDOW = 32 * LB_PER_LANE;
+__device__ unsigned lb_exclusive(const unsigned long long* desc, int blk, unsigned epoch, int* err) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned excl = 0;
+    int base = blk - 1;
+    const unsigned long long t0 = global_ns();
+    while (base >= 0) {
+        unsigned v[LB_PER_LANE];
+        unsigned incm = 0, pendm = 0;
+#pragma unroll
+        for (int u = 0; u < LB_PER_LANE; ++u) {
+            const int i = base - lane * LB_PER_LANE - u;
+            const unsigned long long w = i >= 0 ? lb_load(desc, i) : lb_word(epoch, LB_INC, 0u);
+            const unsigned st = lb_status(w, epoch);
+            v[u] = (unsigned)w;
+            incm |= (st == LB_INC ? 1u : 0u) << u;
+            pendm |= (st == LB_NONE ? 1u : 0u) << u;
+        }
+        const unsigned inc = __ballot_sync(FULL, incm != 0);
+        const int near = inc ? __ffs(inc) - 1 : 32;  // nearest lane holding an inclusive prefix
+        // positions of this lane that count: all before the nearest lane, up to its first inclusive
+        const unsigned use = lane < near ? (1u << LB_PER_LANE) - 1u
+                                         : (lane == near ? ((incm & (0u - incm)) << 1) - 1u : 0u);
+        if (!__any_sync(FULL, (pendm & use) != 0)) {
+            unsigned sum = 0;
+#pragma unroll
+            for (int u = 0; u < LB_PER_LANE; ++u) sum += ((use >> u) & 1u) ? v[u] : 0u;
+            excl += __reduce_add_sync(FULL, sum);
+            if (inc) break;
+            base -= LB_WINDOW;
+            continue;
+        }
+        const bool late = __shfl_sync(FULL, global_ns() - t0 > LB_TIMEOUT_NS ? 1 : 0, 0) != 0;
+        if (late) {
+            if (lane == 0) atomicOr(err, EB_TIMEOUT);
+            break;
+        }
+        __nanosleep(32);
+    }
+    return excl;
 }
 
 // Step totals of cloud k from its buckets (one warp; the buckets are cleared), the knife
@@ -868,43 +1046,20 @@ __global__ void __launch_bounds__(32) finalize(Args<R> A) {
     finalize_cloud<R, INIT>(A, blockIdx.x, threadIdx.x);
 }
 
-// Top level of the cell scan, run by the last scan_reduce block: offsets of the scan blocks,
-// per-cloud counts, starts and tile offsets of the coming step, the overflow-cell carries of the
-// listed tiles, and the coming step's counters.
+// Top level of the cell scan, run by the last scan_cells block to finish: per-cloud counts, starts
+// and tile offsets of the coming step (from the blocks' inclusive prefixes), the coming step's
+// counters and nominal tile size, and the reset of the scan's ticket for the next launch.
 template <class R, int BLOCK>
-__device__ void scan_top_block(const Args<R>& A) {
+__device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
     __shared__ uint32_t wsum[32];
-    __shared__ int s_carry, s_tcarry;
-    const int p = A.parity, q = 1 - p;
-    // 1. exclusive scan of the block sums (written by the other blocks of this kernel: read from L2)
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    for (int base = 0; base < A.nscan_blocks; base += BLOCK * SCAN_ITEMS) {
-        const int i0 = base + threadIdx.x * SCAN_ITEMS;
-        int v[SCAN_ITEMS];
-        uint32_t s = 0;
-#pragma unroll
-        for (int k = 0; k < SCAN_ITEMS; ++k) {
-            v[k] = i0 + k < A.nscan_blocks ? __ldcg(A.block_sums + i0 + k) : 0;
-            s += (uint32_t)v[k];
-        }
-        uint32_t tot;
-        uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
-#pragma unroll
-        for (int k = 0; k < SCAN_ITEMS; ++k) {
-            if (i0 + k < A.nscan_blocks) A.block_off[i0 + k] = (int)ex;
-            ex += (uint32_t)v[k];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) s_carry += (int)tot;
-        __syncthreads();
-    }
-    const int total = s_carry;
+    __shared__ int s_tcarry;
+    const int q = 1 - A.parity;
+    const int total = (int)(unsigned)lb_load(A.scan_desc, A.nscan_blocks - 1);
     // the coming tiling's nominal size: the preferred size, or less where a cell holds so many
     // atoms that a tile snapped to cell boundaries could outgrow the staging capacity
     const int mc = __ldcg(&A.ctl->max_cell);
     const int T = max(min(A.tile_nominal, A.tile_cap + 1 - mc), MIN_TILE);
-    // 2. per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK)
+    // per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK)
     if (threadIdx.x == 0) s_tcarry = 0;
     __syncthreads();
     for (int base = 0; base < A.nclouds; base += BLOCK) {
@@ -912,8 +1067,8 @@ __device__ void scan_top_block(const Args<R>& A) {
         int n = 0, st = 0, nt = 0;
         if (k < A.nclouds) {
             const int fb = A.cloud_first_blk[k], lb = A.cloud_first_blk[k + 1] - 1;
-            st = A.block_off[fb];
-            n = A.block_off[lb] + __ldcg(A.block_sums + lb) - st;
+            st = fb > 0 ? (int)(unsigned)lb_load(A.scan_desc, fb - 1) : 0;
+            n = (int)(unsigned)lb_load(A.scan_desc, lb) - st;
             nt = (n + T - 1) / T;
         }
         uint32_t tot;
@@ -940,157 +1095,213 @@ __device__ void scan_top_block(const Args<R>& A) {
         A.ctl->novf[q] = 0;
         A.ctl->tile_T[q] = T;
         A.ctl->max_cell = 0;
-    }
-    // 3. overflow-cell stayers: exclusive prefix of tile_ovf over the tiles from the lowest to the
-    //    highest listed one (tile_ovf is zero on every unlisted tile, so a listed tile's carry is
-    //    its prefix minus the prefix at its cloud's first tile, or at the lowest listed tile)
-    if (!A.init_mode) {
-        __shared__ int s_lo, s_hi;
-        if (threadIdx.x == 0) {
-            s_lo = 0x7fffffff;
-            s_hi = -1;
-        }
-        __syncthreads();
-        const int m = min(A.ctl->novf[p], A.max_tiles);
-        for (int i = threadIdx.x; i < m; i += BLOCK) {
-            const int b = A.ovf_list[i];
-            atomicMin(&s_lo, b);
-            atomicMax(&s_hi, b);
-        }
-        __syncthreads();
-        const int lo = s_lo, hi = s_hi;
-        if (threadIdx.x == 0) A.ctl->ovf_lo[p] = lo;
-        constexpr int IT = 16;
-        if (threadIdx.x == 0) s_carry = 0;
-        __syncthreads();
-        for (int base = lo; base <= hi; base += BLOCK * IT) {
-            const int i0 = base + threadIdx.x * IT;
-            int v[IT];
-            uint32_t s = 0;
-#pragma unroll
-            for (int k = 0; k < IT; ++k) {
-                v[k] = (i0 + k <= hi) ? A.tile_ovf[i0 + k] : 0;
-                s += (uint32_t)v[k];
-            }
-            uint32_t tot;
-            uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
-#pragma unroll
-            for (int k = 0; k < IT; ++k) {
-                if (i0 + k <= hi) A.tile_ovf_carry[i0 + k] = (int)ex;
-                ex += (uint32_t)v[k];
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) s_carry += (int)tot;
-            __syncthreads();
-        }
+        A.ctl->scan_ticket = 0;
+        A.ctl->scan_epoch = epoch + 1;
     }
 }
 
-// Block sums of the coming cell counts; the last block to finish runs the top level of the scan.
-template <class R>
-__global__ void __launch_bounds__(SCAN_BLOCK) scan_reduce(Args<R> A) {
+// Overflow-cell stayers, run by one block of a physics-step scan_cells launch beside the scan:
+// exclusive prefix of tile_ovf over the tiles from the lowest to the highest listed one (tile_ovf
+// is zero on every unlisted tile, so a listed tile's carry is its prefix minus the prefix at its
+// cloud's first tile, or at the lowest listed tile)
+template <class R, int BLOCK>
+__device__ void ovf_carries(const Args<R>& A) {
     __shared__ uint32_t wsum[32];
-    __shared__ int s_last;
-    const int blk = blockIdx.x;
-    const int cloud = A.scan_blk_cloud[blk];
-    const int c0 = A.scan_blk_cell0[blk];
-    const int cend = cloud_cell_end(A, cloud);
-    __shared__ int s_max;
-    if (threadIdx.x == 0) s_max = 0;
-    uint32_t s = 0;
-    int m = 0;  // largest grid-cell count (the cloud's overflow cell, its last, is split across tiles)
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
-        if (c < cend) {
-            const int cnt = (A.old_start[c + 1] - A.old_start[c]) - A.Lc[c] + A.Ic[c];
-            s += (uint32_t)cnt;
-            if (c < cend - 1) m = max(m, cnt);
-        }
-    }
-    m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
-    uint32_t tot;
-    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
-    block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot);
+    __shared__ int s_carry, s_lo, s_hi;
+    const int p = A.parity;
     if (threadIdx.x == 0) {
-        A.block_sums[blk] = (int)tot;
+        s_lo = 0x7fffffff;
+        s_hi = -1;
+        s_carry = 0;
+    }
+    __syncthreads();
+    const int m = min(A.ctl->novf[p], A.max_tiles);
+    for (int i = threadIdx.x; i < m; i += BLOCK) {
+        const int b = A.ovf_list[i];
+        atomicMin(&s_lo, b);
+        atomicMax(&s_hi, b);
+    }
+    __syncthreads();
+    const int lo = s_lo, hi = s_hi;
+    if (threadIdx.x == 0) A.ctl->ovf_lo[p] = lo;
+    constexpr int IT = 16;
+    for (int base = lo; base <= hi; base += BLOCK * IT) {
+        const int i0 = base + threadIdx.x * IT;
+        int v[IT];
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            v[k] = (i0 + k <= hi) ? A.tile_ovf[i0 + k] : 0;
+            s += (uint32_t)v[k];
+        }
+        uint32_t tot;
+        uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            if (i0 + k <= hi) A.tile_ovf_carry[i0 + k] = (int)ex;
+            ex += (uint32_t)v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += (int)tot;
+        __syncthreads();
+    }
+}
+
+// The cell scan of a step: new start[], the movers' base slots, cleared leaver / incoming counters,
+// the largest grid-cell count, and (last block) the top level.  In a physics step the launch puts
+// scan_extra_blocks(nclouds) blocks ahead of the scan blocks: the overflow-cell carries, then the
+// clouds' step totals, one warp per cloud; after a full sort it carries the scan blocks alone.
+template <class R>
+__global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args<R> A) {
+    __shared__ uint32_t wsum[32];
+    __shared__ int s_blk, s_last, s_max;
+    __shared__ unsigned s_excl;
+    const int nextra = (int)gridDim.x - A.nscan_blocks;
+    if ((int)blockIdx.x < nextra) {
+        if (A.init_mode) return;
+        if (blockIdx.x == 0) {
+            ovf_carries<R, CELL_BLOCK>(A);
+        } else {
+            const int k = (blockIdx.x - 1) * (CELL_BLOCK / 32) + (threadIdx.x >> 5);
+            if (k < A.nclouds) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
+        }
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned epoch = *reinterpret_cast<volatile unsigned*>(&A.ctl->scan_epoch);
+    if (threadIdx.x == 0) {
+        s_blk = atomicAdd(&A.ctl->scan_ticket, 1);
+        s_max = 0;
+    }
+    __syncthreads();
+    const int blk = s_blk;
+    if (blk < A.nscan_blocks) {
+        const int cloud = A.scan_blk_cloud[blk];
+        const int c0 = A.scan_blk_cell0[blk];
+        const int cend = cloud_cell_end(A, cloud);
+        const int cb = c0 + threadIdx.x * CELL_ITEMS;
+        // a block of CELL_CHUNK cells from a 16-byte boundary: vector loads and stores
+        const bool whole = (c0 & 3) == 0 && c0 + CELL_CHUNK <= cend;
+        constexpr int NV = CELL_ITEMS / 4;
+        int cnt[CELL_ITEMS], in[CELL_ITEMS];
+        unsigned lmask = 0, imask = 0;  // cells with leavers / incoming movers (counters to clear)
+        if (whole) {
+            int sv[CELL_ITEMS + 1];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const int4 t = *reinterpret_cast<const int4*>(A.old_start + cb + 4 * v);
+                sv[4 * v] = t.x; sv[4 * v + 1] = t.y; sv[4 * v + 2] = t.z; sv[4 * v + 3] = t.w;
+            }
+            sv[CELL_ITEMS] = A.old_start[cb + CELL_ITEMS];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const int4 l = *reinterpret_cast<const int4*>(A.Lc + cb + 4 * v);
+                const int4 m = *reinterpret_cast<const int4*>(A.Ic + cb + 4 * v);
+                const int lv[4] = {l.x, l.y, l.z, l.w};
+                const int iv[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = 4 * v + u;
+                    in[k] = iv[u];
+                    cnt[k] = sv[k + 1] - sv[k] - lv[u] + iv[u];
+                    lmask |= (lv[u] != 0 ? 1u : 0u) << k;
+                    imask |= (iv[u] != 0 ? 1u : 0u) << k;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < CELL_ITEMS; ++k) {
+                const int c = cb + k;
+                const bool ok = c < cend;
+                const int lv = ok ? A.Lc[c] : 0;
+                in[k] = ok ? A.Ic[c] : 0;
+                cnt[k] = ok ? A.old_start[c + 1] - A.old_start[c] - lv + in[k] : 0;
+                lmask |= (lv != 0 ? 1u : 0u) << k;
+                imask |= (in[k] != 0 ? 1u : 0u) << k;
+            }
+        }
+        uint32_t s = 0;
+        int m = 0;  // largest grid-cell count (the cloud's overflow cell, its last, is split across tiles)
+#pragma unroll
+        for (int k = 0; k < CELL_ITEMS; ++k) {
+            s += (uint32_t)cnt[k];
+            if (cb + k < cend - 1) m = max(m, cnt[k]);
+        }
+        m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
+        if (lane == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan_u32<CELL_BLOCK>(s, wsum, tot);
+        if (threadIdx.x < 32) {
+            unsigned excl = 0;
+            if (blk == 0) {
+                if (lane == 0) lb_store(A.scan_desc, 0, lb_word(epoch, LB_INC, tot));
+            } else {
+                if (lane == 0) lb_store(A.scan_desc, blk, lb_word(epoch, LB_AGG, tot));
+                excl = lb_exclusive(A.scan_desc, blk, epoch, &A.ctl->err);
+                if (lane == 0) lb_store(A.scan_desc, blk, lb_word(epoch, LB_INC, excl + tot));
+            }
+            if (lane == 0) s_excl = excl;
+        }
+        __syncthreads();
+        int st = (int)(ex + s_excl);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            int o[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = 4 * v + u;
+                o[u] = st;
+                if ((imask >> k) & 1u) A.mover_base[cb + k] = st + cnt[k] - in[k];
+                st += cnt[k];
+            }
+            if (whole) {
+                *reinterpret_cast<int4*>(A.new_start + cb + 4 * v) = make_int4(o[0], o[1], o[2], o[3]);
+                if ((lmask >> (4 * v)) & 15u) *reinterpret_cast<int4*>(A.Lc + cb + 4 * v) = make_int4(0, 0, 0, 0);
+                if ((imask >> (4 * v)) & 15u) *reinterpret_cast<int4*>(A.Ic + cb + 4 * v) = make_int4(0, 0, 0, 0);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = 4 * v + u;
+                    if (cb + k < cend) A.new_start[cb + k] = o[u];
+                    if ((lmask >> k) & 1u) A.Lc[cb + k] = 0;
+                    if ((imask >> k) & 1u) A.Ic[cb + k] = 0;
+                }
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicOr(&A.ctl->err, EB_INCONSISTENT);  // more scan blocks than tickets: an earlier launch failed
+    }
+    if (threadIdx.x == 0) {
         if (s_max > 0) atomicMax(&A.ctl->max_cell, s_max);
         __threadfence();
-        s_last = atomicAdd(&A.ctl->scan_done, 1) == (int)gridDim.x - 1;
+        s_last = atomicAdd(&A.ctl->scan_done, 1) == A.nscan_blocks - 1;
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
     if (threadIdx.x == 0) A.ctl->scan_done = 0;
-    scan_top_block<R, SCAN_BLOCK>(A);
+    scan_top_block<R, CELL_BLOCK>(A, epoch);
 }
 
-// New cell starts, the movers' base slots and the coming step's tiles (start and cloud); cleared
-// leaver / incoming counters.  The launch carries one extra block per SCAN_BLOCK / 32 clouds, whose
-// warps close the clouds' step totals (in a physics step) beside the scan blocks.
+// Tile starts of the tiling the scan built after a full sort (no atoms are placed by
+// permute_pass then): the same rule, per cell.
 template <class R>
-__global__ void __launch_bounds__(SCAN_BLOCK) scan_down(Args<R> A) {
-    __shared__ uint32_t wsum[32];
-    const int q = 1 - A.parity;
+__global__ void __launch_bounds__(CELL_BLOCK) init_tiles(Args<R> A) {
     const int blk = blockIdx.x;
-    if (blk >= A.nscan_blocks) {
-        const int k = (blk - A.nscan_blocks) * (SCAN_BLOCK / 32) + (threadIdx.x >> 5);
-        if (!A.init_mode && k < A.nclouds) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
-        return;
-    }
     const int cloud = A.scan_blk_cloud[blk];
     const int c0 = A.scan_blk_cell0[blk];
     const int cend = cloud_cell_end(A, cloud);
-    const int ovf = cend - 1;
-    int cnt[SCAN_ITEMS], oldc[SCAN_ITEMS], lv[SCAN_ITEMS], in[SCAN_ITEMS];
-    uint32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
-        if (c < cend) {
-            oldc[k] = A.old_start[c + 1] - A.old_start[c];
-            lv[k] = A.Lc[c];
-            in[k] = A.Ic[c];
-            cnt[k] = oldc[k] - lv[k] + in[k];
-        } else {
-            oldc[k] = 0; lv[k] = 0; in[k] = 0; cnt[k] = 0;
-        }
-        s += (uint32_t)cnt[k];
-    }
-    uint32_t tot;
-    uint32_t ex = block_excl_scan_u32<SCAN_BLOCK>(s, wsum, tot) + (uint32_t)A.block_off[blk];
-    const CloudDyn& d = A.cdyn[cloud];
-    const int S = d.start[q];
-    const int toff = d.tile_off[q];
-    const int T = A.ctl->tile_T[q];
-    // nominal tile starts S + j*T: the first at or after this thread's first cell, then in order
-    int j = ((int)ex - S + T - 1) / T;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const int c = c0 + threadIdx.x * SCAN_ITEMS + k;
-        if (c < cend) {
-            const int st = (int)ex;
-            A.new_start[c] = st;
-            if (in[k] > 0) A.mover_base[c] = st + oldc[k] - lv[k];
-            if (lv[k]) A.Lc[c] = 0;
-            if (in[k]) A.Ic[c] = 0;
-            const int e = st + cnt[k];
-            for (; S + j * T < e; ++j) {  // nominal starts inside this cell snap to its end
-                const int pnom = S + j * T;
-                const int tbeg = pnom == st ? st : (c == ovf ? pnom : e);
-                const int ti = toff + j;
-                if (ti < A.max_tiles) {
-                    A.tile_begin_next[ti] = tbeg;
-                    A.tile_cloud_next[ti] = cloud;
-                    A.tile_split_next[ti] = (tbeg != st && tbeg != e) ? 1 : 0;
-                }
-            }
-            ex += (uint32_t)cnt[k];
-        }
+    for (int k = 0; k < CELL_ITEMS; ++k) {
+        const int c = c0 + threadIdx.x * CELL_ITEMS + k;
+        if (c >= cend) break;
+        const int st = A.new_start[c], e = A.new_start[c + 1];
+        if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1);
     }
 }
 
-// rank = number of incoming movers of the same cell with a smaller old position
+// rank = number of incoming movers of the same cell with a smaller old position; the mover placed
+// at a grid cell's first position writes the cell's tile starts, every overflow-cell mover checks
+// its own position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
     const int m = A.ctl->movers[A.parity];
@@ -1104,8 +1315,19 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
         }
         int rank = 0;
         for (int k = lo; k < hi; ++k) rank += (A.in_list[k] < r.y) ? 1 : 0;
-        if (lo + rank < hi && r.y >= 0 && r.y < A.capacity) A.src_out[lo + rank] = r.y;
-        else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        const int x = lo + rank;
+        if (x < hi && r.y >= 0 && r.y < A.capacity) {
+            A.src_out[x] = r.y;
+            const int k = r.w & (MREC_OVF_CELL - 1);
+            if (r.w & MREC_OVF_CELL) {
+                ovf_tile_start(A, k, A.new_start[r.x], x);
+            } else if (rank == 0) {
+                const int st = A.new_start[r.x];
+                if (st == lo) cell_tile_starts(A, k, st, hi, false);
+            }
+        } else {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        }
     }
 }
 

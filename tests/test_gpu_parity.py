@@ -181,7 +181,7 @@ def test_profiling_mode_identical():
     orc.step(5)
     assert_same(a, orc)
     t = a.kernel_times()
-    assert len(t) == a.launches_per_step() == 5
+    assert len(t) == a.launches_per_step() == 4
     assert all(v[1] == 5 for v in t.values())
 
 
