@@ -15,13 +15,15 @@
 //                    incoming movers I[c], list movers, and add exact totals into per-cloud
 //                    buckets.  The only heavy pass: the step is computed once.
 //   scan_cells       one-pass scan (decoupled look-back) of the per-cell counts n_c - L_c + I_c:
-//                    new start[], movers' base slots, largest cell; its last block runs the top
-//                    level (next tile size, per-cloud starts and tile offsets); extra blocks
+//                    new start[], movers' base slots, largest cell, the next tiling of a single
+//                    cloud; its last block runs the top level (next tile size, per-cloud starts
+//                    and tile offsets); extra blocks
 //                    compute the overflow-cell carries and close each cloud's step totals
 //                    (diagnostics, knife temperature, step counter)
 //   permute_pass     the next permutation src'[dest] = j for the stayers (4 B per atom instead of
-//                    moving 48 B), each incoming mover's slot in its cell's incoming list, and the
-//                    next tiling's starts from the atoms placed at cell starts
+//                    moving 48 B), each incoming mover's slot in its cell's incoming list, and
+//                    (batched clouds, or a changed tile size) the next tiling's starts from the
+//                    atoms placed at cell starts
 //   mover_rank       deterministic rank of each incoming mover by its old position -> src'
 // The new order is the stable sort by (new cell, moved?, old position): in each new cell the atoms
 // that stayed keep their order, followed by the atoms that entered it, by old position.  Tiles are
@@ -96,6 +98,7 @@ struct Ctl {
     int max_cell;     // largest coming grid-cell count, gathered by scan_cells (cleared by its top level)
     int tile_T[2];    // nominal tile size of the tiling built for each parity
     int scan_ticket;  // scan_cells blocks started: a block's ticket is the scan block it processes
+    int tiles_built[2];  // 1: scan_cells wrote the tiling of that parity (else the atoms' placement does)
     unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
 };
 
@@ -777,9 +780,9 @@ __device__ __forceinline__ void ovf_tile_start(const Args<R>& A, int k, int st, 
 // ---------------------------------------------------------------------------------------------
 // permute_pass: the stayers' part of the next step's gather permutation.  A stayer of cell c with
 // rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
-// KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  The stayer placed at a
-// grid cell's first position writes the cell's tile starts of the coming step; every stayer of an
-// overflow cell checks its own position.  Movers are placed by mover_rank, after this kernel has
+// KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Unless scan_cells built
+// the coming tiling, the stayer placed at a grid cell's first position writes the cell's tile
+// starts; every stayer of an overflow cell checks its own position.  Movers are placed by mover_rank, after this kernel has
 // listed each cell's incoming movers.  Flat streams over the keys and the mover records, no
 // shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
@@ -788,6 +791,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
     const int p = A.parity;
     const int n = A.ctl->n[p];
     const int ntiles = A.ctl->ntiles[p];
+    const bool tiles = A.ctl->tiles_built[1 - p] == 0;  // the coming tiling is built here
     // four consecutive positions per thread and pass: two 16-byte key loads, then the cell
     // starts of all four, then the stores (the loads of one pass are independent)
     constexpr int G = 4;
@@ -842,8 +846,10 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             const int dest = lo[i] + r;
             if (dest >= lo[i] && dest < hi[i]) {
                 A.src_out[dest] = j0 + i;
-                if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kc[i] >= 0 ? kc[i] : cloud_of_cell(A, c[i]), lo[i], dest);
-                else if (r == 0) cell_tile_starts(A, cloud_of_cell(A, c[i]), lo[i], hi[i], false);
+                if (tiles) {
+                    if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kc[i] >= 0 ? kc[i] : cloud_of_cell(A, c[i]), lo[i], dest);
+                    else if (r == 0) cell_tile_starts(A, cloud_of_cell(A, c[i]), lo[i], hi[i], false);
+                }
             } else {
                 atomicOr(&A.ctl->err, EB_INCONSISTENT);
             }
@@ -1093,6 +1099,7 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
+        A.ctl->tiles_built[q] = (A.nclouds == 1 && !A.init_mode && T == A.ctl->tile_T[A.parity]) ? 1 : 0;
         A.ctl->tile_T[q] = T;
         A.ctl->max_cell = 0;
         A.ctl->scan_ticket = 0;
@@ -1168,6 +1175,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
         return;
     }
     const int lane = threadIdx.x & 31;
+    const bool spec = A.nclouds == 1 && !A.init_mode;
     const unsigned epoch = *reinterpret_cast<volatile unsigned*>(&A.ctl->scan_epoch);
     if (threadIdx.x == 0) {
         s_blk = atomicAdd(&A.ctl->scan_ticket, 1);
@@ -1244,6 +1252,11 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
         }
         __syncthreads();
         int st = (int)(ex + s_excl);
+        // one cloud in a physics step: the tiling of the coming step, built here with the current
+        // nominal size (it starts at sorted position 0 and tile 0); kept by the top level when the
+        // coming size turns out the same, else rebuilt where the atoms are placed
+        const int Ts = spec ? A.ctl->tile_T[A.parity] : 0;
+        int j = spec && Ts > 0 ? (st + Ts - 1) / Ts : 0;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             int o[4];
@@ -1252,7 +1265,19 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
                 const int k = 4 * v + u;
                 o[u] = st;
                 if ((imask >> k) & 1u) A.mover_base[cb + k] = st + cnt[k] - in[k];
-                st += cnt[k];
+                const int e = st + cnt[k];
+                if (spec && Ts > 0) {
+                    for (; j * Ts < e; ++j) {  // nominal starts inside this cell snap to its end
+                        const int pnom = j * Ts;
+                        const int tbeg = pnom == st ? st : (cb + k == cend - 1 ? pnom : e);
+                        if (j < A.max_tiles) {
+                            A.tile_begin_next[j] = tbeg;
+                            A.tile_cloud_next[j] = 0;
+                            A.tile_split_next[j] = (tbeg != st && tbeg != e) ? 1 : 0;
+                        }
+                    }
+                }
+                st = e;
             }
             if (whole) {
                 *reinterpret_cast<int4*>(A.new_start + cb + 4 * v) = make_int4(o[0], o[1], o[2], o[3]);
@@ -1299,12 +1324,13 @@ __global__ void __launch_bounds__(CELL_BLOCK) init_tiles(Args<R> A) {
     }
 }
 
-// rank = number of incoming movers of the same cell with a smaller old position; the mover placed
-// at a grid cell's first position writes the cell's tile starts, every overflow-cell mover checks
-// its own position
+// rank = number of incoming movers of the same cell with a smaller old position; unless scan_cells
+// built the coming tiling, the mover placed at a grid cell's first position writes the cell's tile
+// starts, every overflow-cell mover checks its own position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
     const int m = A.ctl->movers[A.parity];
+    const bool tiles = A.ctl->tiles_built[1 - A.parity] == 0;  // the coming tiling is built here
     for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
         const int4 r = A.mrec[i];
         const int lo = A.mover_base[r.x];
@@ -1319,11 +1345,13 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
         if (x < hi && r.y >= 0 && r.y < A.capacity) {
             A.src_out[x] = r.y;
             const int k = r.w & (MREC_OVF_CELL - 1);
-            if (r.w & MREC_OVF_CELL) {
-                ovf_tile_start(A, k, A.new_start[r.x], x);
-            } else if (rank == 0) {
-                const int st = A.new_start[r.x];
-                if (st == lo) cell_tile_starts(A, k, st, hi, false);
+            if (tiles) {
+                if (r.w & MREC_OVF_CELL) {
+                    ovf_tile_start(A, k, A.new_start[r.x], x);
+                } else if (rank == 0) {
+                    const int st = A.new_start[r.x];
+                    if (st == lo) cell_tile_starts(A, k, st, hi, false);
+                }
             }
         } else {
             atomicOr(&A.ctl->err, EB_INCONSISTENT);
