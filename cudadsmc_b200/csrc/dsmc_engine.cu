@@ -121,7 +121,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<CloudDiagDev> cdiag;
     DevBuf<Ctl> ctl;
     DevBuf<unsigned long long> scan_desc;  // LB_STRIDE words per scan block
-    DevBuf<int> scan_blk_cloud, scan_blk_cell0, cloud_first_blk, d_cell_base;
+    DevBuf<int4> scan_blk;
+    DevBuf<int> cloud_first_blk, d_cell_base;
     // runtime
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -243,23 +244,21 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(cdiag.p, 0, nclouds * sizeof(CloudDiagDev)));
         CU(cudaMemset(ctl.p, 0, sizeof(Ctl)));
         // scan blocks: each covers up to CELL_CHUNK cells of a single cloud
-        std::vector<int> bc, b0, first(nclouds + 1);
+        std::vector<int4> hb;
+        std::vector<int> first(nclouds + 1);
         for (int k = 0; k < nclouds; ++k) {
-            first[k] = (int)bc.size();
-            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += CELL_CHUNK) {
-                bc.push_back(k);
-                b0.push_back(c);
-            }
+            first[k] = (int)hb.size();
+            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += CELL_CHUNK)
+                hb.push_back(make_int4(k, c, cloud_cell_base[k + 1], 0));
         }
-        first[nclouds] = (int)bc.size();
-        nscan_blocks = (int)bc.size();
-        scan_blk_cloud.alloc(nscan_blocks); scan_blk_cell0.alloc(nscan_blocks); cloud_first_blk.alloc(nclouds + 1);
+        first[nclouds] = (int)hb.size();
+        nscan_blocks = (int)hb.size();
+        scan_blk.alloc(nscan_blocks); cloud_first_blk.alloc(nclouds + 1);
         scan_desc.alloc((size_t)nscan_blocks * LB_STRIDE);
         CU(cudaMemset(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long)));
         d_cell_base.alloc(nclouds + 1);
         CU(cudaMemcpy(d_cell_base.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(scan_blk_cloud.p, bc.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(scan_blk_cell0.p, b0.data(), nscan_blocks * sizeof(int), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(scan_blk.p, hb.data(), nscan_blocks * sizeof(int4), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(cloud_first_blk.p, first.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
     }
 
@@ -283,7 +282,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.one = phys[0];
             A.scan_desc = scan_desc.p; A.cloud_cell_base = d_cell_base.p;
-            A.scan_blk_cloud = scan_blk_cloud.p; A.scan_blk_cell0 = scan_blk_cell0.p;
+            A.scan_blk = scan_blk.p;
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
             A.max_tiles = max_tiles; A.tile_nominal = tile_nominal; A.tile_cap = CAP;

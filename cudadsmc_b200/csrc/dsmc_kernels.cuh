@@ -156,8 +156,7 @@ template <class R> struct Args {
     Ctl* ctl;
     unsigned long long* scan_desc;  // look-back descriptor of each scan block (LB_STRIDE apart)
     const int* cloud_cell_base;     // first cell of each cloud, nclouds + 1
-    const int* scan_blk_cloud;
-    const int* scan_blk_cell0;
+    const int4* scan_blk;  // per scan block: cloud, first cell, end of the cloud's cells (one load)
     const int* cloud_first_blk;  // nclouds + 1
     int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
     int tile_cap;  // atoms a tile can stage (CAP): a tiling of nominal size T fits cells of CAP - T + 1
@@ -894,11 +893,6 @@ __host__ __device__ constexpr int scan_extra_blocks(int nclouds) {
     return 1 + (nclouds + CELL_BLOCK / 32 - 1) / (CELL_BLOCK / 32);
 }
 
-template <class R>
-__device__ __forceinline__ int cloud_cell_end(const Args<R>& A, int cloud) {
-    return A.clouds[cloud].ovf_cell + 1;
-}
-
 // descriptor of a scan block, one 64-bit word: (epoch << 34) | (status << 32) | value, where the
 // epoch numbers the scan launch that wrote it (a word left by an earlier launch reads as not ready)
 // and the value is the block's sum (LB_AGG) or its inclusive prefix (LB_INC)
@@ -1065,10 +1059,18 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
     // atoms that a tile snapped to cell boundaries could outgrow the staging capacity
     const int mc = __ldcg(&A.ctl->max_cell);
     const int T = max(min(A.tile_nominal, A.tile_cap + 1 - mc), MIN_TILE);
-    // per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK)
+    // per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK; one cloud holds them all)
     if (threadIdx.x == 0) s_tcarry = 0;
+    if (A.nclouds == 1 && threadIdx.x == 0) {
+        CloudDyn& d = A.cdyn[0];
+        d.n[q] = total;
+        d.start[q] = 0;
+        d.ntiles[q] = (total + T - 1) / T;
+        d.tile_off[q] = 0;
+        s_tcarry = d.ntiles[q];
+    }
     __syncthreads();
-    for (int base = 0; base < A.nclouds; base += BLOCK) {
+    for (int base = 0; A.nclouds > 1 && base < A.nclouds; base += BLOCK) {
         const int k = base + threadIdx.x;
         int n = 0, st = 0, nt = 0;
         if (k < A.nclouds) {
@@ -1184,9 +1186,8 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
     __syncthreads();
     const int blk = s_blk;
     if (blk < A.nscan_blocks) {
-        const int cloud = A.scan_blk_cloud[blk];
-        const int c0 = A.scan_blk_cell0[blk];
-        const int cend = cloud_cell_end(A, cloud);
+        const int4 hb = A.scan_blk[blk];
+        const int c0 = hb.y, cend = hb.z;
         const int cb = c0 + threadIdx.x * CELL_ITEMS;
         // a block of CELL_CHUNK cells from a 16-byte boundary: vector loads and stores
         const bool whole = (c0 & 3) == 0 && c0 + CELL_CHUNK <= cend;
@@ -1313,9 +1314,8 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
 template <class R>
 __global__ void __launch_bounds__(CELL_BLOCK) init_tiles(Args<R> A) {
     const int blk = blockIdx.x;
-    const int cloud = A.scan_blk_cloud[blk];
-    const int c0 = A.scan_blk_cell0[blk];
-    const int cend = cloud_cell_end(A, cloud);
+    const int4 hb = A.scan_blk[blk];
+    const int cloud = hb.x, c0 = hb.y, cend = hb.z;
     for (int k = 0; k < CELL_ITEMS; ++k) {
         const int c = c0 + threadIdx.x * CELL_ITEMS + k;
         if (c >= cend) break;
