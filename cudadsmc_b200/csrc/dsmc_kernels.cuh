@@ -401,6 +401,8 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// an L2 prefetch of the line holding p (no register result, so nothing waits on it)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src) {
 #pragma unroll
     for (int o = 0; o < (int)sizeof(R4); o += 16)
@@ -507,11 +509,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 stage(s_pos + t, A.pos_in + s);
                 stage(s_vel + t, A.vel_in + s);
                 s_src[t] = s;
+                prefetch_l2(A.psi_in + s);  // read in the motion phase: an L2 hit by then
             }
         }
         if (threadIdx.x == 0) {
             s_nhead = 0;
             s_ovf = 0;
+        }
+        // the next tile's storage indices into L2 (its first DRAM round trip), while the
+        // gathers of this one are in flight
+        {
+            const int bn = b + gridDim.x;
+            if (bn < ntiles && threadIdx.x < CAP / 32) {
+                const int ntb = A.tile_begin[bn], nte = A.tile_begin[bn + 1];
+                const int x = ntb + 32 * threadIdx.x;
+                if (x < nte) prefetch_l2(A.src_in + x);
+            }
         }
         // each thread's cell pass reads only the positions it staged itself: its own copies
         // suffice, the barrier after the pass publishes the cells and the staged tile
