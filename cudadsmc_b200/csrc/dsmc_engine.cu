@@ -83,6 +83,7 @@ struct dsmc_handle {
     virtual void set_stream(cudaStream_t s) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) = 0;
+    virtual int check_wait_timeout() = 0;
     virtual void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) = 0;
     virtual void adjoint_run(const dsmc_adj_params* p, dsmc_grad* g) = 0;
     virtual void adjoint_loss(const double* theta, double* loss, double* grad) = 0;
@@ -604,6 +605,29 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemcpy(sigvrmax.p, in, total_cells * sizeof(R), cudaMemcpyHostToDevice));
     }
 
+    // The coming step's scan on its own, its ticket counter started at 1: no block processes scan
+    // block 0, whose descriptor therefore never appears in this launch, and the blocks looking
+    // back to it give up after their time limit. The scan reads the current starts and the
+    // (cleared) leaver / incoming counters and writes only the coming step's starts, tiles and
+    // counters, which the next step's scan writes again; the extra blocks (step totals, overflow
+    // carries) are left out of the launch.
+    int check_wait_timeout() override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "wait check before init"};
+        if (nscan_blocks < 2) throw Fail{DSMC_ERR_INVALID, "the wait check needs more than one scan block of cells"};
+        sync();
+        check_err();
+        const int one = 1;
+        CU(cudaMemcpyAsync(&ctl.p->scan_ticket, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+        scan_cells<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(args[parity]);
+        CU(cudaGetLastError());
+        int bits = 0;
+        CU(cudaMemcpyAsync(&bits, &ctl.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        CU(cudaMemsetAsync(&ctl.p->err, 0, sizeof(int), stream));
+        CU(cudaStreamSynchronize(stream));
+        return bits;
+    }
+
     void set_profiling(bool on) override {
         profiling = on;
         for (int k = 0; k < kNumStepKernels; ++k) { prof_ms[k] = 0; prof_n[k] = 0; }
@@ -1025,6 +1049,11 @@ DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, doubl
     return guard(h, [&] { h->kernel_times(names, ms, launches, cap, count); });
 }
 DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h) { return h ? kNumStepKernels : 0; }
+DSMC_API dsmc_status dsmc_check_wait_timeout(dsmc_handle* h, int32_t* bits) {
+    NEED_H;
+    if (!bits) return DSMC_ERR_INVALID;
+    return guard(h, [&] { *bits = h->check_wait_timeout(); });
+}
 DSMC_API dsmc_status dsmc_adjoint_run(dsmc_handle* h, const dsmc_adj_params* p, dsmc_grad* g) {
     NEED_H;
     if (!p || !g) return DSMC_ERR_INVALID;

@@ -28,7 +28,7 @@ EXPORTED_SYMBOLS = (
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
     "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_export",
-    "dsmc_sort_cells_noalloc",
+    "dsmc_sort_cells_noalloc", "dsmc_check_wait_timeout",
 )
 
 
@@ -71,6 +71,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_kernel_times": (i32, [vp, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(i64), i32,
                                     C.POINTER(i32)]),
         "dsmc_launches_per_step": (i32, [vp]),
+        "dsmc_check_wait_timeout": (i32, [vp, C.POINTER(i32)]),
         "dsmc_autotune": (i32, [vp, i32, C.POINTER(i32), C.POINTER(C.c_double)]),
         "dsmc_adjoint_run": (i32, [vp, C.POINTER(AdjParams), C.POINTER(Grad)]),
         "dsmc_adjoint_loss": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -228,6 +229,13 @@ class Simulation:
 
     def launches_per_step(self) -> int:
         return int(self.lib.dsmc_launches_per_step(self._h))
+
+    def check_wait_timeout(self) -> int:
+        """Runs the coming step's cell scan with its first block withheld (dsmc_check_wait_timeout):
+        returns the device error bits it left, 64 (a bounded wait gave up) among them."""
+        bits = C.c_int32(0)
+        self._check(self.lib.dsmc_check_wait_timeout(self._h, C.byref(bits)))
+        return int(bits.value)
 
     # -- pathwise adjoint -----------------------------------------------------------------------------
     def adjoint_run(self, steps: int, checkpoint_every: int = 100, precision: int = _abi.FP64,

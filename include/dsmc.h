@@ -208,6 +208,15 @@ DSMC_API dsmc_status dsmc_kernel_times(dsmc_handle* h, const char** names, doubl
 /* Number of kernel launches one dsmc_step(h, 1) issues. */
 DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h);
 
+/* Check of the bounded device-side waits (no counterpart in the reference, which has none): runs
+ * the coming step's cell scan once on its own with its first scan block withheld, so that the
+ * blocks after it wait for a prefix that never comes. Each gives up after about a second and sets
+ * the timeout bit (64) of the device error bits, which this call writes to *bits (the scan also
+ * sets 32, the bookkeeping bit, for the block left without work) and then clears. The simulation is
+ * left as it was: that scan writes only what the next step's scan rewrites. Needs a handle whose
+ * cells span at least two scan blocks (more than 4096 cells); takes about a second. */
+DSMC_API dsmc_status dsmc_check_wait_timeout(dsmc_handle* h, int32_t* bits);
+
 /* ---- pathwise adjoint ----------------------------------------------------------------------
  * Gradient of a smoothed loss of the physical run with respect to the trap gradient B', the bias
  * B0 and the knife knot heights eta_0..eta_8, with every random choice of the run held fixed.
