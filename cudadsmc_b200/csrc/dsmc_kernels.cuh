@@ -1178,6 +1178,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
     __shared__ uint32_t wsum[32];
     __shared__ int s_blk, s_last, s_max;
     __shared__ unsigned s_excl;
+    __shared__ int s_ovf_st, s_ovf_end;  // the overflow cell's range, when this block holds it
     const int nextra = (int)gridDim.x - A.nscan_blocks;
     if ((int)blockIdx.x < nextra) {
         if (A.init_mode) return;
@@ -1195,6 +1196,8 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
     if (threadIdx.x == 0) {
         s_blk = atomicAdd(&A.ctl->scan_ticket, 1);
         s_max = 0;
+        s_ovf_st = 0;
+        s_ovf_end = 0;
     }
     __syncthreads();
     const int blk = s_blk;
@@ -1270,7 +1273,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
         // nominal size (it starts at sorted position 0 and tile 0); kept by the top level when the
         // coming size turns out the same, else rebuilt where the atoms are placed
         const int Ts = spec ? A.ctl->tile_T[A.parity] : 0;
-        int j = spec && Ts > 0 ? (st + Ts - 1) / Ts : 0;
+        int j = spec && Ts > 0 ? st / Ts + (st % Ts != 0) : 0;  // the first nominal start at or after st
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             int o[4];
@@ -1281,13 +1284,23 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
                 if ((imask >> k) & 1u) A.mover_base[cb + k] = st + cnt[k] - in[k];
                 const int e = st + cnt[k];
                 if (spec && Ts > 0) {
+                    if (cb + k == cend - 1) {  // the overflow cell: its inner starts, below, by the block
+                        if (j * Ts == st && st < e && j < A.max_tiles) {
+                            A.tile_begin_next[j] = st;
+                            A.tile_cloud_next[j] = 0;
+                            A.tile_split_next[j] = 0;
+                        }
+                        s_ovf_st = st;
+                        s_ovf_end = e;
+                        j = e / Ts + (e % Ts != 0);
+                    }
                     for (; j * Ts < e; ++j) {  // nominal starts inside this cell snap to its end
                         const int pnom = j * Ts;
-                        const int tbeg = pnom == st ? st : (cb + k == cend - 1 ? pnom : e);
+                        const int tbeg = pnom == st ? st : e;
                         if (j < A.max_tiles) {
                             A.tile_begin_next[j] = tbeg;
                             A.tile_cloud_next[j] = 0;
-                            A.tile_split_next[j] = (tbeg != st && tbeg != e) ? 1 : 0;
+                            A.tile_split_next[j] = 0;
                         }
                     }
                 }
@@ -1304,6 +1317,18 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
                     if (cb + k < cend) A.new_start[cb + k] = o[u];
                     if ((lmask >> k) & 1u) A.Lc[cb + k] = 0;
                     if ((imask >> k) & 1u) A.Ic[cb + k] = 0;
+                }
+            }
+        }
+        // the overflow cell, which may hold many nominal starts: each begins a tile there (split)
+        if (spec && Ts > 0 && c0 + CELL_CHUNK >= cend) {
+            __syncthreads();
+            const int ost = s_ovf_st, oend = s_ovf_end;
+            for (int jj = ost / Ts + 1 + threadIdx.x; jj * Ts < oend; jj += CELL_BLOCK) {
+                if (jj < A.max_tiles) {
+                    A.tile_begin_next[jj] = jj * Ts;
+                    A.tile_cloud_next[jj] = 0;
+                    A.tile_split_next[jj] = 1;
                 }
             }
         }
