@@ -123,7 +123,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<Ctl> ctl;
     DevBuf<unsigned long long> scan_desc;  // LB_STRIDE words per scan block
     DevBuf<int4> scan_blk;
-    DevBuf<int> cloud_first_blk, d_cell_base;
+    DevBuf<int> cloud_first_blk, d_cell_base, sort_off;
     // runtime
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -132,6 +132,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     int64_t steps_taken = 0;
     Args<R> args[2];
     cudaGraphExec_t graph2 = nullptr;  // two steps: parity 0 then 1
+    cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step of each parity (odd step counts)
     bool use_graphs = true;
     bool profiling = false;
     double prof_ms[kNumStepKernels] = {0};
@@ -185,7 +186,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     }
 
     ~Engine() override {
-        if (graph2) cudaGraphExecDestroy(graph2);
+        drop_graphs();
         for (int i = 0; i <= kNumStepKernels; ++i)
             if (ev[i]) cudaEventDestroy(ev[i]);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -258,6 +259,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         scan_desc.alloc((size_t)nscan_blocks * LB_STRIDE);
         CU(cudaMemset(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long)));
         d_cell_base.alloc(nclouds + 1);
+        sort_off.alloc(nclouds + 1);
         CU(cudaMemcpy(d_cell_base.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(scan_blk.p, hb.data(), nscan_blocks * sizeof(int4), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(cloud_first_blk.p, first.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
@@ -312,17 +314,33 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         for (int k = 0; k < kNumStepKernels; ++k) launch_step_kernel(k, args[p]);
     }
 
-    void build_graph() {
-        if (graph2) return;
+    // the step sequence of parities p0 (and p1 when >= 0) captured into *out
+    void capture_steps(cudaGraphExec_t* out, int p0, int p1) {
         cudaGraph_t g;
         CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(0);
-        enqueue_step(1);
+        enqueue_step(p0);
+        if (p1 >= 0) enqueue_step(p1);
         cudaError_t e = cudaStreamEndCapture(stream, &g);
         if (e != cudaSuccess) throw Fail{DSMC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)};
-        e = cudaGraphInstantiate(&graph2, g, 0);
+        e = cudaGraphInstantiate(out, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) throw Fail{DSMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)};
+    }
+    void build_graph() {
+        if (!graph2) capture_steps(&graph2, 0, 1);
+    }
+    // one step of parity p: its graph, captured on first use
+    void launch_one_step(int p) {
+        if (!graph1[p]) capture_steps(&graph1[p], p, -1);
+        CU(cudaGraphLaunch(graph1[p], stream));
+    }
+    void drop_graphs() {
+        if (graph2) cudaGraphExecDestroy(graph2);
+        graph2 = nullptr;
+        for (int p = 0; p < 2; ++p) {
+            if (graph1[p]) cudaGraphExecDestroy(graph1[p]);
+            graph1[p] = nullptr;
+        }
     }
 
     void step(int n) override {
@@ -348,7 +366,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         } else {
             if (use_graphs && n - done >= 2) build_graph();
             if (use_graphs && parity == 1 && n - done >= 1) {
-                enqueue_step(1);
+                launch_one_step(1);
                 parity = 0;
                 ++done;
             }
@@ -357,7 +375,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
                 done += 2;
             }
             for (; done < n; ++done) {
-                enqueue_step(parity);
+                if (use_graphs) launch_one_step(parity);
+                else enqueue_step(parity);
                 parity ^= 1;
             }
         }
@@ -369,7 +388,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 
     void set_stream(cudaStream_t s) override {
         sync();
-        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        drop_graphs();
         if (own_stream && stream) cudaStreamDestroy(stream);
         own_stream = false;
         stream = s;
@@ -384,13 +403,17 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         std::vector<int> off(nclouds + 1, 0);
         for (int k = 0; k < nclouds; ++k) { off[k] = n; n += counts[k]; }
         off[nclouds] = n;
-        DevBuf<int> d_off, cell, ticket, oflag, orank, gb;
-        d_off.alloc(nclouds + 1);
-        CU(cudaMemcpyAsync(d_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(sort_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
         const int nn = std::max(n, 1);
-        cell.alloc(nn); ticket.alloc(nn); oflag.alloc(nn); orank.alloc(nn);
         const int gblocks = (nn + SCAN_CHUNK - 1) / SCAN_CHUNK;
-        gb.alloc(gblocks);
+        // the sort's per-atom scratch lives in the step's sort keys and mover records (2 and 4 ints
+        // per atom of capacity), which no sort kernel reads and no step keeps across this call
+        // (n <= capacity, gblocks <= n): no allocation here.  in_list is the sort's own.
+        int* const ticket = reinterpret_cast<int*>(keys.p);
+        int* const oflag = reinterpret_cast<int*>(keys.p) + capacity;
+        int* const orank = reinterpret_cast<int*>(mrec.p);
+        int* const gb = reinterpret_cast<int*>(mrec.p) + capacity;
+        int* const cell = reinterpret_cast<int*>(mrec.p) + 2 * (size_t)capacity;
         // reset bookkeeping: parity 1 is "current" with zero atoms, old starts all zero
         CU(cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), stream));
         CU(cudaMemsetAsync(start[1].p, 0, (total_cells + 1) * sizeof(int), stream));
@@ -403,15 +426,15 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         SortArgs<R> S;
         S.pos_src = ps; S.vel_src = vs; S.psi_src = ss;
         S.pos_dst = pos[0].p; S.vel_dst = vel[0].p; S.psi_dst = psi[0].p;
-        S.cloud_atom_off = d_off.p;
-        S.cell = cell.p; S.ticket = ticket.p; S.ovf_flag = oflag.p; S.ovf_rank = orank.p;
+        S.cloud_atom_off = sort_off.p;
+        S.cell = cell; S.ticket = ticket; S.ovf_flag = oflag; S.ovf_rank = orank;
         S.n = n; S.nclouds = nclouds;
         const int ab = (n + 255) / 256;
         if (n > 0) fs_cells<R><<<ab, 256, 0, stream>>>(S, A);
         if (n > 0) {
-            gscan_reduce<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p);
-            gscan_top<<<1, 1024, 0, stream>>>(gb.p, gblocks, nullptr);
-            gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag.p, n, gb.p, orank.p);
+            gscan_reduce<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag, n, gb);
+            gscan_top<<<1, 1024, 0, stream>>>(gb, gblocks, nullptr);
+            gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag, n, gb, orank);
         }
         scan_cells<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
         init_tiles<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
@@ -435,6 +458,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void init(uint64_t seed) override {
         run.seed = seed;
         for (int p = 0; p < 2; ++p) args[p].seed = seed;
+        sync();
+        drop_graphs();  // the step graphs hold the kernel parameters, the seed among them
         int n = 0;
         std::vector<int> off(nclouds + 1, 0), modes(nclouds);
         for (int k = 0; k < nclouds; ++k) {
@@ -668,7 +693,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         sync();
         tile_nominal = T;
         for (int p = 0; p < 2; ++p) args[p].tile_nominal = T;
-        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        drop_graphs();
     }
 
     // ------------------------------------------------------------------ adjoint
@@ -707,7 +732,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             args[p].clog_off = adj_off.p; args[p].clog_cap = cap; args[p].clog_step0 = 0;
             args[p].clog_steps = ap->steps;
         }
-        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        drop_graphs();
         cudaEvent_t e0 = ev[0], e1 = ev[1];
         CU(cudaEventRecord(e0, stream));
         step(ap->steps);
@@ -719,7 +744,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             args[p].clog_ij = nullptr; args[p].clog_n = nullptr; args[p].clog_count = nullptr;
             args[p].clog_off = nullptr; args[p].clog_cap = 0;
         }
-        if (graph2) { cudaGraphExecDestroy(graph2); graph2 = nullptr; }
+        drop_graphs();
         check_err();
         int cnt = 0;
         CU(cudaMemcpy(&cnt, adj_count.p, sizeof(int), cudaMemcpyDeviceToHost));
