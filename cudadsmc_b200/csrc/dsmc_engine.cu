@@ -123,7 +123,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<Ctl> ctl;
     DevBuf<unsigned long long> scan_desc;  // LB_STRIDE words per scan block
     DevBuf<int4> scan_blk;
-    DevBuf<int> cloud_first_blk, d_cell_base, sort_off;
+    DevBuf<int> cloud_first_blk, d_cell_base, sort_off, init_modes;
+    DevBuf<R> init_sv;
     // runtime
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -260,6 +261,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long)));
         d_cell_base.alloc(nclouds + 1);
         sort_off.alloc(nclouds + 1);
+        init_modes.alloc(nclouds);
+        init_sv.alloc(nclouds);
         CU(cudaMemcpy(d_cell_base.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(scan_blk.p, hb.data(), nscan_blocks * sizeof(int4), cudaMemcpyHostToDevice));
         CU(cudaMemcpy(cloud_first_blk.p, first.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice));
@@ -468,25 +471,19 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             modes[k] = cp[k].init_mode;
         }
         off[nclouds] = n;
-        DevBuf<int> d_off, d_modes;
-        d_off.alloc(nclouds + 1);
-        d_modes.alloc(nclouds);
-        CU(cudaMemcpyAsync(d_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
-        CU(cudaMemcpyAsync(d_modes.p, modes.data(), nclouds * sizeof(int), cudaMemcpyHostToDevice, stream));
+        // per-cloud tables in the handle's small buffers (no allocation per call)
+        CU(cudaMemcpyAsync(sort_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(init_modes.p, modes.data(), nclouds * sizeof(int), cudaMemcpyHostToDevice, stream));
         CU(cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), stream));
         if (n > 0)
-            init_atoms<R><<<(n + 255) / 256, 256, 0, stream>>>(args[0], d_off.p, n, d_modes.p, pos[1].p, vel[1].p,
-                                                                psi[1].p, (unsigned long long)seed);
+            init_atoms<R><<<(n + 255) / 256, 256, 0, stream>>>(args[0], sort_off.p, n, init_modes.p, pos[1].p,
+                                                                vel[1].p, psi[1].p, (unsigned long long)seed);
         // (sigma v_r)max per cell
         std::vector<R> sv(nclouds);
         for (int k = 0; k < nclouds; ++k) sv[k] = (R)default_sigvrmax(run, cp[k]);
-        DevBuf<R> d_sv;
-        DevBuf<int> d_cb;
-        d_sv.alloc(nclouds);
-        d_cb.alloc(nclouds + 1);
-        CU(cudaMemcpyAsync(d_sv.p, sv.data(), nclouds * sizeof(R), cudaMemcpyHostToDevice, stream));
-        CU(cudaMemcpyAsync(d_cb.p, cloud_cell_base.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
-        fill_sigvrmax<R><<<(total_cells + 255) / 256, 256, 0, stream>>>(sigvrmax.p, d_cb.p, d_sv.p, nclouds, total_cells);
+        CU(cudaMemcpyAsync(init_sv.p, sv.data(), nclouds * sizeof(R), cudaMemcpyHostToDevice, stream));
+        fill_sigvrmax<R><<<(total_cells + 255) / 256, 256, 0, stream>>>(sigvrmax.p, d_cell_base.p, init_sv.p, nclouds,
+                                                                          total_cells);
         CU(cudaGetLastError());
         sort_and_measure(pos[1].p, vel[1].p, psi[1].p, cloud_atoms_init);
     }
