@@ -106,6 +106,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     int max_tiles = 0;
     int tile_nominal = 0;
     int nscan_blocks = 0;
+    int cell_block = 256;  // threads of a scan_cells block (cell_block_for)
     std::vector<int> cloud_atoms_init;  // initial atoms per cloud
     std::vector<int> cloud_cell_base;
     // device memory
@@ -246,12 +247,14 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(cdyn.p, 0, nclouds * sizeof(CloudDyn)));
         CU(cudaMemset(cdiag.p, 0, nclouds * sizeof(CloudDiagDev)));
         CU(cudaMemset(ctl.p, 0, sizeof(Ctl)));
-        // scan blocks: each covers up to CELL_CHUNK cells of a single cloud
+        // scan blocks: each covers up to cell_block * CELL_ITEMS cells of a single cloud
+        cell_block = cell_block_for(total_cells);
+        const int chunk = cell_block * CELL_ITEMS;
         std::vector<int4> hb;
         std::vector<int> first(nclouds + 1);
         for (int k = 0; k < nclouds; ++k) {
             first[k] = (int)hb.size();
-            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += CELL_CHUNK)
+            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += chunk)
                 hb.push_back(make_int4(k, c, cloud_cell_base[k + 1], 0));
         }
         first[nclouds] = (int)hb.size();
@@ -307,10 +310,16 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 1: scan_cells<R><<<scan_extra_blocks(nclouds) + nscan_blocks, CELL_BLOCK, 0, stream>>>(A); break;
+        case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
         case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
         case 3: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
+    }
+
+    // the cell scan with `extra` leading blocks (overflow carries and step totals) before the scan blocks
+    void launch_scan(const Args<R>& A, int extra) {
+        if (cell_block == 512) scan_cells<R, 512><<<extra + nscan_blocks, 512, 0, stream>>>(A);
+        else scan_cells<R, 256><<<extra + nscan_blocks, 256, 0, stream>>>(A);
     }
 
     void enqueue_step(int p) {
@@ -439,8 +448,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             gscan_top<<<1, 1024, 0, stream>>>(gb, gblocks, nullptr);
             gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag, n, gb, orank);
         }
-        scan_cells<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
-        init_tiles<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
+        launch_scan(A, 0);
+        if (cell_block == 512) init_tiles<R, 512><<<nscan_blocks, 512, 0, stream>>>(A);
+        else init_tiles<R, 256><<<nscan_blocks, 256, 0, stream>>>(A);
         if (n > 0) {
             fs_place<R><<<ab, 256, 0, stream>>>(S, A);
             fs_scatter<R><<<ab, 256, 0, stream>>>(S, A);
@@ -640,7 +650,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         check_err();
         const int one = 1;
         CU(cudaMemcpyAsync(&ctl.p->scan_ticket, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
-        scan_cells<R><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(args[parity]);
+        launch_scan(args[parity], 0);
         CU(cudaGetLastError());
         int bits = 0;
         CU(cudaMemcpyAsync(&bits, &ctl.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream));

@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// The cell scan of a step, in one pass (scan_cells).  Each scan block covers <= CELL_CHUNK cells of
+// The cell scan of a step, in one pass (scan_cells).  Each scan block covers <= CB * CELL_ITEMS cells of
 // one cloud; the count of cell c after the step is (old_start[c+1] - old_start[c]) - L[c] + I[c].
 // A block takes its scan block from a ticket (so blocks start in scan order), publishes its sum,
 // and finds its offset by looking back over the descriptors of the scan blocks before it: it only
@@ -887,24 +887,22 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_ITEMS = 8;  // items per thread of the generic scans (gscan_*)
 constexpr int SCAN_CHUNK = SCAN_BLOCK * SCAN_ITEMS;
-#ifndef DSMC_CELL_BLOCK
-#define DSMC_CELL_BLOCK 512
-#endif
 #ifndef DSMC_LB_STRIDE
 #define DSMC_LB_STRIDE 32
 #endif
-constexpr int CELL_BLOCK = DSMC_CELL_BLOCK;  // threads of a scan_cells block
-constexpr int CELL_ITEMS = 16;               // cells per thread: the launch fits the device at once
-constexpr int CELL_CHUNK = CELL_BLOCK * CELL_ITEMS;
+// scan_cells block (CB threads, CELL_ITEMS cells each): 512 threads on grids of more than
+// CELL_LARGE_GRID cells (fewer tickets and descriptors), 256 below (a shorter block scan on the
+// critical path of a small grid's step)
+constexpr int CELL_ITEMS = 16;
+constexpr int CELL_LARGE_GRID = 1 << 20;
+inline int cell_block_for(int total_cells) { return total_cells > CELL_LARGE_GRID ? 512 : 256; }
 // descriptors lie LB_STRIDE words apart (one per 256 bytes), so that the look-back reads of all
 // blocks spread over the L2 slices instead of queueing on the few that hold a dense array
 constexpr int LB_STRIDE = DSMC_LB_STRIDE;
 
 // blocks of a physics-step scan_cells launch ahead of its scan blocks: one for the overflow-cell
-// carries, then one per CELL_BLOCK / 32 clouds for the clouds' step totals
-__host__ __device__ constexpr int scan_extra_blocks(int nclouds) {
-    return 1 + (nclouds + CELL_BLOCK / 32 - 1) / (CELL_BLOCK / 32);
-}
+// carries, then one per cb / 32 clouds for the clouds' step totals
+inline int scan_extra_blocks(int nclouds, int cb) { return 1 + (nclouds + cb / 32 - 1) / (cb / 32); }
 
 // descriptor of a scan block, one 64-bit word: (epoch << 34) | (status << 32) | value, where the
 // epoch numbers the scan launch that wrote it (a word left by an earlier launch reads as not ready)
@@ -1173,8 +1171,9 @@ __device__ void ovf_carries(const Args<R>& A) {
 // the largest grid-cell count, and (last block) the top level.  In a physics step the launch puts
 // scan_extra_blocks(nclouds) blocks ahead of the scan blocks: the overflow-cell carries, then the
 // clouds' step totals, one warp per cloud; after a full sort it carries the scan blocks alone.
-template <class R>
-__global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args<R> A) {
+template <class R, int CB>
+__global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
+    constexpr int CELL_CHUNK = CB * CELL_ITEMS;
     __shared__ uint32_t wsum[32];
     __shared__ int s_blk, s_last, s_max;
     __shared__ unsigned s_excl;
@@ -1183,9 +1182,9 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
     if ((int)blockIdx.x < nextra) {
         if (A.init_mode) return;
         if (blockIdx.x == 0) {
-            ovf_carries<R, CELL_BLOCK>(A);
+            ovf_carries<R, CB>(A);
         } else {
-            const int k = (blockIdx.x - 1) * (CELL_BLOCK / 32) + (threadIdx.x >> 5);
+            const int k = (blockIdx.x - 1) * (CB / 32) + (threadIdx.x >> 5);
             if (k < A.nclouds) finalize_cloud<R, false>(A, k, threadIdx.x & 31);
         }
         return;
@@ -1255,7 +1254,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
         m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
         if (lane == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
         uint32_t tot;
-        const uint32_t ex = block_excl_scan_u32<CELL_BLOCK>(s, wsum, tot);
+        const uint32_t ex = block_excl_scan_u32<CB>(s, wsum, tot);
         if (threadIdx.x < 32) {
             unsigned excl = 0;
             if (blk == 0) {
@@ -1324,7 +1323,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
         if (spec && Ts > 0 && c0 + CELL_CHUNK >= cend) {
             __syncthreads();
             const int ost = s_ovf_st, oend = s_ovf_end;
-            for (int jj = ost / Ts + 1 + threadIdx.x; jj * Ts < oend; jj += CELL_BLOCK) {
+            for (int jj = ost / Ts + 1 + threadIdx.x; jj * Ts < oend; jj += CB) {
                 if (jj < A.max_tiles) {
                     A.tile_begin_next[jj] = jj * Ts;
                     A.tile_cloud_next[jj] = 0;
@@ -1344,13 +1343,13 @@ __global__ void __launch_bounds__(CELL_BLOCK, 1024 / CELL_BLOCK) scan_cells(Args
     if (!s_last) return;
     __threadfence();
     if (threadIdx.x == 0) A.ctl->scan_done = 0;
-    scan_top_block<R, CELL_BLOCK>(A, epoch);
+    scan_top_block<R, CB>(A, epoch);
 }
 
 // Tile starts of the tiling the scan built after a full sort (no atoms are placed by
 // permute_pass then): the same rule, per cell.
-template <class R>
-__global__ void __launch_bounds__(CELL_BLOCK) init_tiles(Args<R> A) {
+template <class R, int CB>
+__global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
     const int blk = blockIdx.x;
     const int4 hb = A.scan_blk[blk];
     const int cloud = hb.x, c0 = hb.y, cend = hb.z;
