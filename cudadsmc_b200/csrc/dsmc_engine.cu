@@ -183,7 +183,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // blocks for a tile kernel: no more than the tiles of a tiling of the current nominal size
     // (a cloud of n atoms has at most n / T + 1 tiles) nor than fit on the device at once
     int tile_grid(int resident) const {
-        const int bound = capacity / tile_nominal + nclouds + 2;
+        // the smallest nominal size the scan may pick: one block pass when it adapts to the run
+        const int tmin = args[0].tile_fill > 0 ? std::min(tile_nominal, BLOCK - 16) : tile_nominal;
+        const int bound = capacity / tmin + nclouds + 2;
         return std::max(1, std::min(bound, resident));
     }
 
@@ -295,6 +297,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
             A.max_tiles = max_tiles; A.tile_nominal = tile_nominal; A.tile_cap = CAP;
+            A.tile_pass = BLOCK;
+            A.tile_fill = run.tile_atoms > 0 ? 0 : resident_step;  // an explicit size is kept as given
             A.collide_every = run.collide_every; A.parity = p; A.init_mode = 0;
             A.seed = run.seed;
             A.capacity = capacity;
@@ -699,7 +703,10 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void set_tile(int T) {
         sync();
         tile_nominal = T;
-        for (int p = 0; p < 2; ++p) args[p].tile_nominal = T;
+        for (int p = 0; p < 2; ++p) {
+            args[p].tile_nominal = T;
+            args[p].tile_fill = 0;  // a chosen size is kept as given
+        }
         drop_graphs();
     }
 

@@ -160,6 +160,8 @@ template <class R> struct Args {
     const int* cloud_first_blk;  // nclouds + 1
     int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
     int tile_cap;  // atoms a tile can stage (CAP): a tiling of nominal size T fits cells of CAP - T + 1
+    int tile_pass;  // atoms one step_pass block handles per pass (its thread count)
+    int tile_fill;  // > 0 (the resident step_pass blocks): shrink the nominal size for small runs
     int capacity;
     // collision record (adjoint runs): pairs by atom id, directions, per-step offsets
     int2* clog_ij;
@@ -1069,7 +1071,16 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
     // the coming tiling's nominal size: the preferred size, or less where a cell holds so many
     // atoms that a tile snapped to cell boundaries could outgrow the staging capacity
     const int mc = __ldcg(&A.ctl->max_cell);
-    const int T = max(min(A.tile_nominal, A.tile_cap + 1 - mc), MIN_TILE);
+    int Tn = A.tile_nominal;
+    if (A.tile_fill > 0 && A.tile_pass > 0) {
+        // default size for a small run: the largest tile just under a whole number of block
+        // passes that still gives every resident block a tile (a 1e4-atom cloud then runs 240-atom
+        // tiles on 40 blocks instead of 1008-atom tiles on 10)
+        const int per_block = total / A.tile_fill;
+        const int passes = max(1, min((per_block + 16) / A.tile_pass, (Tn + 16) / A.tile_pass));
+        Tn = min(Tn, passes * A.tile_pass - 16);
+    }
+    const int T = max(min(Tn, A.tile_cap + 1 - mc), MIN_TILE);
     // per-cloud counts, starts, tile offsets (clouds in chunks of BLOCK; one cloud holds them all)
     if (threadIdx.x == 0) s_tcarry = 0;
     if (A.nclouds == 1 && threadIdx.x == 0) {
