@@ -254,10 +254,18 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         const int chunk = cell_block * CELL_ITEMS;
         std::vector<int4> hb;
         std::vector<int> first(nclouds + 1);
+        // a cloud whose cells start off a 4-cell boundary gets a first block of the 1-3 cells up to
+        // it, so that its full blocks start on 16-byte boundaries (vector loads and stores)
         for (int k = 0; k < nclouds; ++k) {
             first[k] = (int)hb.size();
-            for (int c = cloud_cell_base[k]; c < cloud_cell_base[k + 1]; c += chunk)
-                hb.push_back(make_int4(k, c, cloud_cell_base[k + 1], 0));
+            const int c_beg = cloud_cell_base[k], c_end = cloud_cell_base[k + 1];
+            int c = c_beg;
+            const int c_al = std::min((c_beg + 3) & ~3, c_end);
+            if (c_al > c) {
+                hb.push_back(make_int4(k, c, c_end, c_al));
+                c = c_al;
+            }
+            for (; c < c_end; c += chunk) hb.push_back(make_int4(k, c, c_end, std::min(c + chunk, c_end)));
         }
         first[nclouds] = (int)hb.size();
         nscan_blocks = (int)hb.size();

@@ -156,7 +156,7 @@ template <class R> struct Args {
     Ctl* ctl;
     unsigned long long* scan_desc;  // look-back descriptor of each scan block (LB_STRIDE apart)
     const int* cloud_cell_base;     // first cell of each cloud, nclouds + 1
-    const int4* scan_blk;  // per scan block: cloud, first cell, end of the cloud's cells (one load)
+    const int4* scan_blk;  // per scan block: cloud, first cell, end of the cloud's cells, end of the block's
     const int* cloud_first_blk;  // nclouds + 1
     int nclouds, total_cells, nscan_blocks, max_tiles, tile_nominal, collide_every, parity, init_mode;
     int tile_cap;  // atoms a tile can stage (CAP): a tiling of nominal size T fits cells of CAP - T + 1
@@ -1213,10 +1213,10 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
     const int blk = s_blk;
     if (blk < A.nscan_blocks) {
         const int4 hb = A.scan_blk[blk];
-        const int c0 = hb.y, cend = hb.z;
+        const int c0 = hb.y, cend = hb.z, c1 = hb.w;  // this block's cells [c0, c1) of a cloud ending at cend
         const int cb = c0 + threadIdx.x * CELL_ITEMS;
         // a block of CELL_CHUNK cells from a 16-byte boundary: vector loads and stores
-        const bool whole = (c0 & 3) == 0 && c0 + CELL_CHUNK <= cend;
+        const bool whole = (c0 & 3) == 0 && c1 - c0 == CELL_CHUNK;
         constexpr int NV = CELL_ITEMS / 4;
         int cnt[CELL_ITEMS], in[CELL_ITEMS];
         unsigned lmask = 0, imask = 0;  // cells with leavers / incoming movers (counters to clear)
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
 #pragma unroll
             for (int k = 0; k < CELL_ITEMS; ++k) {
                 const int c = cb + k;
-                const bool ok = c < cend;
+                const bool ok = c < c1;
                 const int lv = ok ? A.Lc[c] : 0;
                 in[k] = ok ? A.Ic[c] : 0;
                 cnt[k] = ok ? A.old_start[c + 1] - A.old_start[c] - lv + in[k] : 0;
@@ -1324,14 +1324,14 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = 4 * v + u;
-                    if (cb + k < cend) A.new_start[cb + k] = o[u];
+                    if (cb + k < c1) A.new_start[cb + k] = o[u];
                     if ((lmask >> k) & 1u) A.Lc[cb + k] = 0;
                     if ((imask >> k) & 1u) A.Ic[cb + k] = 0;
                 }
             }
         }
         // the overflow cell, which may hold many nominal starts: each begins a tile there (split)
-        if (spec && Ts > 0 && c0 + CELL_CHUNK >= cend) {
+        if (spec && Ts > 0 && c1 >= cend) {
             __syncthreads();
             const int ost = s_ovf_st, oend = s_ovf_end;
             for (int jj = ost / Ts + 1 + threadIdx.x; jj * Ts < oend; jj += CB) {
@@ -1363,10 +1363,10 @@ template <class R, int CB>
 __global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
     const int blk = blockIdx.x;
     const int4 hb = A.scan_blk[blk];
-    const int cloud = hb.x, c0 = hb.y, cend = hb.z;
+    const int cloud = hb.x, c0 = hb.y, cend = hb.z, c1 = hb.w;
     for (int k = 0; k < CELL_ITEMS; ++k) {
         const int c = c0 + threadIdx.x * CELL_ITEMS + k;
-        if (c >= cend) break;
+        if (c >= c1) break;
         const int st = A.new_start[c], e = A.new_start[c + 1];
         if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1);
     }
