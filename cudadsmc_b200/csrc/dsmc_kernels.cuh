@@ -17,9 +17,8 @@
 //   scan_cells       one-pass scan (decoupled look-back) of the per-cell counts n_c - L_c + I_c:
 //                    new start[], movers' base slots, largest cell, the next tiling of a single
 //                    cloud; its last block runs the top level (next tile size, per-cloud starts
-//                    and tile offsets); extra blocks
-//                    compute the overflow-cell carries and close each cloud's step totals
-//                    (diagnostics, knife temperature, step counter)
+//                    and tile offsets); extra blocks compute the overflow-cell carries and close
+//                    each cloud's step totals (diagnostics, knife temperature, step counter)
 //   permute_pass     the next permutation src'[dest] = j for the stayers (4 B per atom instead of
 //                    moving 48 B), each incoming mover's slot in its cell's incoming list, and
 //                    (batched clouds, or a changed tile size) the next tiling's starts from the
@@ -796,9 +795,9 @@ __device__ __forceinline__ void ovf_tile_start(const Args<R>& A, int k, int st, 
 // rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
 // KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Unless scan_cells built
 // the coming tiling, the stayer placed at a grid cell's first position writes the cell's tile
-// starts; every stayer of an overflow cell checks its own position.  Movers are placed by mover_rank, after this kernel has
-// listed each cell's incoming movers.  Flat streams over the keys and the mover records, no
-// shared memory and no barriers.
+// starts; every stayer of an overflow cell checks its own position.  Movers are placed by
+// mover_rank, after this kernel has listed each cell's incoming movers.  Flat streams over the
+// keys and the mover records, no shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
 template <class R>
 __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
@@ -882,9 +881,12 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 // ---------------------------------------------------------------------------------------------
 // The cell scan of a step, in one pass (scan_cells).  Each scan block covers <= CB * CELL_ITEMS cells of
 // one cloud; the count of cell c after the step is (old_start[c+1] - old_start[c]) - L[c] + I[c].
-// A block takes its scan block from a ticket (so blocks start in scan order), publishes its sum,
-// and finds its offset by looking back over the descriptors of the scan blocks before it: it only
-// ever waits on blocks that started before it, and every wait is bounded in time.
+// A block takes its scan block from a ticket (scan blocks are handed out in the order the blocks
+// start), publishes its sum, and finds its offset by looking back over the descriptors of the scan
+// blocks before it: it only ever waits on blocks that started before it, and every wait is
+// bounded in time.  A block covers the cells [c0, c1) of one cloud; a cloud whose cells start off
+// a 4-cell boundary has a short first block up to it, so that its other blocks load and store
+// 16-byte vectors.
 // ---------------------------------------------------------------------------------------------
 constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_ITEMS = 8;  // items per thread of the generic scans (gscan_*)
@@ -1180,7 +1182,7 @@ __device__ void ovf_carries(const Args<R>& A) {
 
 // The cell scan of a step: new start[], the movers' base slots, cleared leaver / incoming counters,
 // the largest grid-cell count, and (last block) the top level.  In a physics step the launch puts
-// scan_extra_blocks(nclouds) blocks ahead of the scan blocks: the overflow-cell carries, then the
+// scan_extra_blocks(nclouds, CB) blocks ahead of the scan blocks: the overflow-cell carries, then the
 // clouds' step totals, one warp per cloud; after a full sort it carries the scan blocks alone.
 template <class R, int CB>
 __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
