@@ -39,7 +39,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--atoms", type=int, default=10_000_000)
-    ap.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=10, help="timed steps of the CPU baseline sample")
+    ap.add_argument("--cpu-warmup", type=int, default=2, help="untimed steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -103,15 +104,31 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def workload(atoms: int):
-    from cudadsmc_b200 import preset
-    run, c = preset(2)
+def workload(atoms: int, source: str = "engine"):
+    """Run and cloud parameters of the 1e7-atom trapped workload.  source="oracle" takes them from
+    the CPU restatement's copy of the preset table, so that the reference arm never loads the
+    engine library."""
+    if source == "oracle":
+        import oracle
+        run, c = oracle.preset(2)
+    else:
+        from cudadsmc_b200 import preset
+        run, c = preset(2)
     c.n_atoms = atoms
     c.capacity = atoms
     return run, c
 
 
-def cpu_baseline(run, cloud, steps: int, threads: int | None = None, warmup: int = 1) -> dict:
+def config_of(args, ws: int) -> dict:
+    """The workload's config dict, printed identically by both arms."""
+    return {"workload": WORKLOAD, "atoms_per_gpu": args.atoms, "cells": 128 ** 3,
+            "trap": "quadrupole B'=2.5 T/m", "T_uK": 50, "dt": 1e-6,
+            "physics": "NTC collide + Larmor + Verlet + Majorana + knife 6->4 kT",
+            "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
+            "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"}
+
+
+def cpu_baseline(run, cloud, steps: int, threads: int | None = None, warmup: int = 2) -> dict:
     """The CPU restatement (OpenMP, float) timed on the host cores for a bounded sample."""
     import oracle
     if threads:
@@ -266,14 +283,14 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    run, c = workload(args.atoms)
+    run, c = workload(args.atoms, source="oracle")
     # the whole --steps K --warmup W run on the host cores (about 0.4 s per step at 1e7 atoms on 16
     # threads), each step the full workload
     res = cpu_baseline(run, c, steps=max(1, args.steps), warmup=args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": max(1, args.steps), "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox cloud)",
-            "config": {"workload": WORKLOAD, "atoms": args.atoms, "cells": 128 ** 3, "host_threads": res["cores"]},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox thermal cloud, no dataset)",
+            "config": config_of(args, ws),
             "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -408,8 +425,9 @@ def main():
         e2e = {"value": a_steps / (e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": out_bytes / args.steps + ctypes.sizeof(Diag),
+               "K": args.steps,
                "definition": "dsmc_set_state from pinned host buffers, K x (dsmc_step(1) + dsmc_diagnostics "
-                             "read back), dsmc_get_state to host; all inside the timed region",
+                             "read back), dsmc_get_state to host; all inside the timed region (K = --steps)",
                "wall_s": wall}
         sim2.close()
 
@@ -431,18 +449,14 @@ def main():
     # ------------------------------------------------------------------ CPU baseline
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(run, c, steps=args.cpu_steps)
+        cpu = cpu_baseline(run, c, steps=args.cpu_steps, warmup=args.cpu_warmup)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded Philox thermal cloud, no dataset)",
-                "config": {"workload": WORKLOAD, "atoms_per_gpu": args.atoms, "cells": 128 ** 3,
-                           "trap": "quadrupole B'=2.5 T/m", "T_uK": 50, "dt": 1e-6,
-                           "physics": "NTC collide + Larmor + Verlet + Majorana + knife 6->4 kT",
-                           "l2": "inputs larger than L2 (48 B/atom x 1e7 = 480 MB per state buffer)",
-                           "parallelism": f"replicas{ws}" if ws > 1 else "single-gpu"},
+                "config": config_of(args, ws),
                 "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint, "fp32_drift": drift,
                 "n_alive_end": d1["n_alive"]}

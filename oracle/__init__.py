@@ -59,6 +59,12 @@ def load() -> C.CDLL:
             "oracle_advance_atoms_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
                                              i64, i32]),
+            "oracle_step_atoms_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32), i64]),
+            "oracle_collide_cell_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double), i32,
+                                            C.POINTER(C.c_double), C.c_uint32, C.c_uint32, C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_double), i32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -142,6 +148,43 @@ def advance_atoms(run: RunParams, cloud: CloudParams, pos, vel, psi, nsteps: int
     load().oracle_advance_atoms_d(C.byref(run), C.byref(cloud), dp(pos), dp(vel), dp(psi),
                                   fate.ctypes.data_as(C.POINTER(C.c_int32)), pos.shape[0], int(nsteps))
     return pos, vel, psi, fate
+
+
+def step_atoms(run: RunParams, cloud: CloudParams, pos, vel, psi, cut_v2: float):
+    """One FP64 timestep of each atom (Larmor, Verlet, Majorana and knife tests with the cut
+    cut_v2 = 2 eta kB T / m, new cell) without collisions or sort: pos/vel/psi (n, 4), the fourth
+    lane of vel the flag bits.  Returns (pos, vel, psi, fate, cell)."""
+    pos = np.array(pos, np.float64, order="C", copy=True)
+    vel = np.array(vel, np.float64, order="C", copy=True)
+    psi = np.array(psi, np.float64, order="C", copy=True)
+    n = pos.shape[0]
+    fate = np.zeros(n, np.int32)
+    cell = np.zeros(n, np.int32)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    load().oracle_step_atoms_d(C.byref(run), C.byref(cloud), dp(pos), dp(vel), dp(psi), float(cut_v2), ip(fate),
+                               ip(cell), n)
+    return pos, vel, psi, fate, cell
+
+
+def collide_cell(run: RunParams, cloud: CloudParams, vel, sigvrmax: float, local_cell: int, step: int):
+    """The NTC collisions of one grid cell in FP64: vel (n, 3) of the cell's atoms in sorted order.
+    Returns (vel, sigvrmax, candidates, pairs (k, 2), directions (k, 3)) after the cell's candidates."""
+    vel = np.asarray(vel, np.float64)
+    n = vel.shape[0]
+    v4 = np.zeros((n, 4), np.float64)
+    v4[:, :3] = vel
+    sv = C.c_double(float(sigvrmax))
+    cand = C.c_int32(0)
+    cap = 4096
+    ij = np.zeros((cap, 2), np.int32)
+    nv = np.zeros((cap, 3), np.float64)
+    acc = load().oracle_collide_cell_d(C.byref(run), C.byref(cloud), v4.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                       C.byref(sv), int(local_cell), int(step), C.byref(cand),
+                                       ij.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       nv.ctypes.data_as(C.POINTER(C.c_double)), cap)
+    k = min(acc, cap)
+    return v4[:, :3].copy(), sv.value, cand.value, ij[:k].copy(), nv[:k].copy()
 
 
 def smooth_loss(run, cloud, theta, width_kT, x, v, steps, log_off, log_ij, log_n, grad=False, fp64=True):

@@ -543,6 +543,64 @@ OAPI int oracle_advance_atoms_d(const dsmc_params* run, const dsmc_cloud_params*
     return 0;
 }
 
+// one timestep of n atoms (Larmor, Verlet, Majorana and knife tests, new cell; no collisions, no
+// sort) in FP64 with the knife cut cut_v2 in units of v^2 (2 eta kB T / m): for the restatement of
+// the step in the tests.  fate[i] 0 alive, 1 Majorana, 2 knife; cell[i] the atom's new cell.
+OAPI int oracle_step_atoms_d(const dsmc_params* run, const dsmc_cloud_params* c, double* pos, double* vel,
+                             double* psi, double cut_v2, int32_t* fate, int32_t* cell, int64_t n) {
+    CloudPhys<double> P;
+    make_cloud_phys<double>(*run, *c, 0, 0, P);
+    for (int64_t i = 0; i < n; ++i) {
+        Atom<double> a;
+        a.x = pos[4 * i]; a.y = pos[4 * i + 1]; a.z = pos[4 * i + 2];
+        a.vx = vel[4 * i]; a.vy = vel[4 * i + 1]; a.vz = vel[4 * i + 2];
+        a.ur = psi[4 * i]; a.ui = psi[4 * i + 1]; a.dr = psi[4 * i + 2]; a.di = psi[4 * i + 3];
+        a.flags = lane_to_u32(vel[4 * i + 3]);
+        AtomOut<double> o;
+        StepCtx sc = {};
+        advance_atom(P, cut_v2, a, o, sc);
+        pos[4 * i] = a.x; pos[4 * i + 1] = a.y; pos[4 * i + 2] = a.z;
+        vel[4 * i] = a.vx; vel[4 * i + 1] = a.vy; vel[4 * i + 2] = a.vz;
+        psi[4 * i] = a.ur; psi[4 * i + 1] = a.ui; psi[4 * i + 2] = a.dr; psi[4 * i + 3] = a.di;
+        fate[i] = o.fate;
+        cell[i] = o.cell;
+    }
+    return 0;
+}
+
+namespace {
+// records the accepted collisions of one cell: pair (i, j) and direction n^
+struct ArrayCollisionLog {
+    int32_t* ij;
+    double* nv;
+    int cap;
+    int count;
+    template <class R> void accept(uint32_t i, uint32_t j, R nx, R ny, R nz) {
+        if (count < cap) {
+            ij[2 * count] = (int32_t)i; ij[2 * count + 1] = (int32_t)j;
+            nv[3 * count] = (double)nx; nv[3 * count + 1] = (double)ny; nv[3 * count + 2] = (double)nz;
+        }
+        ++count;
+    }
+};
+}  // namespace
+
+// the NTC collisions of one grid cell of n atoms in FP64 (vel: n x 4, updated in place; sigvrmax
+// in/out), the cell's local index and the step keying its random numbers; the accepted pairs and
+// their scattering directions go to ij / nv (up to log_cap).  Returns the accepted count.
+OAPI int oracle_collide_cell_d(const dsmc_params* run, const dsmc_cloud_params* c, double* vel, int32_t n,
+                               double* sigvrmax, uint32_t local_cell, uint32_t step, int32_t* candidates,
+                               int32_t* ij, double* nv, int32_t log_cap) {
+    CloudPhys<double> P;
+    make_cloud_phys<double>(*run, *c, 0, 0, P);
+    ArrayCollisionLog lg{ij, nv, log_cap, 0};
+    Q4<double>* v = reinterpret_cast<Q4<double>*>(vel);
+    const CollideResult<double> r =
+        collide_cell<double, Q4<double>, ArrayCollisionLog>(v, n, *sigvrmax, P, local_cell, step, run->seed, &lg);
+    *candidates = r.candidates;
+    return r.accepted;
+}
+
 // MCWF period end (flip + decoherence + renormalisation) of each atom at its position, in FP64:
 // x0 = the trapped population recorded at the period start; flags bit 0 = anti-trapped on input
 // and output; ids and step key the flip's random number.

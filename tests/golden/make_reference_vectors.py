@@ -7,11 +7,14 @@ B' = 20 T/m, B'' = 4e4 T/m^2, include/deviceSystemParameters.cuh:25-27; moment
 g_s muB / 2 with g_s = 0.5, moveAtoms.cu:102; dt = 1e-7 s, wavefunction.cu:45), the state
 after 1 and after 200 iterations of evolveWavefunction + moveAtoms (main.cu:465-476).
 
-    python tests/golden/make_reference_vectors.py
+    python tests/golden/make_reference_vectors.py /root/reference/CUDADSMC
+
+The argument is the CUDADSMC project tree (read only; nothing is written there).
 """
 import ctypes as C
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -22,13 +25,13 @@ REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 MUB, M_RB, KB = 9.27400915e-24, 1.443160648e-25, 1.3806503e-23
 
 
-def build():
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref_host"), "CXX=/usr/bin/g++"], check=True,
-                   capture_output=True)
+def build(ref_tree):
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref_host"), "CXX=/usr/bin/g++", f"REF={ref_tree}"],
+                   check=True, capture_output=True)
 
 
-def main(n=256, steps=(1, 200), seed=2024):
-    build()
+def main(ref_tree, n=256, steps=(1, 200), seed=2024):
+    build(ref_tree)
     mv = C.CDLL(os.path.join(REF_DIR, "libref_move.so"))
     wv = C.CDLL(os.path.join(REF_DIR, "libref_wave.so"))
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
@@ -63,4 +66,6 @@ def main(n=256, steps=(1, 200), seed=2024):
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

@@ -27,7 +27,28 @@ def test_reference_arm_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"] and cb["value"] == d["value"]
-    assert d["config"]["workload"] and d["config"]["atoms"] == 20000
+    assert d["config"]["workload"] and d["config"]["atoms_per_gpu"] == 20000
+
+
+def test_reference_arm_prints_the_same_config_as_the_gpu_arm():
+    sys.path.insert(0, ROOT)
+    import bench
+    res = run_bench({})
+    d = json.loads([x for x in res.stdout.splitlines() if x.startswith("{")][0])
+
+    class A:
+        atoms = 20000
+    assert d["config"] == bench.config_of(A, 1)
+
+
+def test_reference_arm_never_maps_the_engine_library():
+    # the reference arm runs the CPU restatement only: the engine's shared library must not be loaded
+    code = ("import sys, bench; sys.argv = ['bench.py', '--impl', 'reference', '--atoms', '5000', '--steps', '1', "
+            "'--warmup', '0']; bench.main(); maps = open('/proc/self/maps').read(); "
+            "print('ENGINE_MAPPED' if 'libdsmc_b200' in maps else 'ENGINE_NOT_MAPPED')")
+    res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert res.returncode == 0, res.stderr
+    assert "ENGINE_NOT_MAPPED" in res.stdout
 
 
 def test_reference_arm_other_ranks_print_nothing():
