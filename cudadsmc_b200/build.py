@@ -27,7 +27,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "build", "liboracle.so")
 
 ENGINE_SOURCES = ["dsmc_engine.cu", "dsmc_noalloc.cu"]
-ENGINE_HEADERS = ["dsmc_kernels.cuh", "dsmc_physics.h", "dsmc_setup.h"]
+ENGINE_HEADERS = ["dsmc_kernels.cuh", "dsmc_physics.h", "dsmc_radix.cuh", "dsmc_setup.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

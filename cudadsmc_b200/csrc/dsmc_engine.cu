@@ -238,7 +238,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(Ic.p, 0, total_cells * sizeof(int)));
         in_list.alloc(capacity);
         mrec.alloc(capacity);
-        keys.alloc(capacity);
+        keys.alloc(std::max(capacity, 2048));  // >= 4096 ints: the full sort's count table
         tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles); ovf_list.alloc(max_tiles);
         sigvrmax.alloc(total_cells);
         accum.alloc((size_t)nclouds * ACC_BUCKETS);
@@ -428,16 +428,20 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         for (int k = 0; k < nclouds; ++k) { off[k] = n; n += counts[k]; }
         off[nclouds] = n;
         CU(cudaMemcpyAsync(sort_off.p, off.data(), (nclouds + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
-        const int nn = std::max(n, 1);
-        const int gblocks = (nn + SCAN_CHUNK - 1) / SCAN_CHUNK;
-        // the sort's per-atom scratch lives in the step's sort keys and mover records (2 and 4 ints
-        // per atom of capacity), which no sort kernel reads and no step keeps across this call
-        // (n <= capacity, gblocks <= n): no allocation here.  in_list is the sort's own.
-        int* const ticket = reinterpret_cast<int*>(keys.p);
-        int* const oflag = reinterpret_cast<int*>(keys.p) + capacity;
-        int* const orank = reinterpret_cast<int*>(mrec.p);
-        int* const gb = reinterpret_cast<int*>(mrec.p) + capacity;
-        int* const cell = reinterpret_cast<int*>(mrec.p) + 2 * (size_t)capacity;
+        // the sort's scratch lives in the step's sort keys and mover records (2 and 4 ints per atom
+        // of capacity; the keys hold at least 4096 ints), which no sort kernel reads and no step
+        // keeps across this call, and the incoming-mover list: no allocation here.
+        //   mover records: cell ids | radix keys | radix values (two ping-pong pairs)
+        //   sort keys: the digit count table of a pass and its scan's block sums
+        //   in_list: the sorted order (source index of each sorted position)
+        int* const mr = reinterpret_cast<int*>(mrec.p);
+        int* const cell = mr + 2 * (size_t)capacity;
+        int* const rkey[2] = {cell, mr};
+        int* const rval[2] = {mr + 3 * (size_t)capacity, mr + (size_t)capacity};
+        int* const table = reinterpret_cast<int*>(keys.p);
+        const int64_t tsize = radix_table(n);
+        int* const gb = table + tsize;
+        const int tblocks = (int)((tsize + SCAN_CHUNK - 1) / SCAN_CHUNK);
         // reset bookkeeping: parity 1 is "current" with zero atoms, old starts all zero
         CU(cudaMemsetAsync(ctl.p, 0, sizeof(Ctl), stream));
         CU(cudaMemsetAsync(start[1].p, 0, (total_cells + 1) * sizeof(int), stream));
@@ -451,21 +455,28 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         S.pos_src = ps; S.vel_src = vs; S.psi_src = ss;
         S.pos_dst = pos[0].p; S.vel_dst = vel[0].p; S.psi_dst = psi[0].p;
         S.cloud_atom_off = sort_off.p;
-        S.cell = cell; S.ticket = ticket; S.ovf_flag = oflag; S.ovf_rank = orank;
+        S.cell = cell; S.order = in_list.p;
         S.n = n; S.nclouds = nclouds;
         const int ab = (n + 255) / 256;
         if (n > 0) fs_cells<R><<<ab, 256, 0, stream>>>(S, A);
-        if (n > 0) {
-            gscan_reduce<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag, n, gb);
-            gscan_top<<<1, 1024, 0, stream>>>(gb, gblocks, nullptr);
-            gscan_down<<<gblocks, SCAN_BLOCK, 0, stream>>>(oflag, n, gb, orank);
-        }
         launch_scan(A, 0);
         if (cell_block == 512) init_tiles<R, 512><<<nscan_blocks, 512, 0, stream>>>(A);
         else init_tiles<R, 256><<<nscan_blocks, 256, 0, stream>>>(A);
         if (n > 0) {
-            fs_place<R><<<ab, 256, 0, stream>>>(S, A);
-            fs_scatter<R><<<ab, 256, 0, stream>>>(S, A);
+            // stable by (cell, source index): LSD passes over the digits of the cell ids
+            const int nch = radix_chunks(n), passes = radix_passes(total_cells);
+            for (int q = 0; q < passes; ++q) {
+                const bool last = q + 1 == passes;
+                radix_hist<<<nch, RADIX_BLOCK, 0, stream>>>(rkey[q & 1], n, RADIX_BITS * q, table, nch);
+                gscan_reduce<<<tblocks, SCAN_BLOCK, 0, stream>>>(table, (int)tsize, gb);
+                gscan_top<<<1, 1024, 0, stream>>>(gb, tblocks, nullptr);
+                gscan_down<<<tblocks, SCAN_BLOCK, 0, stream>>>(table, (int)tsize, gb, table);
+                radix_scatter<<<nch, RADIX_BLOCK, 0, stream>>>(rkey[q & 1], q == 0 ? nullptr : rval[q & 1], n,
+                                                               RADIX_BITS * q, table, nch,
+                                                               last ? nullptr : rkey[(q + 1) & 1],
+                                                               last ? in_list.p : rval[(q + 1) & 1]);
+            }
+            fs_gather<R><<<ab, 256, 0, stream>>>(S);
             fill_identity<<<ab, 256, 0, stream>>>(src[0].p, n);
         }
         CU(cudaGetLastError());

@@ -33,6 +33,7 @@
 
 #include <cuda_runtime.h>
 #include "dsmc_physics.h"
+#include "dsmc_radix.cuh"
 
 namespace dsmc {
 
@@ -1440,7 +1441,10 @@ __global__ void __launch_bounds__(BLOCK) measure_tiles(Args<R> A) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// full sort (initialisation and set_state): arbitrary order -> stable by (cell, index)
+// full sort (initialisation and set_state): arbitrary order -> stable by (cell, index).
+// fs_cells finds every atom's global cell and counts the cells (the cell scan turns the counts
+// into the sorted starts); the stable radix sort of the cell ids (dsmc_radix.cuh) gives, for
+// every sorted position j, the source index order[j]; fs_gather copies the state there.
 // ---------------------------------------------------------------------------------------------
 template <class R> struct SortArgs {
     typedef typename V4T<R>::type R4;
@@ -1451,10 +1455,8 @@ template <class R> struct SortArgs {
     R4* vel_dst;
     R4* psi_dst;
     const int* cloud_atom_off;  // nclouds + 1, atoms of the source grouped by cloud
-    int* cell;
-    int* ticket;
-    int* ovf_flag;
-    int* ovf_rank;
+    int* cell;                  // global cell of each source atom
+    const int* order;           // sorted position -> source index (after the radix sort)
     int n, nclouds;
 };
 
@@ -1477,37 +1479,17 @@ __global__ void __launch_bounds__(256) fs_cells(SortArgs<R> S, Args<R> A) {
     const auto q = S.pos_src[i];
     const int c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);
     S.cell[i] = c;
-    S.ovf_flag[i] = (c == P.ovf_cell) ? 1 : 0;
-    S.ticket[i] = atomicAdd(&A.Ic[c], 1);
+    atomicAdd(&A.Ic[c], 1);
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) fs_place(SortArgs<R> S, Args<R> A) {
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= S.n) return;
-    if (S.ovf_flag[i]) return;
-    const int c = S.cell[i];
-    A.in_list[A.mover_base[c] + S.ticket[i]] = i;
-}
-
-template <class R>
-__global__ void __launch_bounds__(256) fs_scatter(SortArgs<R> S, Args<R> A) {
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= S.n) return;
-    const int c = S.cell[i];
-    int dest;
-    if (S.ovf_flag[i]) {
-        const int k = find_cloud<R>(S.cloud_atom_off, S.nclouds, i);
-        dest = A.new_start[c] + (S.ovf_rank[i] - S.ovf_rank[S.cloud_atom_off[k]]);
-    } else {
-        const int lo = A.new_start[c], hi = A.new_start[c + 1];
-        int rank = 0;
-        for (int j = lo; j < hi; ++j) rank += (A.in_list[j] < i) ? 1 : 0;
-        dest = lo + rank;
-    }
-    S.pos_dst[dest] = S.pos_src[i];
-    S.vel_dst[dest] = S.vel_src[i];
-    S.psi_dst[dest] = S.psi_src[i];
+__global__ void __launch_bounds__(256) fs_gather(SortArgs<R> S) {
+    const int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= S.n) return;
+    const int i = S.order[j];
+    S.pos_dst[j] = S.pos_src[i];
+    S.vel_dst[j] = S.vel_src[i];
+    S.psi_dst[j] = S.psi_src[i];
 }
 
 // generic exclusive scan of n ints (3 kernels, no inter-block waiting)

@@ -5,13 +5,14 @@
 // it can fail for lack of free memory the pool is holding, and cudaMalloc / cudaFree
 // synchronise the device, stalling every other stream of the application.  For them this
 // entry point sorts one cloud's atoms by cell using only a fixed scratch region compiled into
-// the library (g_noalloc_scratch below, about 6.3 MB, held by every GPU that loads the library
+// the library (g_noalloc_scratch below, about 5.3 MB, held by every GPU that loads the library
 // until the process exits).  The caller passes device pointers for the input positions and for
 // both outputs; nothing is allocated or freed.
 //
 // The order it produces is the engine's full-sort order: stable by (cell, input index), where
 // the cell id and the overflow cell are those of the engine (grid cells z*nx*ny + y*nx + x, then
-// the overflow cell for atoms outside the grid).
+// the overflow cell for atoms outside the grid).  It is the engine's stable radix sort of the
+// cell ids (dsmc_radix.cuh), so its time grows with the atoms, whatever the cells hold.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -20,6 +21,7 @@
 
 #include "dsmc.h"
 #include "dsmc_physics.h"
+#include "dsmc_radix.cuh"
 #include "dsmc_setup.h"
 
 namespace {
@@ -31,25 +33,49 @@ constexpr int kMaxCells = (1 << 18) + 1;    // grid cells + overflow cell per ca
 constexpr int kBlock = 256;
 constexpr int kItems = 8;
 constexpr int kChunk = kBlock * kItems;     // elements per scan block
-constexpr int kMaxScanBlocks = (kMaxCells + kChunk - 1) / kChunk + 1;
+constexpr int kMaxTable = RADIX_DIGITS * ((kMaxAtoms + RADIX_CHUNK - 1) / RADIX_CHUNK);  // digit counts of a pass
+constexpr int kMaxScanLen = kMaxCells > kMaxTable ? kMaxCells : kMaxTable;
+constexpr int kMaxScanBlocks = (kMaxScanLen + kChunk - 1) / kChunk + 1;
 
-// layout of the scratch (ints): per-cell counters, then per-atom cell / ticket / overflow
-// flag / overflow rank / incoming list, then scan block sums
+// layout of the scratch (ints): per-cell counters, the radix keys and values (two ping-pong
+// pairs; the first keys are the atoms' cells), the digit count table, then scan block sums
 constexpr int kOffCounts = 0;
-constexpr int kOffCell = kOffCounts + kMaxCells + 1;
-constexpr int kOffTicket = kOffCell + kMaxAtoms;
-constexpr int kOffOvf = kOffTicket + kMaxAtoms;
-constexpr int kOffOvfRank = kOffOvf + kMaxAtoms;
-constexpr int kOffList = kOffOvfRank + kMaxAtoms;
-constexpr int kOffBlocks = kOffList + kMaxAtoms;
+constexpr int kOffKeyA = kOffCounts + kMaxCells + 1;
+constexpr int kOffKeyB = kOffKeyA + kMaxAtoms;
+constexpr int kOffValA = kOffKeyB + kMaxAtoms;
+constexpr int kOffValB = kOffValA + kMaxAtoms;
+constexpr int kOffTable = kOffValB + kMaxAtoms;
+constexpr int kOffBlocks = kOffTable + kMaxTable;
 constexpr int kScratchInts = kOffBlocks + kMaxScanBlocks + 1;
 
 static __device__ __align__(256) int g_noalloc_scratch[kScratchInts];
 
-// device address of the scratch, looked up once per device with that device current
+// Device address of the scratch, looked up once per device with that device current, and again
+// when the device's current context is no longer the one of the lookup (after a
+// cudaDeviceReset the module is loaded anew and the array may sit elsewhere).
 constexpr int kMaxDevices = 64;
-int* g_scratch_addr[kMaxDevices] = {};
+struct ScratchAddr {
+    int* addr;
+    void* ctx;
+};
+ScratchAddr g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
+
+// the driver's cuCtxGetCurrent through the runtime (no link against the driver library)
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+        looked = true;
+    }
+    return fn;
+}
 
 cudaError_t scratch_for_current_device(int** out) {
     int dev = 0;
@@ -57,13 +83,21 @@ cudaError_t scratch_for_current_device(int** out) {
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    // the current context (null until the runtime has made the device's context current, which
+    // the symbol lookup does)
+    CtxGetCurrentFn get = ctx_get_current();
+    void* ctx = nullptr;
+    if (get && get(&ctx) != 0) ctx = nullptr;
+    ScratchAddr& s = g_scratch_addr[dev];
+    if (!s.addr || !ctx || s.ctx != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = static_cast<int*>(p);
+        if (get && get(&ctx) != 0) ctx = nullptr;
+        s.addr = static_cast<int*>(p);
+        s.ctx = ctx;
     }
-    *out = g_scratch_addr[dev];
+    *out = s.addr;
     return cudaSuccess;
 }
 
@@ -106,9 +140,8 @@ __global__ void k_cells(const R4* pos, int n, CloudPhys<R> P, int* scratch) {
     if (i >= n) return;
     const R4 q = pos[i];
     const int c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);  // ids start at 0 (cell_base 0)
-    scratch[kOffCell + i] = c;
-    scratch[kOffOvf + i] = (c == P.ovf_cell) ? 1 : 0;
-    scratch[kOffTicket + i] = atomicAdd(&scratch[kOffCounts + c], 1);
+    scratch[kOffKeyA + i] = c;
+    atomicAdd(&scratch[kOffCounts + c], 1);
 }
 
 // exclusive scan of in[0..n) into out[0..n) (3 kernels, block sums in the scratch)
@@ -159,29 +192,6 @@ __global__ void k_scan_down(const int* in, int n, const int* boff, int* out) {
     }
 }
 
-__global__ void k_place(int n, const int* start, int* scratch) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n || scratch[kOffOvf + i]) return;
-    const int c = scratch[kOffCell + i];
-    scratch[kOffList + start[c] + scratch[kOffTicket + i]] = i;
-}
-
-__global__ void k_scatter(int n, const int* start, const int* scratch, int* order) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n) return;
-    const int c = scratch[kOffCell + i];
-    int dest;
-    if (scratch[kOffOvf + i]) {
-        dest = start[c] + scratch[kOffOvfRank + i];
-    } else {
-        const int lo = start[c], hi = start[c + 1];
-        int rank = 0;
-        for (int j = lo; j < hi; ++j) rank += (scratch[kOffList + j] < i) ? 1 : 0;
-        dest = lo + rank;
-    }
-    order[dest] = i;
-}
-
 void scan(const int* in, int n, int* out, int* bsum, int* total, cudaStream_t s) {
     const int nb = (n + kChunk - 1) / kChunk;
     k_scan_reduce<<<nb, kBlock, 0, s>>>(in, n, bsum);
@@ -203,9 +213,21 @@ dsmc_status sort_cells(const dsmc_params& rp, const dsmc_cloud_params& cp, const
     // cell starts (the caller's output) and the total in cell_start[ncells]
     scan(scratch + kOffCounts, ncells, cell_start, scratch + kOffBlocks, cell_start + ncells, s);
     if (n > 0) {
-        scan(scratch + kOffOvf, n, scratch + kOffOvfRank, scratch + kOffBlocks, nullptr, s);
-        k_place<<<ab, kBlock, 0, s>>>(n, cell_start, scratch);
-        k_scatter<<<ab, kBlock, 0, s>>>(n, cell_start, scratch, order);
+        // stable by (cell, input index): LSD passes over the digits of the cell ids, the last one
+        // writing the caller's order
+        int* const key[2] = {scratch + kOffKeyA, scratch + kOffKeyB};
+        int* const val[2] = {scratch + kOffValA, scratch + kOffValB};
+        int* const table = scratch + kOffTable;
+        const int nch = radix_chunks(n), passes = radix_passes(ncells);
+        const int tsize = (int)radix_table(n);
+        for (int q = 0; q < passes; ++q) {
+            const bool last = q + 1 == passes;
+            radix_hist<<<nch, RADIX_BLOCK, 0, s>>>(key[q & 1], n, RADIX_BITS * q, table, nch);
+            scan(table, tsize, table, scratch + kOffBlocks, nullptr, s);
+            radix_scatter<<<nch, RADIX_BLOCK, 0, s>>>(key[q & 1], q == 0 ? nullptr : val[q & 1], n, RADIX_BITS * q,
+                                                      table, nch, last ? nullptr : key[(q + 1) & 1],
+                                                      last ? order : val[(q + 1) & 1]);
+        }
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DSMC_OK : DSMC_ERR_CUDA;
@@ -221,6 +243,11 @@ DSMC_API dsmc_status dsmc_sort_cells_noalloc(const dsmc_params* run, const dsmc_
     if (n > kMaxAtoms) return DSMC_ERR_CAPACITY;
     if (cloud_cells(*cloud) > kMaxCells) return DSMC_ERR_CAPACITY;
     if (run->precision != DSMC_FP32 && run->precision != DSMC_FP64) return DSMC_ERR_INVALID;
+    // the positions are read as 16-byte (float4) or 32-byte (double4) vectors
+    const uintptr_t align = run->precision == DSMC_FP32 ? 16u : 32u;
+    if (n > 0 && ((uintptr_t)pos_dev % align) != 0) return DSMC_ERR_INVALID;
+    // an error left pending on this thread by earlier work is the caller's: report it untouched
+    if (cudaPeekAtLastError() != cudaSuccess) return DSMC_ERR_STATE;
     int* scratch = nullptr;
     if (scratch_for_current_device(&scratch) != cudaSuccess) return DSMC_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);

@@ -273,9 +273,14 @@ DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, 
  * DSMC_FP64; x, y, z used), order_dev receives n indices (order_dev[j] = input index of the atom
  * in sorted position j, stable by (cell, input index)), cell_start_dev receives
  * cells[0]*cells[1]*cells[2] + 2 ints (start of every grid cell, then of the overflow cell, then n).
- * Work is enqueued on cuda_stream.  Scratch lives in a fixed device array of about 6.3 MB inside
- * the library: at most 262144 atoms and 262144 grid cells per call (DSMC_ERR_CAPACITY beyond).
- * The first call on a device looks up that array's address (make it before any stream capture);
+ * pos_dev must be 16-byte aligned for DSMC_FP32 and 32-byte aligned for DSMC_FP64 (the positions
+ * are read as vectors; DSMC_ERR_INVALID otherwise).  Work is enqueued on cuda_stream.  If a CUDA
+ * error is already pending on the calling thread the call launches nothing and returns
+ * DSMC_ERR_STATE, leaving that error for its owner.  Scratch lives in a fixed device array of
+ * about 5.3 MB inside the library: at most 262144 atoms and 262144 grid cells per call
+ * (DSMC_ERR_CAPACITY beyond).  The sort is a stable radix sort of the cell ids, so its time
+ * follows the atom count whatever the cells hold.  The first call on a device (and the first
+ * after a cudaDeviceReset) looks up that array's address (make it before any stream capture);
  * every call shares the array, so calls that overlap on the GPU race and must be serialised. */
 DSMC_API dsmc_status dsmc_sort_cells_noalloc(const dsmc_params* run, const dsmc_cloud_params* cloud,
                                              const void* pos_dev, int64_t n, int32_t* order_dev,
