@@ -114,6 +114,7 @@ class AdjParams(C.Structure):
         ("precision", C.c_int32),
         ("reserved0", C.c_int32),
         ("sigmoid_width_kT", C.c_double),
+        ("majorana_width", C.c_double),
     ]
 
 
@@ -129,9 +130,13 @@ class Grad(C.Structure):
         ("ms_record", C.c_double),
         ("ms_forward", C.c_double),
         ("ms_backward", C.c_double),
+        ("dE_dtheta", C.c_double * 11),
+        ("dN_dtheta", C.c_double * 11),
     ]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}
         d["dL_deta"] = list(self.dL_deta)
+        d["dE_dtheta"] = list(self.dE_dtheta)
+        d["dN_dtheta"] = list(self.dN_dtheta)
         return d

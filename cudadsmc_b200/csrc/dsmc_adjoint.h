@@ -1,23 +1,33 @@
 // dsmc_adjoint.h -- the smoothed timestep used for gradients and its hand-written adjoint.
 //
-// Gradient model.  The physical run (engine, hard energy knife) fixes every random choice: the
-// collision events of each step (pair of atoms by id, scattering direction n^) are recorded and
-// replayed.  In the smoothed model no atom is removed: each atom carries a survival weight w,
-// multiplied every step by s = sigmoid((cut - e) / width), where e = v^2 + kappa (|B| - B_floor)
-// is the knife energy in units of m/2, cut = 2 eta(step) kB T0 / m and width = 2 (width_kT) kB T0 / m.
-// One step of one atom (after the recorded collisions of the step are applied):
+// Gradient model.  The physical run (engine, hard Majorana and energy cuts) fixes every random
+// choice: the collision events of each step (pair of atoms by id, scattering direction n^) are
+// recorded and replayed.  In the smoothed model no atom is removed: each atom carries a survival
+// weight w, multiplied every step by the knife's s_K = sigmoid((cut - e) / width) -- e = v^2 +
+// kappa (|B| - B_floor) the knife energy in units of m/2, cut = 2 eta(step) kB T0 / m, width =
+// 2 (width_kT) kB T0 / m -- and, when the run has Majorana loss, by s_M = sigmoid(<s.B^> / width_M)
+// in place of the hard test <s.B^> < 0 (evaporation.cu:86-95).  One step of one atom (after the
+// recorded collisions of the step are applied), in the order of the engine's step:
+//     psi1 = [cos t - i sin t (s.B^(x))] psi,  t = (mu dt / hbar) |B(x)|   (wavefunction.cu:39-73)
 //     v1 = v + dt/2 a(x),  x1 = x + dt v1,  v2 = v1 + dt/2 a(x1),  a = -(mu/m) grad|B|
-//     e = |v2|^2 + kappa (|B(x1)| - B_floor),  w' = w sigmoid((cut - e)/width)
-// Loss after the last step: L = (m/2) (sum w e / sum w) / (kB T0) + sum w / N0
-// (final mean energy per retained atom in units of kB T0, plus the retained fraction).
+//     e = |v2|^2 + kappa (|B(x1)| - B_floor),  w' = w s_K(e) s_M(<s.B^(x1)>_psi1)
+// (the rotation is unitary, so the engine's renormalisation, which only removes rounding, is left
+// out).  Loss after the last step: L = L_E + L_N with L_E = (m/2) (sum w e / sum w) / (kB T0) (the
+// final mean energy per retained atom in units of kB T0) and L_N = sum w / N0 (the retained
+// fraction); the adjoint carries both seeds at once and returns dL_E/dtheta and dL_N/dtheta.
 // Parameters: B' (gradient), B0 (bias along z) of the linear trap B = (B'x/2, B'y/2, B0 - B'z),
 // and the knot heights eta_k of the knife ramp.
 //
 // The adjoint is written out by hand: for the field of the linear trap, with J = diag(h, h, -B'),
 // h = B'/2, b = B^/|B| the unit field:  grad|B| = J b,  Hessian H = J (I - b b^T) J / |B|,
-// d|B|/dB' = b . (x/2, y/2, -z),  d|B|/dB0 = b_z,  d(grad|B|)/dtheta = dJ/dtheta b + J (I - b b^T) dB/dtheta / |B|.
-// A collision with fixed n^ maps (vi, vj) to (c + r n^/2, c - r n^/2), c = (vi + vj)/2, r = |vi - vj|;
-// its adjoint is  vi_bar = c_bar/2 + r_bar u/r,  vj_bar = c_bar/2 - r_bar u/r,  with
+// d|B|/dB' = b . (x/2, y/2, -z),  d|B|/dB0 = b_z,  d(grad|B|)/dtheta = dJ/dtheta b + J (I - b b^T) dB/dtheta / |B|;
+// an adjoint (b_bar, |B|_bar) of the unit field and the magnitude pulls back to the field vector as
+// B_bar = (I - b b^T) b_bar / |B| + b |B|_bar, then to x (J B_bar), B' ((x/2, y/2, -z) . B_bar) and
+// B0 (B_bar_z).  The rotation psi1 = c psi + s T(b) psi (T linear in b and in psi) has the adjoint
+// psi_bar = c psi1_bar + s T(b)^T psi1_bar, t_bar = -s (psi1_bar . psi) + c (psi1_bar . T(b) psi),
+// b_bar_k = s psi1_bar . T(e_k) psi.  A collision with fixed n^ maps (vi, vj) to
+// (c + r n^/2, c - r n^/2), c = (vi + vj)/2, r = |vi - vj|; its adjoint is
+// vi_bar = c_bar/2 + r_bar u/r,  vj_bar = c_bar/2 - r_bar u/r,  with
 // c_bar = vi'_bar + vj'_bar, r_bar = n^ . (vi'_bar - vj'_bar)/2, u = vi - vj.
 #ifndef DSMC_ADJOINT_H
 #define DSMC_ADJOINT_H
@@ -29,10 +39,15 @@ namespace dsmc {
 // number of differentiable parameters: B', B0, then the knife knots
 constexpr int ADJ_NPARAM = 2 + 9;
 
+// adjoint seeds carried together: 0 = the mean energy term L_E, 1 = the retained fraction L_N
+constexpr int ADJ_SEEDS = 2;
+
 template <class R> struct SmoothConsts {
     R Bp, B0, B_floor;
     R dt, half_dt, accel_scale, kappa;  // accel_scale = mu / m
     R inv_width;                        // 1 / width (v^2 units)
+    R theta_per_B;                      // Larmor angle per tesla, mu dt / hbar (0: no precession)
+    R inv_width_maj;                    // 1 / width of the Majorana sigmoid in <s.B^> (0: no Majorana weight)
     double cut_scale;                   // d cut / d eta = 2 kB T0 / m
 };
 
@@ -83,30 +98,79 @@ DSMC_HD void quad_field(R Bp, R B0, R x, R y, R z, bool derivs, QuadField<R>& f)
 
 template <class R> DSMC_HD R sigmoid(R z) { return R(1) / (R(1) + xexp(-z)); }
 
+// psi1 = c psi + s T(b) psi: the Larmor rotation of the spinor p = (Re u, Im u, Re d, Im d) by the
+// angle with cos c, sin s about the unit field b (the rows of wavefunction.cu:51-70)
+template <class R> DSMC_HD void larmor_apply(R c, R s, const R* b, const R* p, R* q) {
+    q[0] = p[0] * c + (b[0] * p[3] - b[1] * p[2] + b[2] * p[1]) * s;
+    q[1] = p[1] * c + (-b[0] * p[2] - b[1] * p[3] - b[2] * p[0]) * s;
+    q[2] = p[2] * c + (b[0] * p[1] + b[1] * p[0] - b[2] * p[3]) * s;
+    q[3] = p[3] * c + (-b[0] * p[0] + b[1] * p[1] + b[2] * p[2]) * s;
+}
+// <s.B^> = 2 bx Re(u* d) + 2 by Im(u* d) + bz (|u|^2 - |d|^2)   (evaporation.cu:88-90)
+template <class R> DSMC_HD R spin_projection(const R* b, const R* p) {
+    const R re = p[0] * p[2] + p[1] * p[3];
+    const R im = p[0] * p[3] - p[1] * p[2];
+    const R dz = p[0] * p[0] + p[1] * p[1] - p[2] * p[2] - p[3] * p[3];
+    return R(2) * (b[0] * re + b[1] * im) + b[2] * dz;
+}
+
 // one smoothed step of one atom (collisions already applied to v); returns e
 template <class R>
-DSMC_HD R smooth_step(const SmoothConsts<R>& C, R cut, R* x, R* v, R& w) {
+DSMC_HD R smooth_step(const SmoothConsts<R>& C, R cut, R* x, R* v, R* psi, R& w) {
     QuadField<R> f0, f1;
     quad_field(C.Bp, C.B0, x[0], x[1], x[2], false, f0);
+    if (C.theta_per_B != R(0)) {
+        R s, c;
+        xsincos(C.theta_per_B * f0.absB, &s, &c);
+        R q[4];
+        larmor_apply(c, s, f0.b, psi, q);
+        for (int k = 0; k < 4; ++k) psi[k] = q[k];
+    }
     const R as = -C.accel_scale;
     for (int i = 0; i < 3; ++i) v[i] = v[i] + C.half_dt * (as * f0.g[i]);
     for (int i = 0; i < 3; ++i) x[i] = x[i] + C.dt * v[i];
     quad_field(C.Bp, C.B0, x[0], x[1], x[2], false, f1);
     for (int i = 0; i < 3; ++i) v[i] = v[i] + C.half_dt * (as * f1.g[i]);
     const R e = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + C.kappa * (f1.absB - C.B_floor);
-    w = w * sigmoid((cut - e) * C.inv_width);
+    R sw = sigmoid((cut - e) * C.inv_width);
+    if (C.inv_width_maj != R(0)) sw = sw * sigmoid(spin_projection(f1.b, psi) * C.inv_width_maj);
+    w = w * sw;
     return e;
 }
 
-// Adjoint of smooth_step.  In: the state (x, v, w) the step started from (v after collisions),
-// the adjoints xb, vb, wb of its outputs.  Out: xb, vb, wb overwritten with the adjoints of the
-// inputs; theta_b[0..1] (B', B0) incremented; cut_b receives d/d cut.
+// adjoint of (b, |B|) at x through the field vector: accumulates into xb (3) and tb (B', B0)
 template <class R>
-DSMC_HD void smooth_step_adjoint(const SmoothConsts<R>& C, R cut, const R* x0, const R* v0, R w0, R* xb, R* vb,
-                                 R& wb, R* theta_b, R& cut_b) {
+DSMC_HD void field_vec_adjoint(R Bp, const R* x, const QuadField<R>& f, const R* bb, R absBb, R* xb, R* tb) {
+    const R inv = f.absB > R(0) ? R(1) / f.absB : R(0);
+    const R d = f.b[0] * bb[0] + f.b[1] * bb[1] + f.b[2] * bb[2];
+    R Bb[3];
+    for (int i = 0; i < 3; ++i) Bb[i] = (bb[i] - f.b[i] * d) * inv + f.b[i] * absBb;
+    const R h = R(0.5) * Bp;
+    xb[0] += h * Bb[0];
+    xb[1] += h * Bb[1];
+    xb[2] += -Bp * Bb[2];
+    tb[0] += R(0.5) * x[0] * Bb[0] + R(0.5) * x[1] * Bb[1] - x[2] * Bb[2];
+    tb[1] += Bb[2];
+}
+
+// Adjoint of smooth_step for ADJ_SEEDS seeds at once.  In: the state (x, v, psi, w) the step
+// started from (v after collisions), the adjoints xb, vb, pb, wb of its outputs (per seed).  Out:
+// xb, vb, pb, wb overwritten with the adjoints of the inputs; theta_b[seed][0..1] (B', B0)
+// incremented; cut_b[seed] receives d/d cut.
+template <class R>
+DSMC_HD void smooth_step_adjoint(const SmoothConsts<R>& C, R cut, const R* x0, const R* v0, const R* p0, R w0,
+                                 R (*xb)[3], R (*vb)[3], R (*pb)[4], R* wb, R (*theta_b)[2], R* cut_b) {
     // recompute the forward intermediates
     QuadField<R> f0, f1;
     quad_field(C.Bp, C.B0, x0[0], x0[1], x0[2], true, f0);
+    const bool larmor = C.theta_per_B != R(0);
+    R sn = R(0), cs = R(1), p1[4];
+    if (larmor) {
+        xsincos(C.theta_per_B * f0.absB, &sn, &cs);
+        larmor_apply(cs, sn, f0.b, p0, p1);
+    } else {
+        for (int k = 0; k < 4; ++k) p1[k] = p0[k];
+    }
     const R as = -C.accel_scale;
     R v1[3], x1[3], v2[3];
     for (int i = 0; i < 3; ++i) v1[i] = v0[i] + C.half_dt * (as * f0.g[i]);
@@ -114,38 +178,80 @@ DSMC_HD void smooth_step_adjoint(const SmoothConsts<R>& C, R cut, const R* x0, c
     quad_field(C.Bp, C.B0, x1[0], x1[1], x1[2], true, f1);
     for (int i = 0; i < 3; ++i) v2[i] = v1[i] + C.half_dt * (as * f1.g[i]);
     const R e = v2[0] * v2[0] + v2[1] * v2[1] + v2[2] * v2[2] + C.kappa * (f1.absB - C.B_floor);
-    const R s = sigmoid((cut - e) * C.inv_width);
-    // w' = w s
-    const R sb = wb * w0;
-    wb = wb * s;
-    const R zb = sb * s * (R(1) - s);
-    const R eb = -zb * C.inv_width;
-    cut_b = zb * C.inv_width;
-    // e = |v2|^2 + kappa (|B(x1)| - B_floor)
-    R v2b[3], x1b[3];
-    for (int i = 0; i < 3; ++i) {
-        v2b[i] = vb[i] + R(2) * eb * v2[i];
-        x1b[i] = xb[i] + eb * C.kappa * f1.g[i];
+    const R sK = sigmoid((cut - e) * C.inv_width);
+    const bool maj = C.inv_width_maj != R(0);
+    const R sM = maj ? sigmoid(spin_projection(f1.b, p1) * C.inv_width_maj) : R(1);
+    const R re = p1[0] * p1[2] + p1[1] * p1[3];
+    const R im = p1[0] * p1[3] - p1[1] * p1[2];
+    const R dz = p1[0] * p1[0] + p1[1] * p1[1] - p1[2] * p1[2] - p1[3] * p1[3];
+    for (int q = 0; q < ADJ_SEEDS; ++q) {
+        // w' = w sK sM
+        const R wo = wb[q];
+        wb[q] = wo * (sK * sM);
+        const R zKb = wo * w0 * sM * sK * (R(1) - sK);
+        const R eb = -zKb * C.inv_width;
+        cut_b[q] = zKb * C.inv_width;
+        // the Majorana weight: <s.B^> of psi1 at x1
+        R p1b[4] = {pb[q][0], pb[q][1], pb[q][2], pb[q][3]};
+        R b1b[3] = {R(0), R(0), R(0)};
+        if (maj) {
+            const R projb = wo * w0 * sK * sM * (R(1) - sM) * C.inv_width_maj;
+            b1b[0] = projb * (R(2) * re);
+            b1b[1] = projb * (R(2) * im);
+            b1b[2] = projb * dz;
+            const R reb = R(2) * f1.b[0] * projb, imb = R(2) * f1.b[1] * projb, dzb = f1.b[2] * projb;
+            p1b[0] += reb * p1[2] + imb * p1[3] + R(2) * dzb * p1[0];
+            p1b[1] += reb * p1[3] - imb * p1[2] + R(2) * dzb * p1[1];
+            p1b[2] += reb * p1[0] - imb * p1[1] - R(2) * dzb * p1[2];
+            p1b[3] += reb * p1[1] + imb * p1[0] - R(2) * dzb * p1[3];
+        }
+        // e = |v2|^2 + kappa (|B(x1)| - B_floor), and the unit field at x1
+        R v2b[3], x1b[3];
+        for (int i = 0; i < 3; ++i) {
+            v2b[i] = vb[q][i] + R(2) * eb * v2[i];
+            x1b[i] = xb[q][i];
+        }
+        field_vec_adjoint(C.Bp, x1, f1, b1b, eb * C.kappa, x1b, theta_b[q]);
+        // v2 = v1 + hdt as g(x1)
+        R g1b[3];
+        for (int i = 0; i < 3; ++i) g1b[i] = C.half_dt * as * v2b[i];
+        for (int i = 0; i < 3; ++i) x1b[i] += f1.H[i][0] * g1b[0] + f1.H[i][1] * g1b[1] + f1.H[i][2] * g1b[2];
+        theta_b[q][0] += f1.dg_dBp[0] * g1b[0] + f1.dg_dBp[1] * g1b[1] + f1.dg_dBp[2] * g1b[2];
+        theta_b[q][1] += f1.dg_dB0[0] * g1b[0] + f1.dg_dB0[1] * g1b[1] + f1.dg_dB0[2] * g1b[2];
+        // x1 = x0 + dt v1 ; v1 = v0 + hdt as g(x0)
+        R v1b[3];
+        for (int i = 0; i < 3; ++i) v1b[i] = v2b[i] + C.dt * x1b[i];
+        R g0b[3];
+        for (int i = 0; i < 3; ++i) g0b[i] = C.half_dt * as * v1b[i];
+        for (int i = 0; i < 3; ++i) {
+            xb[q][i] = x1b[i] + f0.H[i][0] * g0b[0] + f0.H[i][1] * g0b[1] + f0.H[i][2] * g0b[2];
+            vb[q][i] = v1b[i];
+        }
+        theta_b[q][0] += f0.dg_dBp[0] * g0b[0] + f0.dg_dBp[1] * g0b[1] + f0.dg_dBp[2] * g0b[2];
+        theta_b[q][1] += f0.dg_dB0[0] * g0b[0] + f0.dg_dB0[1] * g0b[1] + f0.dg_dB0[2] * g0b[2];
+        // psi1 = c psi0 + s T(b0) psi0, angle t = theta_per_B |B(x0)|
+        if (larmor) {
+            R tp[4];  // T(b0)^T psi1_bar
+            tp[0] = -f0.b[2] * p1b[1] + f0.b[1] * p1b[2] - f0.b[0] * p1b[3];
+            tp[1] = f0.b[2] * p1b[0] + f0.b[0] * p1b[2] + f0.b[1] * p1b[3];
+            tp[2] = -f0.b[1] * p1b[0] - f0.b[0] * p1b[1] + f0.b[2] * p1b[3];
+            tp[3] = f0.b[0] * p1b[0] - f0.b[1] * p1b[1] - f0.b[2] * p1b[2];
+            R cb = R(0), sb = R(0);
+            for (int k = 0; k < 4; ++k) {
+                cb += p1b[k] * p0[k];
+                sb += tp[k] * p0[k];  // psi1_bar . T(b0) psi0
+            }
+            R b0b[3];
+            b0b[0] = sn * (p1b[0] * p0[3] - p1b[1] * p0[2] + p1b[2] * p0[1] - p1b[3] * p0[0]);
+            b0b[1] = sn * (-p1b[0] * p0[2] - p1b[1] * p0[3] + p1b[2] * p0[0] + p1b[3] * p0[1]);
+            b0b[2] = sn * (p1b[0] * p0[1] - p1b[1] * p0[0] - p1b[2] * p0[3] + p1b[3] * p0[2]);
+            const R tb_ = -sn * cb + cs * sb;
+            field_vec_adjoint(C.Bp, x0, f0, b0b, C.theta_per_B * tb_, xb[q], theta_b[q]);
+            for (int k = 0; k < 4; ++k) pb[q][k] = cs * p1b[k] + sn * tp[k];
+        } else {
+            for (int k = 0; k < 4; ++k) pb[q][k] = p1b[k];
+        }
     }
-    theta_b[0] += eb * C.kappa * f1.dabs_dBp;
-    theta_b[1] += eb * C.kappa * f1.dabs_dB0;
-    // v2 = v1 + hdt as g(x1)
-    R g1b[3];
-    for (int i = 0; i < 3; ++i) g1b[i] = C.half_dt * as * v2b[i];
-    for (int i = 0; i < 3; ++i) x1b[i] += f1.H[i][0] * g1b[0] + f1.H[i][1] * g1b[1] + f1.H[i][2] * g1b[2];
-    theta_b[0] += f1.dg_dBp[0] * g1b[0] + f1.dg_dBp[1] * g1b[1] + f1.dg_dBp[2] * g1b[2];
-    theta_b[1] += f1.dg_dB0[0] * g1b[0] + f1.dg_dB0[1] * g1b[1] + f1.dg_dB0[2] * g1b[2];
-    // x1 = x0 + dt v1 ; v1 = v0 + hdt as g(x0)
-    R v1b[3];
-    for (int i = 0; i < 3; ++i) v1b[i] = v2b[i] + C.dt * x1b[i];
-    R g0b[3];
-    for (int i = 0; i < 3; ++i) g0b[i] = C.half_dt * as * v1b[i];
-    for (int i = 0; i < 3; ++i) {
-        xb[i] = x1b[i] + f0.H[i][0] * g0b[0] + f0.H[i][1] * g0b[1] + f0.H[i][2] * g0b[2];
-        vb[i] = v1b[i];
-    }
-    theta_b[0] += f0.dg_dBp[0] * g0b[0] + f0.dg_dBp[1] * g0b[1] + f0.dg_dBp[2] * g0b[2];
-    theta_b[1] += f0.dg_dB0[0] * g0b[0] + f0.dg_dB0[1] * g0b[1] + f0.dg_dB0[2] * g0b[2];
 }
 
 // collision of a recorded pair with fixed direction n (in place)

@@ -63,6 +63,17 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #define DSMC_FP32_MINB 4
 #endif
 
+// the step kernel: one tile per warp (step_warp), or one tile per block staged in shared memory
+// (step_pass)
+#ifndef DSMC_STEP_WARP
+#define DSMC_STEP_WARP 1
+#endif
+// default nominal tile of step_warp (atoms): a little under a whole number of 32-atom passes
+#ifndef DSMC_WARP_TILE
+#define DSMC_WARP_TILE 240
+#endif
+constexpr int kMaxTileAtoms = 1 << 20;
+
 const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
 constexpr int kNumStepKernels = 4;
 
@@ -86,7 +97,8 @@ struct dsmc_handle {
     virtual int check_wait_timeout() = 0;
     virtual void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) = 0;
     virtual void adjoint_run(const dsmc_adj_params* p, dsmc_grad* g) = 0;
-    virtual void adjoint_loss(const double* theta, double* loss, double* grad) = 0;
+    virtual void adjoint_loss(const double* theta, double* parts, double* grad_e, double* grad_n) = 0;
+    virtual void adjoint_export_spinors(double* psi0, int64_t atoms_cap) = 0;
     virtual void adjoint_export(double* x0, double* v0, int64_t atoms_cap, int32_t* off, int64_t off_cap, int32_t* ij,
                                 double* nv, int64_t log_cap, int64_t* n_atoms, int64_t* n_log, int32_t* steps) = 0;
 };
@@ -154,24 +166,34 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         // cell boundaries overshoots its nominal size by part of a cell
         // preferred nominal tile: three passes of the block, less a part of a cell for the snap
         // to cell boundaries (each step's scan lowers it where a cell is fuller than CAP - T + 1)
+#if DSMC_STEP_WARP
+        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : DSMC_WARP_TILE;
+        if (tile_nominal > kMaxTileAtoms) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(kMaxTileAtoms)};
+#else
         tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP - BLOCK - 16;
         // a grid cell holds at most CAP - T + 1 atoms (DSMC_ERR_CELL_FULL beyond): T <= CAP - 128
         if (tile_nominal > CAP - 128) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP - 128)};
+#endif
         if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
         allocate();
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
         for (int i = 0; i <= kNumStepKernels; ++i) CU(cudaEventCreate(&ev[i]));
+        int dev = 0, nsm = 0, occ = 0;
+        CU(cudaGetDevice(&dev));
+        CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+#if DSMC_STEP_WARP
+        smem_tile = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_warp<R, BLOCK, MINB, false>, BLOCK, 0));
+#else
         smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int) + sizeof(uint16_t));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
-        int dev = 0, nsm = 0, occ = 0;
-        CU(cudaGetDevice(&dev));
-        CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB, false>, BLOCK, smem_tile));
+#endif
         resident_step = nsm * std::max(occ, 1);
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R>, 256, 0));
         resident_permute = nsm * std::max(occ, 1);
@@ -187,6 +209,19 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         const int tmin = args[0].tile_fill > 0 ? std::min(tile_nominal, BLOCK - 16) : tile_nominal;
         const int bound = capacity / tmin + nclouds + 2;
         return std::max(1, std::min(bound, resident));
+    }
+
+    // blocks of the step kernel: no more than the tiles of the smallest tiling the scan may build
+    // need (one per warp for step_warp) nor than fit on the device at once
+    int step_grid() const {
+#if DSMC_STEP_WARP
+        const int tmin = args[0].tile_fill > 0 ? kMinTile : tile_nominal;
+        const long long tiles = (long long)capacity / tmin + nclouds + 2;
+        const long long blocks = (tiles + BLOCK / 32 - 1) / (BLOCK / 32);
+        return (int)std::max(1ll, std::min(blocks, (long long)resident_step));
+#else
+        return tile_grid(resident_step);
+#endif
     }
 
     ~Engine() override {
@@ -304,9 +339,16 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.scan_blk = scan_blk.p;
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
-            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal; A.tile_cap = CAP;
+            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal;
+#if DSMC_STEP_WARP
+            A.tile_cap = 1 << 29;  // nothing is staged: a tile holds cells of any size
+            A.tile_pass = 32;
+            A.tile_fill = run.tile_atoms > 0 ? 0 : resident_step * (BLOCK / 32);  // an explicit size is kept as given
+#else
+            A.tile_cap = CAP;
             A.tile_pass = BLOCK;
             A.tile_fill = run.tile_atoms > 0 ? 0 : resident_step;  // an explicit size is kept as given
+#endif
             A.collide_every = run.collide_every; A.parity = p; A.init_mode = 0;
             A.seed = run.seed;
             A.capacity = capacity;
@@ -317,10 +359,15 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
         case 0:
+#if DSMC_STEP_WARP
+            if (nclouds == 1) step_warp<R, BLOCK, MINB, true><<<step_grid(), BLOCK, 0, stream>>>(A);
+            else step_warp<R, BLOCK, MINB, false><<<step_grid(), BLOCK, 0, stream>>>(A);
+#else
             if (nclouds == 1)
-                step_pass<R, BLOCK, CAP, MINB, true><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
+                step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             else
-                step_pass<R, BLOCK, CAP, MINB, false><<<tile_grid(resident_step), BLOCK, smem_tile, stream>>>(A);
+                step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
+#endif
             break;
         case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
         case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
@@ -693,13 +740,17 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
         if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
+#if DSMC_STEP_WARP
+        const int cands[] = {48, 80, 112, 144, 176, 208, 240, 304, 368, 496, 624, 752, 1008};
+#else
         const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, CAP - BLOCK - 16, 768, 960, 1024};
+#endif
         int best = tile_nominal;
         double best_ms = 1e300;
         const bool prof = profiling;
         profiling = false;
         for (int T : cands) {
-            if (T > CAP - 128) continue;
+            if (!DSMC_STEP_WARP && T > CAP - 128) continue;
             set_tile(T);
             step(1);  // builds the tiling of size T
             CU(cudaEventRecord(ev[0], stream));
@@ -731,11 +782,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 
     // ------------------------------------------------------------------ adjoint
     // record: the physical run's initial state by atom id and its collision events
-    DevBuf<double> adj_x0, adj_v0, adj_n, adj_sums, adj_theta_b;
+    DevBuf<double> adj_x0, adj_v0, adj_p0, adj_n, adj_sums, adj_theta_b;
     DevBuf<int2> adj_ij;
     DevBuf<int> adj_off, adj_count;
     int adj_steps = -1, adj_natoms = 0, adj_nlog = 0, adj_K = 100, adj_prec = DSMC_FP64;
-    double adj_width = 0.2;
+    double adj_width = 0.2, adj_maj_width = 0.05;
 
     void adjoint_run(const dsmc_adj_params* ap, dsmc_grad* g) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "adjoint before init"};
@@ -752,9 +803,12 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (n != (int)cp[0].n_atoms) throw Fail{DSMC_ERR_STATE, "adjoint: atoms were lost before the run"};
         adj_steps = ap->steps; adj_natoms = n; adj_K = ap->checkpoint_every; adj_prec = ap->precision;
         adj_width = ap->sigmoid_width_kT;
+        adj_maj_width = ap->majorana_width > 0 ? ap->majorana_width : 0.05;
         adj_x0.alloc(3 * (size_t)std::max(n, 1)); adj_v0.alloc(3 * (size_t)std::max(n, 1));
+        adj_p0.alloc(4 * (size_t)std::max(n, 1));
         if (n > 0)
-            state_by_id<R><<<(n + 255) / 256, 256, 0, stream>>>(args[parity], n, adj_x0.p, adj_v0.p, &ctl.p->err);
+            state_by_id<R><<<(n + 255) / 256, 256, 0, stream>>>(args[parity], n, adj_x0.p, adj_v0.p, adj_p0.p,
+                                                                 &ctl.p->err);
         const int cap = 1 << 22;
         adj_ij.alloc(cap); adj_n.alloc(3 * (size_t)cap); adj_off.alloc(ap->steps + 1); adj_count.alloc(1);
         CU(cudaMemsetAsync(adj_off.p, 0, (ap->steps + 1) * sizeof(int), stream));
@@ -786,16 +840,19 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         // the smoothed model at the run's own parameters, forward and backward
         double theta[ADJ_NPARAM];
         own_theta(theta);
-        double loss = 0, tb[ADJ_NPARAM] = {0}, W = 0, Sm = 0, ms_f = 0, ms_b = 0;
-        smoothed(theta, true, &loss, tb, &W, &Sm, &ms_f, &ms_b);
+        double parts[2] = {0, 0}, tb[ADJ_SEEDS * ADJ_NPARAM] = {0}, ms_f = 0, ms_b = 0;
+        smoothed(theta, true, parts, tb, &ms_f, &ms_b);
         memset(g, 0, sizeof(*g));
-        g->loss = loss;
-        const double kT = phys[0].kB * cp[0].temperature;
-        g->mean_energy_kT = 0.5 * cp[0].mass * Sm / W / kT;
-        g->retained_fraction = W / (double)n;
-        g->dL_dBp = tb[0];
-        g->dL_dB0 = tb[1];
-        for (int k = 0; k < 9; ++k) g->dL_deta[k] = tb[2 + k];
+        g->loss = parts[0] + parts[1];
+        g->mean_energy_kT = parts[0];
+        g->retained_fraction = parts[1];
+        for (int k = 0; k < ADJ_NPARAM; ++k) {
+            g->dE_dtheta[k] = tb[k];
+            g->dN_dtheta[k] = tb[ADJ_NPARAM + k];
+        }
+        g->dL_dBp = tb[0] + tb[ADJ_NPARAM];
+        g->dL_dB0 = tb[1] + tb[ADJ_NPARAM + 1];
+        for (int k = 0; k < 9; ++k) g->dL_deta[k] = tb[2 + k] + tb[ADJ_NPARAM + 2 + k];
         g->collisions = adj_nlog;
         g->ms_record = ms_rec;
         g->ms_forward = ms_f;
@@ -808,15 +865,15 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         for (int k = 0; k < 9; ++k) theta[2 + k] = cp[0].knife_eta[k];
     }
 
-    void smoothed(const double* theta, bool grad, double* loss, double* tb, double* W, double* Sm, double* ms_f,
-                  double* ms_b) {
-        if (adj_prec == DSMC_FP64) smoothed_t<double>(theta, grad, loss, tb, W, Sm, ms_f, ms_b);
-        else smoothed_t<float>(theta, grad, loss, tb, W, Sm, ms_f, ms_b);
+    // the smoothed loss terms parts = (L_E, L_N) at theta and, with grad, their gradients in tb
+    // (ADJ_SEEDS x ADJ_NPARAM: d L_E, then d L_N)
+    void smoothed(const double* theta, bool grad, double* parts, double* tb, double* ms_f, double* ms_b) {
+        if (adj_prec == DSMC_FP64) smoothed_t<double>(theta, grad, parts, tb, ms_f, ms_b);
+        else smoothed_t<float>(theta, grad, parts, tb, ms_f, ms_b);
     }
 
     template <class S>
-    void smoothed_t(const double* theta, bool grad, double* loss, double* tb, double* Wout, double* Sout,
-                    double* ms_f, double* ms_b) {
+    void smoothed_t(const double* theta, bool grad, double* parts, double* tb, double* ms_f, double* ms_b) {
         typedef typename V4T<S>::type S4;
         const int n = adj_natoms, steps = adj_steps, K = adj_K;
         const dsmc_cloud_params& c = cp[0];
@@ -831,39 +888,45 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         A.C.accel_scale = (S)(c.moment / c.mass);
         A.C.kappa = (S)(2.0 * c.moment / c.mass);
         A.C.inv_width = (S)(1.0 / (2.0 * adj_width * kB * c.temperature / c.mass));
+        A.C.theta_per_B = (c.flags & DSMC_F_LARMOR) ? (S)(c.moment * run.dt / run_hbar(run)) : (S)0;
+        A.C.inv_width_maj = (c.flags & DSMC_F_MAJORANA) ? (S)(1.0 / adj_maj_width) : (S)0;
         A.C.cut_scale = 2.0 * kB * c.temperature / c.mass;
         A.n = n;
         const int nn = std::max(n, 1);
-        DevBuf<S4> x, v, xb, vb, vpre, seg_x, seg_v, ck_x, ck_v;
+        DevBuf<S4> x, v, ps, xb, vb, pb, vpre, seg_x, seg_v, seg_p, ck_x, ck_v, ck_p;
         DevBuf<S> w, e, wb, seg_w, ck_w;
-        x.alloc(nn); v.alloc(nn); w.alloc(nn); e.alloc(nn);
+        x.alloc(nn); v.alloc(nn); ps.alloc(nn); w.alloc(nn); e.alloc(nn);
         const int nseg = (steps + K - 1) / K;
         const int ab = (nn + 255) / 256;
         const int sum_blocks = std::min(ab, 1184);
         partials_buf.alloc(sum_blocks);
         adj_sums.alloc(2);
-        A.x = x.p; A.v = v.p; A.w = w.p; A.e = e.p;
+        A.x = x.p; A.v = v.p; A.psi = ps.p; A.w = w.p; A.e = e.p;
         A.ij = adj_ij.p; A.nv = adj_n.p; A.off = adj_off.p; A.partials = partials_buf.p;
         if (grad) {
             vpre.alloc(2 * (size_t)std::max(adj_nlog, 1));
-            seg_x.alloc((size_t)K * nn); seg_v.alloc((size_t)K * nn); seg_w.alloc((size_t)K * nn);
-            ck_x.alloc((size_t)nseg * nn); ck_v.alloc((size_t)nseg * nn); ck_w.alloc((size_t)nseg * nn);
-            xb.alloc(nn); vb.alloc(nn); wb.alloc(nn);
-            adj_theta_b.alloc(ADJ_NPARAM);
-            CU(cudaMemsetAsync(adj_theta_b.p, 0, ADJ_NPARAM * sizeof(double), stream));
-            A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_w = seg_w.p;
-            A.xb = xb.p; A.vb = vb.p; A.wb = wb.p; A.theta_b = adj_theta_b.p;
+            seg_x.alloc((size_t)K * nn); seg_v.alloc((size_t)K * nn); seg_p.alloc((size_t)K * nn);
+            seg_w.alloc((size_t)K * nn);
+            ck_x.alloc((size_t)nseg * nn); ck_v.alloc((size_t)nseg * nn); ck_p.alloc((size_t)nseg * nn);
+            ck_w.alloc((size_t)nseg * nn);
+            xb.alloc(ADJ_SEEDS * (size_t)nn); vb.alloc(ADJ_SEEDS * (size_t)nn); pb.alloc(ADJ_SEEDS * (size_t)nn);
+            wb.alloc(ADJ_SEEDS * (size_t)nn);
+            adj_theta_b.alloc(ADJ_SEEDS * ADJ_NPARAM);
+            CU(cudaMemsetAsync(adj_theta_b.p, 0, ADJ_SEEDS * ADJ_NPARAM * sizeof(double), stream));
+            A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_psi = seg_p.p; A.seg_w = seg_w.p;
+            A.xb = xb.p; A.vb = vb.p; A.pb = pb.p; A.wb = wb.p; A.theta_b = adj_theta_b.p;
         }
         std::vector<S> cuts(steps);
         for (int t = 0; t < steps; ++t)
             cuts[t] = (S)(A.C.cut_scale * knife_eta(c.knife_nknots, c.knife_step, theta + 2, (double)t));
         CU(cudaEventRecord(ev[0], stream));
-        if (n > 0) sm_load<S><<<ab, 256, 0, stream>>>(A, adj_x0.p, adj_v0.p);
+        if (n > 0) sm_load<S><<<ab, 256, 0, stream>>>(A, adj_x0.p, adj_v0.p, adj_p0.p);
         for (int t = 0; t < steps; ++t) {
             if (grad && t % K == 0) {
                 const size_t o = (size_t)(t / K) * nn;
                 CU(cudaMemcpyAsync(ck_x.p + o, x.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_v.p + o, v.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+                CU(cudaMemcpyAsync(ck_p.p + o, ps.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_w.p + o, w.p, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
             }
             sm_collide<S><<<1, 32, 0, stream>>>(A, t, 0);
@@ -880,9 +943,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (ms_f) *ms_f = mf;
         const double kT = kB * c.temperature;
         const double Wd = sums[0], Sd = sums[1];
-        *loss = 0.5 * c.mass * Sd / Wd / kT + Wd / (double)n;
-        if (Wout) *Wout = Wd;
-        if (Sout) *Sout = Sd;
+        parts[0] = 0.5 * c.mass * Sd / Wd / kT;
+        parts[1] = Wd / (double)n;
         CU(cudaGetLastError());
         if (!grad) return;
         CU(cudaEventRecord(ev[2], stream));
@@ -893,6 +955,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             const size_t o = (size_t)s * nn;
             CU(cudaMemcpyAsync(x.p, ck_x.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
             CU(cudaMemcpyAsync(v.p, ck_v.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(ps.p, ck_p.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
             CU(cudaMemcpyAsync(w.p, ck_w.p + o, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
             for (int t = t0; t < t1; ++t) {
                 sm_collide<S><<<1, 32, 0, stream>>>(A, t, 1);
@@ -907,7 +970,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             }
         }
         CU(cudaEventRecord(ev[3], stream));
-        CU(cudaMemcpyAsync(tb, adj_theta_b.p, ADJ_NPARAM * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CU(cudaMemcpyAsync(tb, adj_theta_b.p, ADJ_SEEDS * ADJ_NPARAM * sizeof(double), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
         CU(cudaGetLastError());
         float mb = 0;
@@ -916,15 +979,24 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     }
     DevBuf<TilePartial> partials_buf;
 
-    void adjoint_loss(const double* theta, double* loss, double* grad) override {
+    void adjoint_loss(const double* theta, double* parts, double* grad_e, double* grad_n) override {
         if (adj_steps < 0) throw Fail{DSMC_ERR_STATE, "dsmc_adjoint_loss needs a recorded run (dsmc_adjoint_run)"};
         double own[ADJ_NPARAM];
         own_theta(own);
         const double* th = theta ? theta : own;
-        double tb[ADJ_NPARAM] = {0};
-        smoothed(th, grad != nullptr, loss, tb, nullptr, nullptr, nullptr, nullptr);
-        if (grad)
-            for (int k = 0; k < ADJ_NPARAM; ++k) grad[k] = tb[k];
+        double tb[ADJ_SEEDS * ADJ_NPARAM] = {0};
+        smoothed(th, grad_e != nullptr || grad_n != nullptr, parts, tb, nullptr, nullptr);
+        for (int k = 0; k < ADJ_NPARAM; ++k) {
+            if (grad_e) grad_e[k] = tb[k];
+            if (grad_n) grad_n[k] = tb[ADJ_NPARAM + k];
+        }
+    }
+
+    void adjoint_export_spinors(double* psi0, int64_t atoms_cap) override {
+        if (adj_steps < 0) throw Fail{DSMC_ERR_STATE, "nothing recorded (dsmc_adjoint_run)"};
+        if (atoms_cap < adj_natoms) throw Fail{DSMC_ERR_INVALID, "spinor buffer too small"};
+        sync();
+        CU(cudaMemcpy(psi0, adj_p0.p, 4 * (size_t)adj_natoms * sizeof(double), cudaMemcpyDeviceToHost));
     }
 
     void adjoint_export(double* x0, double* v0, int64_t atoms_cap, int32_t* off, int64_t off_cap, int32_t* ij,
@@ -1120,7 +1192,24 @@ DSMC_API dsmc_status dsmc_adjoint_run(dsmc_handle* h, const dsmc_adj_params* p, 
 DSMC_API dsmc_status dsmc_adjoint_loss(dsmc_handle* h, const double* theta, double* loss, double* grad) {
     NEED_H;
     if (!loss) return DSMC_ERR_INVALID;
-    return guard(h, [&] { h->adjoint_loss(theta, loss, grad); });
+    return guard(h, [&] {
+        double parts[2], ge[ADJ_NPARAM], gn[ADJ_NPARAM];
+        h->adjoint_loss(theta, parts, grad ? ge : nullptr, grad ? gn : nullptr);
+        *loss = parts[0] + parts[1];
+        if (grad)
+            for (int k = 0; k < ADJ_NPARAM; ++k) grad[k] = ge[k] + gn[k];
+    });
+}
+DSMC_API dsmc_status dsmc_adjoint_loss_parts(dsmc_handle* h, const double* theta, double* parts, double* grad_energy,
+                                             double* grad_retained) {
+    NEED_H;
+    if (!parts) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->adjoint_loss(theta, parts, grad_energy, grad_retained); });
+}
+DSMC_API dsmc_status dsmc_adjoint_export_spinors(dsmc_handle* h, double* psi0, int64_t atoms_cap) {
+    NEED_H;
+    if (!psi0) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->adjoint_export_spinors(psi0, atoms_cap); });
 }
 DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0, int64_t atoms_cap, int32_t* off,
                                          int64_t off_cap, int32_t* ij, double* nv, int64_t log_cap,

@@ -730,8 +730,14 @@ struct NoCollisionLog {
     template <class R> DSMC_HD void accept(uint32_t, uint32_t, R, R, R) {}
 };
 
-template <class R, class V4, class Log = NoCollisionLog>
-DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPhys<R>& P,
+// Element access of the velocities a cell's collisions update: a plain array of n consecutive
+// 4-lane vectors here; the GPU step passes an accessor that reaches each atom through the sorted
+// order's permutation (vload / vstore overloads beside it).
+template <class V4> DSMC_HD V4 vload(V4* vel, uint32_t i) { return vel[i]; }
+template <class V4> DSMC_HD void vstore(V4* vel, uint32_t i, const V4& v) { vel[i] = v; }
+
+template <class R, class VA, class Log = NoCollisionLog>
+DSMC_HD CollideResult<R> collide_cell(VA vel, int n, R& sigvrmax, const CloudPhys<R>& P,
                                       uint32_t local_cell, uint32_t step, uint64_t seed, Log* log = nullptr) {
     CollideResult<R> res;
     res.accepted = 0;
@@ -749,8 +755,8 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
         uint32_t i = index_below(w.x, (uint32_t)n);
         uint32_t j = index_below(w.y, (uint32_t)(n - 1));
         j += (j >= i) ? 1u : 0u;
-        V4 vi = vel[i];
-        V4 vj = vel[j];
+        auto vi = vload(vel, i);
+        auto vj = vload(vel, j);
         R dx = vi.x - vj.x, dy = vi.y - vj.y, dz = vi.z - vj.z;
         R vr = xsqrt(dx * dx + dy * dy + dz * dz);
         R svr = P.sigma * vr;
@@ -771,8 +777,8 @@ DSMC_HD CollideResult<R> collide_cell(V4* vel, int n, R& sigvrmax, const CloudPh
             R cx = R(0.5) * (vi.x + vj.x), cy = R(0.5) * (vi.y + vj.y), cz = R(0.5) * (vi.z + vj.z);
             vi.x = cx + hv * nx; vi.y = cy + hv * ny; vi.z = cz + hv * nz;
             vj.x = cx - hv * nx; vj.y = cy - hv * ny; vj.z = cz - hv * nz;
-            vel[i] = vi;
-            vel[j] = vj;
+            vstore(vel, i, vi);
+            vstore(vel, j, vj);
             res.accepted += 1;
             if (log) log->accept(i, j, nx, ny, nz);
         }

@@ -27,7 +27,8 @@ EXPORTED_SYMBOLS = (
     "dsmc_batch_create", "dsmc_batch_step",
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
-    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_export",
+    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_loss_parts",
+    "dsmc_adjoint_export", "dsmc_adjoint_export_spinors",
     "dsmc_sort_cells_noalloc", "dsmc_check_wait_timeout",
 )
 
@@ -75,6 +76,9 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_autotune": (i32, [vp, i32, C.POINTER(i32), C.POINTER(C.c_double)]),
         "dsmc_adjoint_run": (i32, [vp, C.POINTER(AdjParams), C.POINTER(Grad)]),
         "dsmc_adjoint_loss": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "dsmc_adjoint_loss_parts": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]),
+        "dsmc_adjoint_export_spinors": (i32, [vp, C.POINTER(C.c_double), i64]),
         "dsmc_adjoint_export": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, C.POINTER(i32), i64,
                                       C.POINTER(i32), C.POINTER(C.c_double), i64, C.POINTER(i64), C.POINTER(i64),
                                       C.POINTER(i32)]),
@@ -239,10 +243,12 @@ class Simulation:
 
     # -- pathwise adjoint -----------------------------------------------------------------------------
     def adjoint_run(self, steps: int, checkpoint_every: int = 100, precision: int = _abi.FP64,
-                    sigmoid_width_kT: float = 0.2) -> dict:
+                    sigmoid_width_kT: float = 0.2, majorana_width: float = 0.05) -> dict:
         """Runs `steps` physical steps recording the collisions, then the smoothed loss and its
-        gradient w.r.t. (B', B0, knife knots); see dsmc_adjoint_run in include/dsmc.h."""
-        p = AdjParams(int(steps), int(checkpoint_every), int(precision), 0, float(sigmoid_width_kT))
+        gradient w.r.t. (B', B0, knife knots): of the sum (dL_*) and of each term (dE_dtheta for the
+        mean energy, dN_dtheta for the retained fraction); see dsmc_adjoint_run in include/dsmc.h."""
+        p = AdjParams(int(steps), int(checkpoint_every), int(precision), 0, float(sigmoid_width_kT),
+                      float(majorana_width))
         g = Grad()
         self._check(self.lib.dsmc_adjoint_run(self._h, C.byref(p), C.byref(g)))
         return g.as_dict()
@@ -257,6 +263,17 @@ class Simulation:
                                                dp(g) if grad else None))
         return (loss.value, g) if grad else loss.value
 
+    def adjoint_loss_parts(self, theta=None, grad: bool = False):
+        """The two terms (L_E, L_N) of the smoothed loss at theta and, with grad, their gradients."""
+        parts = np.zeros(2, np.float64)
+        ge = np.zeros(11, np.float64)
+        gn = np.zeros(11, np.float64)
+        th = None if theta is None else np.ascontiguousarray(theta, np.float64)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.dsmc_adjoint_loss_parts(self._h, dp(th) if th is not None else None, dp(parts),
+                                                     dp(ge) if grad else None, dp(gn) if grad else None))
+        return (parts, ge, gn) if grad else parts
+
     def adjoint_export(self) -> dict:
         na, nl, st = C.c_int64(), C.c_int64(), C.c_int32()
         self._check(self.lib.dsmc_adjoint_export(self._h, None, None, 0, None, 0, None, None, 0, C.byref(na),
@@ -268,7 +285,9 @@ class Simulation:
         ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
         self._check(self.lib.dsmc_adjoint_export(self._h, dp(x0), dp(v0), n, ip(off), steps + 1, ip(ij), dp(nv),
                                                  max(m, 1), C.byref(na), C.byref(nl), C.byref(st)))
-        return {"x0": x0, "v0": v0, "off": off, "ij": ij[:m], "n": nv[:m], "steps": steps}
+        psi0 = np.zeros((max(n, 1), 4))
+        self._check(self.lib.dsmc_adjoint_export_spinors(self._h, dp(psi0), max(n, 1)))
+        return {"x0": x0, "v0": v0, "psi0": psi0[:n], "off": off, "ij": ij[:m], "n": nv[:m], "steps": steps}
 
     def autotune(self, steps_per_candidate: int = 5) -> tuple[int, float]:
         """Chooses the tile size by timing (advances the simulation); returns (tile, ms/step)."""

@@ -41,7 +41,7 @@
 #endif
 #define DSMC_API DSMC_EXTERN __attribute__((visibility("default")))
 
-#define DSMC_ABI_VERSION 1
+#define DSMC_ABI_VERSION 2
 
 typedef enum dsmc_status {
     DSMC_OK = 0,
@@ -222,22 +222,27 @@ DSMC_API dsmc_status dsmc_check_wait_timeout(dsmc_handle* h, int32_t* bits);
  * B0 and the knife knot heights eta_0..eta_8, with every random choice of the run held fixed.
  * dsmc_adjoint_run, called right after dsmc_init_cloud on a one-cloud quadrupole handle, runs the
  * physical simulation for `steps` steps recording every accepted collision (pair of atom ids,
- * scattering direction), then evaluates the smoothed model -- all atoms kept, each with a
- * survival weight multiplied every step by sigmoid((cut - E)/(width kB T0)) -- and its adjoint,
- * checkpointed every `checkpoint_every` steps with per-segment recomputation.
- * Loss: (sum w E / sum w) / (kB T0) + sum w / N0.  No counterpart in the reference. */
+ * scattering direction), then evaluates the smoothed model -- all atoms kept, spinors precessing
+ * about the local field as in the run (DSMC_F_LARMOR), each atom with a survival weight multiplied
+ * every step by sigmoid((cut - E)/(width kB T0)) and, when the cloud has DSMC_F_MAJORANA, by
+ * sigmoid(<s.B^> / majorana_width) in place of the hard test <s.B^> < 0 -- and its adjoint through
+ * Verlet, the Larmor rotation and the collision rotations, checkpointed every `checkpoint_every`
+ * steps with per-segment recomputation.  Loss: L = L_E + L_N, L_E = (sum w E / sum w) / (kB T0),
+ * L_N = sum w / N0; the gradient of each term is returned as well as that of their sum.
+ * theta = (B', B0, eta_0 .. eta_8).  No counterpart in the reference. */
 typedef struct dsmc_adj_params {
     int32_t steps;             /* physical steps recorded and differentiated */
     int32_t checkpoint_every;  /* checkpoint interval K of the smoothed model */
     int32_t precision;         /* DSMC_FP32 or DSMC_FP64 for the smoothed model and its adjoint */
     int32_t reserved0;
-    double sigmoid_width_kT;   /* width of the survival sigmoid in units of kB T0 */
+    double sigmoid_width_kT;   /* width of the knife's survival sigmoid in units of kB T0 */
+    double majorana_width;     /* width of the Majorana survival sigmoid in <s.B^> (<= 0: 0.05) */
 } dsmc_adj_params;
 
 typedef struct dsmc_grad {
     double loss;               /* mean_energy_kT + retained_fraction */
-    double mean_energy_kT;     /* sum w E / sum w / (kB T0) after the last step */
-    double retained_fraction;  /* sum w / N0 */
+    double mean_energy_kT;     /* L_E = sum w E / sum w / (kB T0) after the last step */
+    double retained_fraction;  /* L_N = sum w / N0 */
     double dL_dBp;             /* d loss / d B' (per T/m) */
     double dL_dB0;             /* d loss / d bias (per T) */
     double dL_deta[9];         /* d loss / d knot height */
@@ -245,13 +250,21 @@ typedef struct dsmc_grad {
     double ms_record;          /* device time of the recorded physical run */
     double ms_forward;         /* device time of the smoothed forward pass */
     double ms_backward;        /* device time of the recomputation + adjoint pass */
+    double dE_dtheta[11];      /* d L_E / d theta */
+    double dN_dtheta[11];      /* d L_N / d theta */
 } dsmc_grad;
 
 DSMC_API dsmc_status dsmc_adjoint_run(dsmc_handle* h, const dsmc_adj_params* p, dsmc_grad* out);
-/* Smoothed loss of the recorded run at theta = (B', B0, eta_0..eta_8) (NULL: the run's own
- * parameters); grad (11 doubles, may be NULL) receives its gradient.  Same recorded collisions:
- * central differences of this function are common-random-number finite differences. */
+/* Smoothed loss of the recorded run at theta (NULL: the run's own parameters); grad (11 doubles,
+ * may be NULL) receives its gradient.  Same recorded collisions: central differences of this
+ * function are common-random-number finite differences. */
 DSMC_API dsmc_status dsmc_adjoint_loss(dsmc_handle* h, const double* theta, double* loss, double* grad);
+/* The same with the two terms apart: parts[0] = L_E, parts[1] = L_N; grad_energy and
+ * grad_retained (11 doubles each, may be NULL) receive their gradients. */
+DSMC_API dsmc_status dsmc_adjoint_loss_parts(dsmc_handle* h, const double* theta, double* parts, double* grad_energy,
+                                             double* grad_retained);
+/* The recorded run's initial spinors by atom id (4 doubles each: Re u, Im u, Re d, Im d). */
+DSMC_API dsmc_status dsmc_adjoint_export_spinors(dsmc_handle* h, double* psi0, int64_t atoms_cap);
 /* The recorded run: initial positions and velocities by atom id (3 doubles each), per-step
  * offsets (steps + 1), collision pairs (2 ints) and directions (3 doubles).  NULL buffers skip. */
 DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0, int64_t atoms_cap, int32_t* off,

@@ -50,9 +50,10 @@ def load() -> C.CDLL:
             "oracle_field_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), i64]),
             "oracle_smooth_loss": (C.c_double, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
-                                                C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, i32,
-                                                C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double),
-                                                C.POINTER(C.c_double), i32]),
+                                                C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double), i64, i32, C.POINTER(C.c_int32),
+                                                C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double), C.POINTER(C.c_double), i32]),
             "oracle_mcwf_end_d": (i32, [C.POINTER(RunParams), C.POINTER(CloudParams), C.POINTER(C.c_double),
                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), i32, i64]),
@@ -187,21 +188,30 @@ def collide_cell(run: RunParams, cloud: CloudParams, vel, sigvrmax: float, local
     return v4[:, :3].copy(), sv.value, cand.value, ij[:k].copy(), nv[:k].copy()
 
 
-def smooth_loss(run, cloud, theta, width_kT, x, v, steps, log_off, log_ij, log_n, grad=False, fp64=True):
-    """Smoothed-knife loss of the recorded run and, with grad=True, its gradient (B', B0, knots)."""
+def smooth_loss(run, cloud, theta, width_kT, x, v, psi, steps, log_off, log_ij, log_n, grad=False, fp64=True,
+                majorana_width=0.05):
+    """Smoothed loss of the recorded run (mean energy term + retained fraction).
+
+    Returns (loss, parts) -- parts = (L_E, L_N) -- and with grad=True also (grad_E, grad_N), the
+    gradients of each part w.r.t. (B', B0, knots)."""
     dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
     theta = np.ascontiguousarray(theta, np.float64)
     x = np.ascontiguousarray(x, np.float64)
     v = np.ascontiguousarray(v, np.float64)
+    psi = np.ascontiguousarray(psi, np.float64)
     off = np.ascontiguousarray(log_off, np.int32)
     ij = np.ascontiguousarray(log_ij, np.int32)
     ln = np.ascontiguousarray(log_n, np.float64)
-    g = np.zeros(11, np.float64)
-    loss = load().oracle_smooth_loss(C.byref(run), C.byref(cloud), dp(theta), float(width_kT), dp(x), dp(v),
-                                     x.shape[0], int(steps), ip(off), ip(ij), dp(ln),
-                                     dp(g) if grad else None, 1 if fp64 else 0)
-    return (loss, g) if grad else loss
+    parts = np.zeros(2, np.float64)
+    ge = np.zeros(11, np.float64)
+    gn = np.zeros(11, np.float64)
+    loss = load().oracle_smooth_loss(C.byref(run), C.byref(cloud), dp(theta), float(width_kT), float(majorana_width),
+                                     dp(x), dp(v), dp(psi), x.shape[0], int(steps), ip(off), ip(ij), dp(ln), dp(parts),
+                                     dp(ge) if grad else None, dp(gn) if grad else None, 1 if fp64 else 0)
+    if grad:
+        return loss, parts, ge, gn
+    return loss, parts
 
 
 def max_threads() -> int:

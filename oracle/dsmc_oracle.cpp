@@ -203,7 +203,7 @@ template <class R> struct Oracle final : OracleBase {
                     if (m < 2) continue;
                     R svm = sigvrmax[c];
                     CollideResult<R> r =
-                        collide_cell<R, V>(&vel[start[c]], m, svm, C, (uint32_t)(c - C.cell_base), st, run.seed);
+                        collide_cell<R>(&vel[start[c]], m, svm, C, (uint32_t)(c - C.cell_base), st, run.seed);
                     sigvrmax[c] = svm;
                     ca += r.accepted;
                     cc += r.candidates;
@@ -596,7 +596,7 @@ OAPI int oracle_collide_cell_d(const dsmc_params* run, const dsmc_cloud_params* 
     ArrayCollisionLog lg{ij, nv, log_cap, 0};
     Q4<double>* v = reinterpret_cast<Q4<double>*>(vel);
     const CollideResult<double> r =
-        collide_cell<double, Q4<double>, ArrayCollisionLog>(v, n, *sigvrmax, P, local_cell, step, run->seed, &lg);
+        collide_cell<double, Q4<double>*, ArrayCollisionLog>(v, n, *sigvrmax, P, local_cell, step, run->seed, &lg);
     *candidates = r.candidates;
     return r.accepted;
 }
@@ -628,14 +628,16 @@ OAPI int oracle_mcwf_end_d(const dsmc_params* run, const dsmc_cloud_params* c, c
 }
 
 // ---- smoothed model (gradient path) ---------------------------------------------------------
-// theta = (B', B0, eta_0 .. eta_8); x, v: n x 3 in atom-id order; log_off: steps + 1 offsets into
-// the recorded collisions (pairs log_ij, directions log_n).  Returns the smoothed loss and, if
-// grad is not null, its gradient by the hand-written adjoint (all states stored, serial).
+// theta = (B', B0, eta_0 .. eta_8); x, v: n x 3 and psi: n x 4 in atom-id order; log_off: steps +
+// 1 offsets into the recorded collisions (pairs log_ij, directions log_n).  Returns the smoothed
+// loss L_E + L_N (parts[0] = L_E, parts[1] = L_N) and, if grad_e / grad_n are not null, the
+// gradients of each part by the hand-written adjoint (all states stored, serial).
 #include "dsmc_adjoint.h"
 
 namespace {
 template <class R>
-SmoothConsts<R> smooth_consts(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT) {
+SmoothConsts<R> smooth_consts(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT,
+                              double maj_width) {
     const double kB = run_kB(run);
     SmoothConsts<R> C;
     C.Bp = (R)theta[0];
@@ -646,23 +648,27 @@ SmoothConsts<R> smooth_consts(const dsmc_params& run, const dsmc_cloud_params& c
     C.accel_scale = (R)(c.moment / c.mass);
     C.kappa = (R)(2.0 * c.moment / c.mass);
     C.inv_width = (R)(1.0 / (2.0 * width_kT * kB * c.temperature / c.mass));
+    C.theta_per_B = (c.flags & DSMC_F_LARMOR) ? (R)(c.moment * run.dt / run_hbar(run)) : (R)0;
+    C.inv_width_maj = ((c.flags & DSMC_F_MAJORANA) && maj_width > 0) ? (R)(1.0 / maj_width) : (R)0;
     C.cut_scale = 2.0 * kB * c.temperature / c.mass;
     return C;
 }
 
 template <class R>
-double smooth_run(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT,
-                  const double* x0, const double* v0, int64_t n, int steps, const int* off, const int* ij,
-                  const double* ln, double* grad) {
-    const SmoothConsts<R> C = smooth_consts<R>(run, c, theta, width_kT);
+void smooth_run(const dsmc_params& run, const dsmc_cloud_params& c, const double* theta, double width_kT,
+                double maj_width, const double* x0, const double* v0, const double* p0, int64_t n, int steps,
+                const int* off, const int* ij, const double* ln, double* parts, double* grad_e, double* grad_n) {
+    const SmoothConsts<R> C = smooth_consts<R>(run, c, theta, width_kT, maj_width);
     const int nk = c.knife_nknots;
     const double kB = run_kB(run);
-    std::vector<R> x(3 * n), v(3 * n), w(n, R(1)), e(n);
+    std::vector<R> x(3 * n), v(3 * n), ps(4 * n), w(n, R(1)), e(n);
     for (int64_t i = 0; i < 3 * n; ++i) { x[i] = (R)x0[i]; v[i] = (R)v0[i]; }
-    const bool keep = grad != nullptr;
-    std::vector<R> xs, vs, ws, vpre;  // per step: start x, post-collision v, start w; pre-collision pairs
-    if (keep) { xs.resize((size_t)steps * 3 * n); vs.resize((size_t)steps * 3 * n); ws.resize((size_t)steps * n);
-                vpre.resize((size_t)off[steps] * 6); }
+    for (int64_t i = 0; i < 4 * n; ++i) ps[i] = (R)p0[i];
+    const bool keep = grad_e != nullptr || grad_n != nullptr;
+    // per step: start x, post-collision v, start psi and w; pre-collision pairs
+    std::vector<R> xs, vs, pss, ws, vpre;
+    if (keep) { xs.resize((size_t)steps * 3 * n); vs.resize((size_t)steps * 3 * n); pss.resize((size_t)steps * 4 * n);
+                ws.resize((size_t)steps * n); vpre.resize((size_t)off[steps] * 6); }
     std::vector<double> cuts(steps);
     for (int t = 0; t < steps; ++t) {
         for (int k = off[t]; k < off[t + 1]; ++k) {
@@ -678,9 +684,10 @@ double smooth_run(const dsmc_params& run, const dsmc_cloud_params& c, const doub
         if (keep) {
             memcpy(&xs[(size_t)t * 3 * n], x.data(), 3 * n * sizeof(R));
             memcpy(&vs[(size_t)t * 3 * n], v.data(), 3 * n * sizeof(R));
+            memcpy(&pss[(size_t)t * 4 * n], ps.data(), 4 * n * sizeof(R));
             memcpy(&ws[(size_t)t * n], w.data(), n * sizeof(R));
         }
-        for (int64_t i = 0; i < n; ++i) e[i] = smooth_step(C, cut, &x[3 * i], &v[3 * i], w[i]);
+        for (int64_t i = 0; i < n; ++i) e[i] = smooth_step(C, cut, &x[3 * i], &v[3 * i], &ps[4 * i], w[i]);
     }
     i128 W = 0, S = 0;
     for (int64_t i = 0; i < n; ++i) {
@@ -688,54 +695,80 @@ double smooth_run(const dsmc_params& run, const dsmc_cloud_params& c, const doub
         S += fx_from((double)w[i] * (double)e[i]);
     }
     const double Wd = fx_to_double(W), Sd = fx_to_double(S), kT = kB * c.temperature;
-    const double loss = 0.5 * c.mass * Sd / Wd / kT + Wd / (double)n;
-    if (!keep) return loss;
-    // adjoint seeds at the final state
-    std::vector<R> xb(3 * n), vb(3 * n), wb(n);
-    double th[ADJ_NPARAM] = {0};
+    parts[0] = 0.5 * c.mass * Sd / Wd / kT;
+    parts[1] = Wd / (double)n;
+    if (!keep) return;
+    // adjoint seeds at the final state: 0 = L_E, 1 = L_N
+    std::vector<R> xb(ADJ_SEEDS * 3 * n, R(0)), vb(ADJ_SEEDS * 3 * n, R(0)), pb(ADJ_SEEDS * 4 * n, R(0)),
+        wb(ADJ_SEEDS * n, R(0));
+    double th[ADJ_SEEDS][ADJ_NPARAM] = {{0}};
     for (int64_t i = 0; i < n; ++i) {
-        const double dLdw = 0.5 * c.mass * ((double)e[i] / Wd - Sd / (Wd * Wd)) / kT + 1.0 / (double)n;
-        const double dLde = 0.5 * c.mass * (double)w[i] / (Wd * kT);
+        const double dEdw = 0.5 * c.mass * ((double)e[i] / Wd - Sd / (Wd * Wd)) / kT;
+        const double dEde = 0.5 * c.mass * (double)w[i] / (Wd * kT);
         QuadField<R> f;
         quad_field(C.Bp, C.B0, x[3 * i], x[3 * i + 1], x[3 * i + 2], true, f);
         for (int a = 0; a < 3; ++a) {
-            xb[3 * i + a] = (R)(dLde * (double)C.kappa * (double)f.g[a]);
-            vb[3 * i + a] = (R)(dLde * 2.0 * (double)v[3 * i + a]);
+            xb[3 * i + a] = (R)(dEde * (double)C.kappa * (double)f.g[a]);
+            vb[3 * i + a] = (R)(dEde * 2.0 * (double)v[3 * i + a]);
         }
-        wb[i] = (R)dLdw;
-        th[0] += dLde * (double)C.kappa * (double)f.dabs_dBp;
-        th[1] += dLde * (double)C.kappa * (double)f.dabs_dB0;
+        wb[i] = (R)dEdw;
+        wb[n + i] = (R)(1.0 / (double)n);
+        th[0][0] += dEde * (double)C.kappa * (double)f.dabs_dBp;
+        th[0][1] += dEde * (double)C.kappa * (double)f.dabs_dB0;
     }
     for (int t = steps - 1; t >= 0; --t) {
         const R cut = (R)cuts[t];
-        double cutb_sum = 0;
+        double cutb_sum[ADJ_SEEDS] = {0, 0};
         for (int64_t i = 0; i < n; ++i) {
-            R tb[2] = {0, 0};
-            R cb = 0;
+            R axb[ADJ_SEEDS][3], avb[ADJ_SEEDS][3], apb[ADJ_SEEDS][4], awb[ADJ_SEEDS], tb[ADJ_SEEDS][2], cb[ADJ_SEEDS];
+            for (int q = 0; q < ADJ_SEEDS; ++q) {
+                for (int a = 0; a < 3; ++a) { axb[q][a] = xb[(q * n + i) * 3 + a]; avb[q][a] = vb[(q * n + i) * 3 + a]; }
+                for (int a = 0; a < 4; ++a) apb[q][a] = pb[(q * n + i) * 4 + a];
+                awb[q] = wb[q * n + i];
+                tb[q][0] = tb[q][1] = R(0);
+                cb[q] = R(0);
+            }
             smooth_step_adjoint(C, cut, &xs[(size_t)t * 3 * n + 3 * i], &vs[(size_t)t * 3 * n + 3 * i],
-                                ws[(size_t)t * n + i], &xb[3 * i], &vb[3 * i], wb[i], tb, cb);
-            th[0] += (double)tb[0];
-            th[1] += (double)tb[1];
-            cutb_sum += (double)cb;
+                                &pss[(size_t)t * 4 * n + 4 * i], ws[(size_t)t * n + i], axb, avb, apb, awb, tb, cb);
+            for (int q = 0; q < ADJ_SEEDS; ++q) {
+                for (int a = 0; a < 3; ++a) { xb[(q * n + i) * 3 + a] = axb[q][a]; vb[(q * n + i) * 3 + a] = avb[q][a]; }
+                for (int a = 0; a < 4; ++a) pb[(q * n + i) * 4 + a] = apb[q][a];
+                wb[q * n + i] = awb[q];
+                th[q][0] += (double)tb[q][0];
+                th[q][1] += (double)tb[q][1];
+                cutb_sum[q] += (double)cb[q];
+            }
         }
         int k0;
         double f;
         knot_weights(nk, c.knife_step, (double)t, &k0, &f);
-        th[2 + k0] += cutb_sum * C.cut_scale * (1.0 - f);
-        if (f != 0.0) th[2 + k0 + 1] += cutb_sum * C.cut_scale * f;
+        for (int q = 0; q < ADJ_SEEDS; ++q) {
+            th[q][2 + k0] += cutb_sum[q] * C.cut_scale * (1.0 - f);
+            if (f != 0.0) th[q][2 + k0 + 1] += cutb_sum[q] * C.cut_scale * f;
+        }
         for (int k = off[t + 1] - 1; k >= off[t]; --k) {
             const R nn[3] = {(R)ln[3 * k], (R)ln[3 * k + 1], (R)ln[3 * k + 2]};
-            collide_fixed_adjoint(&vpre[6 * k], &vpre[6 * k + 3], nn, &vb[3 * ij[2 * k]], &vb[3 * ij[2 * k + 1]]);
+            for (int q = 0; q < ADJ_SEEDS; ++q)
+                collide_fixed_adjoint(&vpre[6 * k], &vpre[6 * k + 3], nn, &vb[(q * n + ij[2 * k]) * 3],
+                                      &vb[(q * n + ij[2 * k + 1]) * 3]);
         }
     }
-    for (int p = 0; p < ADJ_NPARAM; ++p) grad[p] = th[p];
-    return loss;
+    for (int p = 0; p < ADJ_NPARAM; ++p) {
+        if (grad_e) grad_e[p] = th[0][p];
+        if (grad_n) grad_n[p] = th[1][p];
+    }
 }
 }  // namespace
 
+// The smoothed loss of a recorded run (L_E + L_N; parts[0..1] = L_E, L_N) and the gradient of each
+// part (grad_e, grad_n: 11 doubles each, or null).  psi holds the initial spinors by atom id;
+// maj_width is the width of the Majorana survival sigmoid in <s.B^> (used when the cloud has
+// Majorana loss).
 OAPI double oracle_smooth_loss(const dsmc_params* run, const dsmc_cloud_params* c, const double* theta,
-                               double width_kT, const double* x, const double* v, int64_t n, int steps,
-                               const int* off, const int* ij, const double* ln, double* grad, int fp64) {
-    if (fp64) return smooth_run<double>(*run, *c, theta, width_kT, x, v, n, steps, off, ij, ln, grad);
-    return smooth_run<float>(*run, *c, theta, width_kT, x, v, n, steps, off, ij, ln, grad);
+                               double width_kT, double maj_width, const double* x, const double* v, const double* psi,
+                               int64_t n, int steps, const int* off, const int* ij, const double* ln, double* parts,
+                               double* grad_e, double* grad_n, int fp64) {
+    if (fp64) smooth_run<double>(*run, *c, theta, width_kT, maj_width, x, v, psi, n, steps, off, ij, ln, parts, grad_e, grad_n);
+    else smooth_run<float>(*run, *c, theta, width_kT, maj_width, x, v, psi, n, steps, off, ij, ln, parts, grad_e, grad_n);
+    return parts[0] + parts[1];
 }

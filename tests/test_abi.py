@@ -85,7 +85,7 @@ def test_presets():
 
 def test_status_strings():
     lib = dsmc.load_library()
-    assert lib.dsmc_abi_version() == 1
+    assert lib.dsmc_abi_version() == 2
     assert lib.dsmc_status_string(5) == b"cell too full for one tile"
 
 
