@@ -14,6 +14,7 @@ FP32, FP64 = 0, 1
 TRAP_QUADRUPOLE, TRAP_IOFFE_PRITCHARD, TRAP_BOX = 0, 1, 2
 F_COLLIDE, F_LARMOR, F_MAJORANA, F_KNIFE, F_NORMALISE, F_KNIFE_FIXED_T, F_MCWF = 1, 2, 4, 8, 16, 32, 64
 INIT_THERMAL, INIT_UNIFORM = 0, 1
+REC_EVAPORATED, REC_CELL_COLLISIONS = 1, 2  # dsmc_set_recording
 MAX_KNOTS = 9
 
 # named workloads (dsmc_preset)

@@ -10,7 +10,9 @@
 // collisionsPerPrint x loopsPerCollision motion steps (main.cu:410-524) and a snapshot is
 // written (main.cu:526-577).  Snapshots replace the HDF5 file /atomData/* with one .npy file
 // per dataset and frame in DIR (positions, velocities, psiUp, psiDn, atomID, atomIsSpinUp,
-// cellID, atomCount, atomNumber, simuatedTime) -- the names of the reference datasets.
+// cellID, atomCount, atomNumber, simuatedTime, evapPos, evapVel, collisionCount) -- the names
+// of the reference datasets; cudadsmc_b200.snapshots.read_snapshots stacks the frames into the
+// reference's (N, k, t) arrays.
 // --loops-per-collision is the reference's loopsPerCollision (main.cu:168: motion steps per
 // collision step, the engine's collide_every); --mcwf turns on the spin-flip and decoherence
 // path that the reference runs once per collision step (main.cu:501-520).
@@ -97,6 +99,15 @@ void snapshot(dsmc_handle* h, const std::string& dir, int frame, int64_t cap, co
     int32_t number = (int32_t)n;
     write_npy(dir + "/atomNumber" + f, "<i4", {1}, &number, 4);
     write_npy(dir + "/simuatedTime" + f, "<f8", {1}, &d.time, 8);
+    // evaporated atoms by atom id (zeros for atoms not lost) and the last collision step's counts
+    std::vector<double> ep(3 * cap), evl(3 * cap);
+    if (check(dsmc_get_evaporated(h, 0, ep.data(), evl.data(), nullptr, nullptr, cap), h, "dsmc_get_evaporated")) {
+        write_npy(dir + "/evapPos" + f, "<f8", {(long)cap, 3}, ep.data(), ep.size() * 8);
+        write_npy(dir + "/evapVel" + f, "<f8", {(long)cap, 3}, evl.data(), evl.size() * 8);
+    }
+    std::vector<int32_t> coll(ncells);
+    if (check(dsmc_get_cell_collisions(h, coll.data(), ncells, &ncells), h, "dsmc_get_cell_collisions"))
+        write_npy(dir + "/collisionCount" + f, "<i4", {(long)ncells}, coll.data(), coll.size() * 4);
 }
 
 }  // namespace
@@ -145,7 +156,12 @@ int main(int argc, char** argv) {
     dsmc_handle* h = nullptr;
     if (!check(dsmc_create(&run, &cloud, 1, &h), nullptr, "dsmc_create")) return 1;
     if (!check(dsmc_init_cloud(h, seed), h, "dsmc_init_cloud")) return 1;
-    if (!out.empty()) mkdir(out.c_str(), 0755);
+    if (!out.empty()) {
+        mkdir(out.c_str(), 0755);
+        // the evapPos / evapVel / collisionCount datasets need the step's records
+        if (!check(dsmc_set_recording(h, DSMC_REC_EVAPORATED | DSMC_REC_CELL_COLLISIONS), h, "dsmc_set_recording"))
+            return 1;
+    }
     dsmc_diag d;
     dsmc_diagnostics(h, -1, &d);
     const double e0 = d.e_kin + d.e_pot;

@@ -99,6 +99,9 @@ struct dsmc_handle {
     virtual void adjoint_run(const dsmc_adj_params* p, dsmc_grad* g) = 0;
     virtual void adjoint_loss(const double* theta, double* parts, double* grad_e, double* grad_n) = 0;
     virtual void adjoint_export_spinors(double* psi0, int64_t atoms_cap) = 0;
+    virtual void set_recording(int flags) = 0;
+    virtual void get_evaporated(int cloud, double* pos3, double* vel3, int32_t* step, int32_t* fate, int64_t cap) = 0;
+    virtual void get_cell_collisions(int32_t* counts, int64_t cap, int64_t* total) = 0;
     virtual void adjoint_export(double* x0, double* v0, int64_t atoms_cap, int32_t* off, int64_t off_cap, int32_t* ij,
                                 double* nv, int64_t log_cap, int64_t* n_atoms, int64_t* n_log, int32_t* steps) = 0;
 };
@@ -245,7 +248,10 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             make_cloud_phys<R>(run, c, k, (int)cells, phys[k]);
             cloud_cell_base[k] = (int)cells;
             cells += cloud_cells(c);
-            cap += c.capacity > 0 ? c.capacity : c.n_atoms;
+            const int64_t ck = c.capacity > 0 ? c.capacity : c.n_atoms;
+            phys[k].id_base = (int32_t)std::min<int64_t>(cap, INT32_MAX);
+            phys[k].id_cap = (int32_t)std::min<int64_t>(ck, INT32_MAX);
+            cap += ck;
             cloud_atoms_init[k] = (int)c.n_atoms;
         }
         cloud_cell_base[nclouds] = (int)cells;
@@ -992,6 +998,70 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         }
     }
 
+    // ------------------------------------------------------------------ snapshot records
+    DevBuf<R4> rec_pos, rec_vel;
+    DevBuf<int2> rec_coll;
+    int rec_flags = 0;
+
+    void set_recording(int flags) override {
+        if (flags & ~(DSMC_REC_EVAPORATED | DSMC_REC_CELL_COLLISIONS)) throw Fail{DSMC_ERR_INVALID, "unknown record flags"};
+        sync();
+        if ((flags & DSMC_REC_EVAPORATED) && !rec_pos.p) { rec_pos.alloc(capacity); rec_vel.alloc(capacity); }
+        if ((flags & DSMC_REC_CELL_COLLISIONS) && !rec_coll.p) rec_coll.alloc(total_cells);
+        // cleared on every call: never lost (step lane all ones), never collided (step -1)
+        if (flags & DSMC_REC_EVAPORATED) {
+            CU(cudaMemsetAsync(rec_pos.p, 0xff, capacity * sizeof(R4), stream));
+            CU(cudaMemsetAsync(rec_vel.p, 0, capacity * sizeof(R4), stream));
+        }
+        if (flags & DSMC_REC_CELL_COLLISIONS) CU(cudaMemsetAsync(rec_coll.p, 0xff, total_cells * sizeof(int2), stream));
+        rec_flags = flags;
+        for (int p = 0; p < 2; ++p) {
+            args[p].rec_evap_pos = (flags & DSMC_REC_EVAPORATED) ? rec_pos.p : nullptr;
+            args[p].rec_evap_vel = (flags & DSMC_REC_EVAPORATED) ? rec_vel.p : nullptr;
+            args[p].rec_cell_coll = (flags & DSMC_REC_CELL_COLLISIONS) ? rec_coll.p : nullptr;
+        }
+        drop_graphs();  // the step graphs hold the kernel parameters
+        sync();
+    }
+
+    void get_evaporated(int cloud, double* pos3, double* vel3, int32_t* step_out, int32_t* fate, int64_t cap) override {
+        if (!(rec_flags & DSMC_REC_EVAPORATED)) throw Fail{DSMC_ERR_STATE, "evaporated atoms are not recorded (dsmc_set_recording)"};
+        if (cloud < 0 || cloud >= nclouds) throw Fail{DSMC_ERR_INVALID, "cloud index"};
+        const int base = phys[cloud].id_base, n = phys[cloud].id_cap;
+        if (cap < n) throw Fail{DSMC_ERR_INVALID, "buffers smaller than the cloud's capacity"};
+        sync();
+        std::vector<R4> hp(n), hv(n);
+        if (n > 0) {
+            CU(cudaMemcpy(hp.data(), rec_pos.p + base, n * sizeof(R4), cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(hv.data(), rec_vel.p + base, n * sizeof(R4), cudaMemcpyDeviceToHost));
+        }
+        for (int i = 0; i < n; ++i) {
+            const uint32_t st = lane_to_u32(hp[i].w);
+            const bool lost = st != 0xffffffffu;
+            if (pos3) { pos3[3 * i] = lost ? (double)hp[i].x : 0.0; pos3[3 * i + 1] = lost ? (double)hp[i].y : 0.0;
+                        pos3[3 * i + 2] = lost ? (double)hp[i].z : 0.0; }
+            if (vel3) { vel3[3 * i] = (double)hv[i].x; vel3[3 * i + 1] = (double)hv[i].y; vel3[3 * i + 2] = (double)hv[i].z; }
+            if (step_out) step_out[i] = lost ? (int32_t)st : -1;
+            if (fate) fate[i] = lost ? (int32_t)lane_to_u32(hv[i].w) : 0;
+        }
+    }
+
+    void get_cell_collisions(int32_t* counts, int64_t cap, int64_t* total) override {
+        if (!(rec_flags & DSMC_REC_CELL_COLLISIONS)) throw Fail{DSMC_ERR_STATE, "cell collisions are not recorded (dsmc_set_recording)"};
+        if (total) *total = total_cells;
+        if (!counts) return;
+        if (cap < total_cells) throw Fail{DSMC_ERR_INVALID, "buffer smaller than the cell count"};
+        sync();
+        Ctl h;
+        CU(cudaMemcpy(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        // the last step that ran the collisions: the largest s below the coming step with s % collide_every == 0
+        const int next = h.step[parity];
+        const int last = next > 0 ? ((next - 1) / run.collide_every) * run.collide_every : -1;
+        std::vector<int2> hc(total_cells);
+        CU(cudaMemcpy(hc.data(), rec_coll.p, total_cells * sizeof(int2), cudaMemcpyDeviceToHost));
+        for (int c = 0; c < total_cells; ++c) counts[c] = (last >= 0 && hc[c].x == last) ? hc[c].y : 0;
+    }
+
     void adjoint_export_spinors(double* psi0, int64_t atoms_cap) override {
         if (adj_steps < 0) throw Fail{DSMC_ERR_STATE, "nothing recorded (dsmc_adjoint_run)"};
         if (atoms_cap < adj_natoms) throw Fail{DSMC_ERR_INVALID, "spinor buffer too small"};
@@ -1205,6 +1275,19 @@ DSMC_API dsmc_status dsmc_adjoint_loss_parts(dsmc_handle* h, const double* theta
     NEED_H;
     if (!parts) return DSMC_ERR_INVALID;
     return guard(h, [&] { h->adjoint_loss(theta, parts, grad_energy, grad_retained); });
+}
+DSMC_API dsmc_status dsmc_set_recording(dsmc_handle* h, int32_t flags) {
+    NEED_H;
+    return guard(h, [&] { h->set_recording(flags); });
+}
+DSMC_API dsmc_status dsmc_get_evaporated(dsmc_handle* h, int32_t cloud, double* pos, double* vel, int32_t* step,
+                                         int32_t* fate, int64_t cap) {
+    NEED_H;
+    return guard(h, [&] { h->get_evaporated(cloud, pos, vel, step, fate, cap); });
+}
+DSMC_API dsmc_status dsmc_get_cell_collisions(dsmc_handle* h, int32_t* counts, int64_t cap, int64_t* total) {
+    NEED_H;
+    return guard(h, [&] { h->get_cell_collisions(counts, cap, total); });
 }
 DSMC_API dsmc_status dsmc_adjoint_export_spinors(dsmc_handle* h, double* psi0, int64_t atoms_cap) {
     NEED_H;

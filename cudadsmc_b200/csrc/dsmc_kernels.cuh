@@ -169,6 +169,12 @@ template <class R> struct Args {
     int* clog_count;
     int* clog_off;
     int clog_cap, clog_step0, clog_steps;
+    // snapshot records (null when off): per atom id slot (cloud's id_base + id) the state at the
+    // step it was lost -- position with the step number in the fourth lane, velocity with the fate
+    // -- and per global cell (step, accepted collisions) of the last step that collided it
+    R4* rec_evap_pos;
+    R4* rec_evap_vel;
+    int2* rec_cell_coll;
     unsigned long long seed;
 };
 
@@ -908,6 +914,7 @@ __global__ void __launch_bounds__(WBLOCK, MINB) step_warp(const __grid_constant_
                     A.sigvrmax[c] = svm;
                     acc.coll += (unsigned)cr.accepted;
                     acc.cand += (unsigned)cr.candidates;
+                    if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
                 }
             }
             __syncwarp();
@@ -1061,6 +1068,14 @@ __global__ void __launch_bounds__(WBLOCK, MINB) step_warp(const __grid_constant_
                     add_limbs(bk->eB, fx_from(o.absB));
                     atomicAdd(o.fate == FATE_MAJORANA ? &bk->n_maj : &bk->n_knife, 1ull);
                     A.keys[j] = make_int2(-1, KIND_LOST);
+                    const unsigned id = lane_to_u32(q.w);
+                    if (A.rec_evap_pos && id < (unsigned)P.id_cap) {
+                        R4 ep, ev;
+                        ep.x = a.x; ep.y = a.y; ep.z = a.z; ep.w = lane_from_u32((uint32_t)step, R(0));
+                        ev.x = a.vx; ev.y = a.vy; ev.z = a.vz; ev.w = lane_from_u32((uint32_t)o.fate, R(0));
+                        A.rec_evap_pos[P.id_base + id] = ep;
+                        A.rec_evap_vel[P.id_base + id] = ev;
+                    }
                 }
             }
         }

@@ -424,6 +424,8 @@ template <class R> struct CloudPhys {
     R prop_min_x, prop_min_y, prop_min_z;  // proposal box of the rejection sampler
     R prop_len_x, prop_len_y, prop_len_z;
     int32_t knife_nknots;
+    int32_t id_base;  // first slot of this cloud in by-atom-id records (the capacities of the clouds before it)
+    int32_t id_cap;   // atom ids of this cloud that have a slot there (its capacity)
     int32_t pad0;
     double knife_step[9];
     double knife_eta[9];

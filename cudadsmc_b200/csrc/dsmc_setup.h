@@ -118,6 +118,9 @@ inline void make_cloud_phys(const dsmc_params& run, const dsmc_cloud_params& c, 
         P.prop_len_x = (R)(hi[0] - lo[0]); P.prop_len_y = (R)(hi[1] - lo[1]); P.prop_len_z = (R)(hi[2] - lo[2]);
     }
     P.knife_nknots = c.knife_nknots;
+    P.id_base = 0;  // set by the owner of the by-id records, which knows every cloud's capacity
+    P.id_cap = (int32_t)c.capacity;
+    P.pad0 = 0;
     for (int i = 0; i < DSMC_MAX_KNOTS; ++i) {
         P.knife_step[i] = c.knife_step[i];
         P.knife_eta[i] = c.knife_eta[i];

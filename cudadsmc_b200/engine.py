@@ -27,7 +27,8 @@ EXPORTED_SYMBOLS = (
     "dsmc_batch_create", "dsmc_batch_step",
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
-    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_loss_parts",
+    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_set_recording", "dsmc_get_evaporated", "dsmc_get_cell_collisions",
+    "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_loss_parts",
     "dsmc_adjoint_export", "dsmc_adjoint_export_spinors",
     "dsmc_sort_cells_noalloc", "dsmc_check_wait_timeout",
 )
@@ -79,6 +80,10 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_adjoint_loss_parts": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]),
         "dsmc_adjoint_export_spinors": (i32, [vp, C.POINTER(C.c_double), i64]),
+        "dsmc_set_recording": (i32, [vp, i32]),
+        "dsmc_get_evaporated": (i32, [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(i32),
+                                      C.POINTER(i32), i64]),
+        "dsmc_get_cell_collisions": (i32, [vp, C.POINTER(i32), i64, C.POINTER(i64)]),
         "dsmc_adjoint_export": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), i64, C.POINTER(i32), i64,
                                       C.POINTER(i32), C.POINTER(C.c_double), i64, C.POINTER(i64), C.POINTER(i64),
                                       C.POINTER(i32)]),
@@ -240,6 +245,32 @@ class Simulation:
         bits = C.c_int32(0)
         self._check(self.lib.dsmc_check_wait_timeout(self._h, C.byref(bits)))
         return int(bits.value)
+
+    # -- snapshot records ---------------------------------------------------------------------------
+    def set_recording(self, flags: int) -> None:
+        """Turns the snapshot records on (cleared) or off: REC_EVAPORATED, REC_CELL_COLLISIONS."""
+        self._check(self.lib.dsmc_set_recording(self._h, int(flags)))
+
+    def evaporated(self, cloud: int = 0) -> dict:
+        """The lost atoms of a cloud by atom id: position, velocity, step and fate (1 Majorana,
+        2 knife) at the step each was lost in (step -1 and zeros for atoms never lost)."""
+        c = self.clouds[cloud]
+        n = int(c.capacity if c.capacity > 0 else c.n_atoms)
+        pos, vel = np.zeros((max(n, 1), 3)), np.zeros((max(n, 1), 3))
+        step, fate = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._check(self.lib.dsmc_get_evaporated(self._h, int(cloud), dp(pos), dp(vel), ip(step), ip(fate), max(n, 1)))
+        return {"pos": pos[:n], "vel": vel[:n], "step": step[:n], "fate": fate[:n]}
+
+    def cell_collisions(self) -> np.ndarray:
+        """Accepted collisions of every global cell in the last step that ran the collisions."""
+        total = C.c_int64()
+        self._check(self.lib.dsmc_get_cell_collisions(self._h, None, 0, C.byref(total)))
+        out = np.zeros(max(total.value, 1), np.int32)
+        self._check(self.lib.dsmc_get_cell_collisions(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size,
+                                                      C.byref(total)))
+        return out[:total.value]
 
     # -- pathwise adjoint -----------------------------------------------------------------------------
     def adjoint_run(self, steps: int, checkpoint_every: int = 100, precision: int = _abi.FP64,

@@ -217,6 +217,28 @@ DSMC_API int32_t dsmc_launches_per_step(dsmc_handle* h);
  * cells span at least two scan blocks (more than 4096 cells); takes about a second. */
 DSMC_API dsmc_status dsmc_check_wait_timeout(dsmc_handle* h, int32_t* bits);
 
+/* ---- snapshot records ------------------------------------------------------------------------
+ * The reference's snapshots carry, beside the state, each atom's position and velocity at the
+ * step it was tagged for loss (evapPos / evapVel by atom, zeros for atoms never lost,
+ * evaporation.cu:68-106, main.cu:234-264) and each cell's accepted collisions in the last
+ * collision step (collisionCount, collisions.cu:335-436, main.cu:291-304).  They cost memory and
+ * stores in the step, so they are kept only when asked for.  dsmc_set_recording(h, flags) turns
+ * them on (clearing them) or off; the step then writes them (no host synchronisation). */
+enum {
+    DSMC_REC_EVAPORATED = 1,       /* position / velocity / step / fate of every atom lost, by atom id */
+    DSMC_REC_CELL_COLLISIONS = 2   /* accepted collisions of every cell in the last collision step */
+};
+DSMC_API dsmc_status dsmc_set_recording(dsmc_handle* h, int32_t flags);
+/* Cloud `cloud`'s lost atoms by atom id (arrays of at least the cloud's capacity; NULL skips):
+ * pos / vel 3 doubles each (zeros for an atom never lost), step the step it was lost in (-1:
+ * never), fate how it was lost: 1 Majorana (<s.B^> < 0), 2 energy knife (0: never lost). */
+DSMC_API dsmc_status dsmc_get_evaporated(dsmc_handle* h, int32_t cloud, double* pos, double* vel, int32_t* step,
+                                         int32_t* fate, int64_t cap);
+/* Accepted collisions per global cell (every cloud's grid cells then its overflow cell, as
+ * dsmc_get_cell_starts) in the last step that ran the collisions; *total receives the cell count
+ * (counts may be NULL to query it). */
+DSMC_API dsmc_status dsmc_get_cell_collisions(dsmc_handle* h, int32_t* counts, int64_t cap, int64_t* total);
+
 /* ---- pathwise adjoint ----------------------------------------------------------------------
  * Gradient of a smoothed loss of the physical run with respect to the trap gradient B', the bias
  * B0 and the knife knot heights eta_0..eta_8, with every random choice of the run held fixed.

@@ -40,6 +40,10 @@ def load() -> C.CDLL:
             "oracle_get_cell_starts": (i32, [vp, C.POINTER(C.c_int32), i64, C.POINTER(i64)]),
             "oracle_get_sigvrmax": (i32, [vp, vp, i64]),
             "oracle_set_sigvrmax": (i32, [vp, vp, i64]),
+            "oracle_set_recording": (i32, [vp, i32]),
+            "oracle_get_evaporated": (i32, [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), i64]),
+            "oracle_get_cell_collisions": (i32, [vp, C.POINTER(C.c_int32), i64]),
             "oracle_max_threads": (i32, []),
             "oracle_set_threads": (None, [i32]),
             "oracle_preset": (i32, [i32, C.POINTER(RunParams), C.POINTER(CloudParams)]),
@@ -285,6 +289,27 @@ class Oracle:
         b = StateBuffers(pos.ctypes.data, vel.ctypes.data, psi.ctypes.data, pos.shape[0],
                          counts.ctypes.data_as(C.POINTER(C.c_int64)))
         self._check(self.lib.oracle_set_state(self._h, C.byref(b)))
+
+    def set_recording(self, flags: int) -> None:
+        self._check(self.lib.oracle_set_recording(self._h, int(flags)))
+
+    def evaporated(self, cloud: int = 0) -> dict:
+        c = self.clouds[cloud]
+        n = int(c.capacity if c.capacity > 0 else c.n_atoms)
+        pos, vel = np.zeros((max(n, 1), 3)), np.zeros((max(n, 1), 3))
+        step, fate = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.int32)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._check(self.lib.oracle_get_evaporated(self._h, int(cloud), dp(pos), dp(vel), ip(step), ip(fate),
+                                                   max(n, 1)))
+        return {"pos": pos[:n], "vel": vel[:n], "step": step[:n], "fate": fate[:n]}
+
+    def cell_collisions(self) -> np.ndarray:
+        total = C.c_int64()
+        self._check(self.lib.oracle_get_cell_starts(self._h, None, 0, C.byref(total)))
+        out = np.zeros(max(total.value, 1), np.int32)
+        self._check(self.lib.oracle_get_cell_collisions(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), out.size))
+        return out[:total.value]
 
     def cell_starts(self) -> np.ndarray:
         total = C.c_int64()

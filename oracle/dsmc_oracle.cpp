@@ -61,6 +61,9 @@ struct OracleBase {
     virtual void cell_starts(int32_t* st, int64_t cap, int64_t* total) = 0;
     virtual void get_sigvrmax(void* out, int64_t cap) = 0;
     virtual void set_sigvrmax(const void* in, int64_t n) = 0;
+    virtual void set_recording(int flags) = 0;
+    virtual void get_evaporated(int k, double* p3, double* v3, int32_t* st, int32_t* fa, int64_t cap) = 0;
+    virtual void get_cell_collisions(int32_t* counts, int64_t cap) = 0;
 };
 
 struct OFail { std::string msg; };
@@ -80,6 +83,12 @@ template <class R> struct Oracle final : OracleBase {
     std::vector<CloudAcc> acc;
     int step_no = 0;
     bool ready = false;
+    // snapshot records (DSMC_REC_* flags): lost atoms by id slot, collisions per cell and step
+    int rec_flags = 0;
+    std::vector<V> rec_pos, rec_vel;
+    std::vector<int> rec_step, rec_fate;
+    std::vector<int> rec_coll_step, rec_coll_count;
+    int64_t id_slots = 0;
 
     Oracle(const dsmc_params& r, const dsmc_cloud_params* c, int n, bool f) : run(r), cp(c, c + n), nclouds(n), fast(f) {
         phys.resize(n);
@@ -91,6 +100,10 @@ template <class R> struct Oracle final : OracleBase {
             make_cloud_phys<R>(run, cp[k], k, cells, phys[k]);
             cell_base[k] = cells;
             cells += (int)cloud_cells(cp[k]);
+            const int64_t ck = cp[k].capacity > 0 ? cp[k].capacity : cp[k].n_atoms;
+            phys[k].id_base = (int32_t)id_slots;
+            phys[k].id_cap = (int32_t)ck;
+            id_slots += ck;
         }
         cell_base[n] = cells;
         total_cells = cells;
@@ -207,6 +220,10 @@ template <class R> struct Oracle final : OracleBase {
                     sigvrmax[c] = svm;
                     ca += r.accepted;
                     cc += r.candidates;
+                    if (rec_flags & DSMC_REC_CELL_COLLISIONS) {
+                        rec_coll_step[c] = step_no;
+                        rec_coll_count[c] = r.accepted;
+                    }
                 }
                 coll[k] = ca;
                 cand[k] = cc;
@@ -286,6 +303,14 @@ template <class R> struct Oracle final : OracleBase {
                     ev += fx_from((double)v2[i]);
                     eb += fx_from((double)absB[i]);
                     if (fate[i] == FATE_MAJORANA) ++maj; else ++kn;
+                    const uint32_t id = lane_to_u32(pos[i].w);
+                    if ((rec_flags & DSMC_REC_EVAPORATED) && id < (uint32_t)phys[k].id_cap) {
+                        const int64_t slot = phys[k].id_base + (int64_t)id;
+                        rec_pos[slot] = pos[i];
+                        rec_vel[slot] = vel[i];
+                        rec_step[slot] = step_no;
+                        rec_fate[slot] = fate[i];
+                    }
                 }
             }
             a.step = step_no + 1;
@@ -310,6 +335,37 @@ template <class R> struct Oracle final : OracleBase {
         for (int c = 0; c < total_cells; ++c) start[c + 1] += start[c];
         pos.swap(P2); vel.swap(V2); psi.swap(S2);
         ++step_no;
+    }
+
+    void set_recording(int flags) override {
+        rec_flags = flags;
+        if (flags & DSMC_REC_EVAPORATED) {
+            rec_pos.assign(id_slots, V{0, 0, 0, 0});
+            rec_vel.assign(id_slots, V{0, 0, 0, 0});
+            rec_step.assign(id_slots, -1);
+            rec_fate.assign(id_slots, 0);
+        }
+        if (flags & DSMC_REC_CELL_COLLISIONS) {
+            rec_coll_step.assign(total_cells, -1);
+            rec_coll_count.assign(total_cells, 0);
+        }
+    }
+    void get_evaporated(int k, double* p3, double* v3, int32_t* st, int32_t* fa, int64_t cap) override {
+        if (!(rec_flags & DSMC_REC_EVAPORATED) || k < 0 || k >= nclouds || cap < phys[k].id_cap) throw OFail{"get_evaporated"};
+        for (int i = 0; i < phys[k].id_cap; ++i) {
+            const int64_t s = phys[k].id_base + i;
+            for (int a = 0; a < 3; ++a) {
+                if (p3) p3[3 * i + a] = (double)(&rec_pos[s].x)[a];
+                if (v3) v3[3 * i + a] = (double)(&rec_vel[s].x)[a];
+            }
+            if (st) st[i] = rec_step[s];
+            if (fa) fa[i] = rec_fate[s];
+        }
+    }
+    void get_cell_collisions(int32_t* counts, int64_t cap) override {
+        if (!(rec_flags & DSMC_REC_CELL_COLLISIONS) || cap < total_cells) throw OFail{"get_cell_collisions"};
+        const int last = step_no > 0 ? ((step_no - 1) / run.collide_every) * run.collide_every : -1;
+        for (int c = 0; c < total_cells; ++c) counts[c] = (last >= 0 && rec_coll_step[c] == last) ? rec_coll_count[c] : 0;
     }
 
     // The same order as the stable sort, built in parallel: for every new cell its stayers
@@ -449,6 +505,15 @@ OAPI int oracle_get_sigvrmax(void* h, void* out, int64_t cap) {
 }
 OAPI int oracle_set_sigvrmax(void* h, const void* in, int64_t n) {
     return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->set_sigvrmax(in, n); });
+}
+OAPI int oracle_set_recording(void* h, int flags) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->set_recording(flags); });
+}
+OAPI int oracle_get_evaporated(void* h, int cloud, double* pos, double* vel, int32_t* step, int32_t* fate, int64_t cap) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->get_evaporated(cloud, pos, vel, step, fate, cap); });
+}
+OAPI int oracle_get_cell_collisions(void* h, int32_t* counts, int64_t cap) {
+    return oguard((OracleBase*)h, [&] { ((OracleBase*)h)->get_cell_collisions(counts, cap); });
 }
 OAPI int oracle_max_threads(void) {
 #ifdef _OPENMP

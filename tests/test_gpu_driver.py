@@ -57,3 +57,39 @@ def test_driver_snapshots_match_the_abi_run(tmp_path):
         counts = load("atomCount")
         np.testing.assert_array_equal(counts, np.diff(sim.cell_starts()))
         assert load("simuatedTime")[0] == pytest.approx(frame * per * run.dt)
+
+
+def test_driver_snapshot_records_match_the_oracle(tmp_path):
+    """The driver's evapPos / evapVel / collisionCount datasets (recorded by the GPU step) and the
+    state frames, read back as (N, k, t) arrays, against the oracle's run with its own records:
+    the trapped workload's physics (Larmor, Majorana, knife, collisions) scaled to 20000 atoms on
+    24^3 cells, FP32, bit for bit."""
+    import oracle
+    from cudadsmc_b200.snapshots import read_snapshots
+    nc, n, prints, per = 24, 20000, 3, 6
+    out = tmp_path / "snap"
+    res = subprocess.run([DRIVER, str(nc), str(n), "--preset", "2", "--prints", str(prints), "--steps-per-print",
+                          str(per), "--out", str(out), "--seed", "7"], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr
+    data = read_snapshots(str(out))
+    run, c = preset(2)
+    c.cells[0] = c.cells[1] = c.cells[2] = nc
+    c.n_atoms = c.capacity = n
+    c.alpha = 3e6 / n
+    orc = oracle.Oracle(run, c)
+    orc.init_cloud(7)
+    orc.set_recording(3)
+    for frame in range(prints + 1):
+        if frame:
+            orc.step(per)
+        st = orc.get_state()
+        m = st["pos"].shape[0]
+        assert data["atomNumber"][0, 0, frame] == m
+        np.testing.assert_array_equal(data["positions"][:m, :, frame], st["pos"][:, :3].astype(np.float64))
+        np.testing.assert_array_equal(data["velocities"][:m, :, frame], st["vel"][:, :3].astype(np.float64))
+        ev = orc.evaporated(0)
+        np.testing.assert_array_equal(data["evapPos"][:, :, frame], ev["pos"])
+        np.testing.assert_array_equal(data["evapVel"][:, :, frame], ev["vel"])
+        np.testing.assert_array_equal(data["collisionCount"][:, 0, frame], orc.cell_collisions())
+    assert np.count_nonzero(ev["step"] >= 0) > 0  # atoms were lost
+    assert data["collisionCount"][:, 0, prints].sum() > 0
