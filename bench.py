@@ -45,8 +45,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=50)
+    ap.add_argument("--batched", action="store_true",
+                    help="time the 256-cloud batched ensemble instead, sharded over the ranks (torchrun)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-drift", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=20)
     ap.add_argument("--drift-steps", type=int, default=200)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
@@ -230,6 +234,35 @@ def fp32_drift(stream, atoms: int, steps: int) -> dict:
             "definition": "|FP32 - FP64| / |FP64| per diagnostic after the same steps from the same state"}
 
 
+def fp64_throughput(stream, atoms: int, steps: int, warmup: int) -> dict:
+    """The same workload with FP64 state and arithmetic (the reference's precision): device-timed
+    atom-steps/s over `steps` steps after `warmup`, for a like-precision point beside the FP32 line."""
+    import torch
+    from cudadsmc_b200 import FP64, Simulation
+    run, c = workload(atoms)
+    run.precision = FP64
+    s = Simulation(run, c)
+    s.set_stream(stream.cuda_stream)
+    s.init_cloud(run.seed)
+    s.step(warmup)
+    s.synchronize()
+    d0 = s.diagnostics()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    d1 = s.diagnostics()
+    s.set_profiling(True)
+    s.step(3)
+    kt = s.kernel_times()
+    s.close()
+    return {"value": (d1["atom_steps"] - d0["atom_steps"]) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
+            "steps": steps, "warmup": warmup, "dtype": "f64",
+            "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in kt.items()}}
+
+
 def batched_vs_sequential(stream, steps: int) -> dict:
     """256 clouds stepped together in one handle vs the same clouds as 256 single-cloud handles
     run one after another on the same stream; per-cloud results are identical (checked)."""
@@ -241,6 +274,7 @@ def batched_vs_sequential(stream, steps: int) -> dict:
     batch.set_stream(stream.cuda_stream)
     batch.init_cloud(run.seed)
     tile, _ = batch.autotune(3)
+    table = batch.autotune_table()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     d0 = batch.diagnostics()
     e0.record(stream)
@@ -273,10 +307,70 @@ def batched_vs_sequential(stream, steps: int) -> dict:
     atoms = d1["atom_steps"] - d0["atom_steps"]
     batch.close()
     return {"clouds": len(clouds), "atoms": int(sum(c.n_atoms for c in clouds)), "steps": steps,
-            "tile_atoms": tile, "batched_atom_steps_per_s": atoms / (ms_batch * 1e-3),
+            "tile_atoms": tile, "blocks_per_sm": table["chosen_blocks_per_sm"],
+            "autotune": [{"tile_atoms": t, "blocks_per_sm": b, "ms_per_step": round(m, 5)}
+                         for t, b, m in zip(table["tile_atoms"], table["blocks_per_sm"], table["ms_per_step"])],
+            "batched_atom_steps_per_s": atoms / (ms_batch * 1e-3),
             "sequential_atom_steps_per_s": atoms / (ms_seq * 1e-3), "speedup": ms_seq / ms_batch,
             "ms_per_step_batched": ms_batch / steps, "ms_per_step_sequential": ms_seq / steps,
             "identical_per_cloud_results": bool(same)}
+
+
+def run_batched_sharded(args):
+    """`--batched`: the 256-cloud batched ensemble, its clouds sharded over the ranks (each rank one
+    batched handle holding its shard), per-cloud diagnostics gathered with one NCCL all-reduce after
+    the timed steps; rank 0 checks them against the whole batch run on its own GPU."""
+    import torch
+    import torch.distributed as dist
+    from cudadsmc_b200 import Simulation
+    from cudadsmc_b200.replicas import GATHERED_FIELDS, run_sharded_batch
+    from cudadsmc_b200.workloads import batched_ensemble
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    run, clouds = batched_ensemble()
+
+    def make_sim(r, cl):
+        s = Simulation(r, cl)
+        s.set_stream(stream.cuda_stream)
+        return s
+
+    def timer(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    if ws > 1:
+        dist.barrier()
+    ms, atom_steps, table = run_sharded_batch(make_sim, run, clouds, args.batched_steps, run.seed, timer)
+    same = None
+    if rank == 0:
+        if ws > 1:
+            s = make_sim(run, clouds)
+            s.init_cloud(run.seed)
+            s.step(args.batched_steps)
+            s.synchronize()
+            same = all(float(s.diagnostics(k)[f]) == table[k][f] for k in range(len(clouds)) for f in GATHERED_FIELDS)
+            s.close()
+        line = {"metric": "atom-steps/s, 256-cloud batched ensemble", "value": atom_steps / (ms * 1e-3), "unit": UNIT,
+                "n_gpus": ws, "steps": args.batched_steps, "warmup": 0, "ms_per_step": ms / args.batched_steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded Philox clouds, no dataset)",
+                "config": {"workload": "batched-256-clouds", "clouds": len(clouds),
+                           "atoms": int(sum(c.n_atoms for c in clouds)),
+                           "parallelism": f"clouds sharded over {ws} ranks" if ws > 1 else "single-gpu"},
+                "identical_to_single_gpu_batch": same}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
 
 
 def run_reference(args):
@@ -303,6 +397,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched:
+        return run_batched_sharded(args)
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -441,6 +537,11 @@ def main():
     if rank == 0 and ws == 1 and not args.no_drift:
         drift = fp32_drift(stream, args.atoms, args.drift_steps)
 
+    # ------------------------------------------------------------------ FP64 throughput
+    fp64 = None
+    if rank == 0 and ws == 1 and not args.no_fp64:
+        fp64 = fp64_throughput(stream, args.atoms, args.fp64_steps, args.warmup)
+
     # ------------------------------------------------------------------ forward + adjoint vs plain
     adjoint = None
     if rank == 0 and ws == 1 and not args.no_adjoint:
@@ -458,7 +559,7 @@ def main():
                 "data": "synthetic (seeded Philox thermal cloud, no dataset)",
                 "config": config_of(args, ws),
                 "clocks": clk, "gpu_launches": args.steps * sim.launches_per_step(),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint, "fp32_drift": drift,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "adjoint": adjoint, "fp32_drift": drift, "fp64": fp64,
                 "n_alive_end": d1["n_alive"]}
         print(json.dumps(line), flush=True)
     sim.close()

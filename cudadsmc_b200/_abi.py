@@ -65,6 +65,8 @@ class RunParams(C.Structure):
         ("seed", C.c_uint64),
         ("tile_atoms", C.c_int32),
         ("use_graphs", C.c_int32),
+        ("step_blocks_per_sm", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
     def copy(self) -> "RunParams":

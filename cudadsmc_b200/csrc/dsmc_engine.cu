@@ -96,6 +96,7 @@ struct dsmc_handle {
     virtual void kernel_times(const char** names, double* ms, int64_t* launches, int cap, int* count) = 0;
     virtual int check_wait_timeout() = 0;
     virtual void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) = 0;
+    virtual void autotune_table(int32_t* T, int32_t* B, double* ms, int cap, int32_t* count, int32_t* chosen_b) = 0;
     virtual void adjoint_run(const dsmc_adj_params* p, dsmc_grad* g) = 0;
     virtual void adjoint_loss(const double* theta, double* parts, double* grad_e, double* grad_n) = 0;
     virtual void adjoint_export_spinors(double* psi0, int64_t atoms_cap) = 0;
@@ -159,6 +160,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // resident blocks of the tile kernels on the whole device (their grid-stride loops cover
     // any tile count, so a launch never needs more blocks than fit at once)
     int resident_step = 0, resident_permute = 0, resident_measure = 0;
+    int num_sms = 0, step_occ = 0;  // SMs, and step-kernel blocks that fit on one SM
+    int step_bps = 0;               // step-kernel blocks per SM in use (<= step_occ)
 
     Engine(const dsmc_params& r, const dsmc_cloud_params* clouds, int n) {
         run = r;
@@ -197,7 +200,10 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
                                 (int)smem_tile));
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB, false>, BLOCK, smem_tile));
 #endif
-        resident_step = nsm * std::max(occ, 1);
+        num_sms = nsm;
+        step_occ = std::max(occ, 1);
+        step_bps = (r.step_blocks_per_sm > 0 && r.step_blocks_per_sm < step_occ) ? r.step_blocks_per_sm : step_occ;
+        resident_step = nsm * step_bps;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, permute_pass<R>, 256, 0));
         resident_permute = nsm * std::max(occ, 1);
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, measure_tiles<R, 256>, 256, 0));
@@ -740,9 +746,12 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         profiling = on;
         for (int k = 0; k < kNumStepKernels; ++k) { prof_ms[k] = 0; prof_n[k] = 0; }
     }
-    // Times dsmc_step with each candidate tile size (the simulation advances meanwhile; results do
-    // not depend on the tiling) and keeps the fastest.  A new size takes effect one step after it
-    // is set (the tiling of a step is built by the scan of the step before).
+    // Times dsmc_step with each candidate launch shape (nominal tile size x step-kernel blocks per
+    // SM; the simulation advances meanwhile; results do not depend on the shape) and keeps the
+    // fastest.  A new tile size takes effect one step after it is set (the tiling of a step is
+    // built by the scan of the step before).
+    std::vector<int> tune_T, tune_B;
+    std::vector<double> tune_ms;
     void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
         if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
@@ -751,29 +760,50 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 #else
         const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, CAP - BLOCK - 16, 768, 960, 1024};
 #endif
-        int best = tile_nominal;
+        int best = tile_nominal, best_b = step_bps;
         double best_ms = 1e300;
         const bool prof = profiling;
         profiling = false;
-        for (int T : cands) {
-            if (!DSMC_STEP_WARP && T > CAP - 128) continue;
-            set_tile(T);
-            step(1);  // builds the tiling of size T
-            CU(cudaEventRecord(ev[0], stream));
-            step(steps_per_candidate);
-            CU(cudaEventRecord(ev[1], stream));
-            CU(cudaEventSynchronize(ev[1]));
-            float ms = 0;
-            CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-            const double per = ms / steps_per_candidate;
-            if (per < best_ms) { best_ms = per; best = T; }
+        tune_T.clear(); tune_B.clear(); tune_ms.clear();
+        for (int bps = step_occ; bps >= 1 && bps >= step_occ - 2; --bps) {
+            for (int T : cands) {
+                if (!DSMC_STEP_WARP && T > CAP - 128) continue;
+                set_shape(T, bps);
+                step(1);  // builds the tiling of size T
+                CU(cudaEventRecord(ev[0], stream));
+                step(steps_per_candidate);
+                CU(cudaEventRecord(ev[1], stream));
+                CU(cudaEventSynchronize(ev[1]));
+                float ms = 0;
+                CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+                const double per = ms / steps_per_candidate;
+                tune_T.push_back(T); tune_B.push_back(bps); tune_ms.push_back(per);
+                if (per < best_ms) { best_ms = per; best = T; best_b = bps; }
+            }
         }
-        set_tile(best);
+        set_shape(best, best_b);
         step(1);
         profiling = prof;
         check_err();
         if (chosen) *chosen = best;
         if (ms_per_step) *ms_per_step = best_ms;
+    }
+    void autotune_table(int32_t* T, int32_t* B, double* ms, int cap, int32_t* count, int32_t* chosen_b) override {
+        const int n = (int)tune_T.size();
+        for (int i = 0; i < std::min(n, cap); ++i) {
+            if (T) T[i] = tune_T[i];
+            if (B) B[i] = tune_B[i];
+            if (ms) ms[i] = tune_ms[i];
+        }
+        if (count) *count = n;
+        if (chosen_b) *chosen_b = step_bps;
+    }
+
+    // a launch shape: nominal tile size T and step-kernel blocks per SM
+    void set_shape(int T, int bps) {
+        step_bps = std::max(1, std::min(bps, step_occ));
+        resident_step = num_sms * step_bps;
+        set_tile(T);
     }
 
     void set_tile(int T) {
@@ -1304,4 +1334,9 @@ DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, 
                                    double* ms_per_step) {
     NEED_H;
     return guard(h, [&] { h->autotune(steps_per_candidate, tile_atoms, ms_per_step); });
+}
+DSMC_API dsmc_status dsmc_autotune_table(dsmc_handle* h, int32_t* tile_atoms, int32_t* blocks_per_sm, double* ms,
+                                         int32_t cap, int32_t* count, int32_t* chosen_blocks_per_sm) {
+    NEED_H;
+    return guard(h, [&] { h->autotune_table(tile_atoms, blocks_per_sm, ms, cap, count, chosen_blocks_per_sm); });
 }

@@ -27,7 +27,7 @@ EXPORTED_SYMBOLS = (
     "dsmc_batch_create", "dsmc_batch_step",
     "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
-    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_set_recording", "dsmc_get_evaporated", "dsmc_get_cell_collisions",
+    "dsmc_launches_per_step", "dsmc_autotune", "dsmc_autotune_table", "dsmc_set_recording", "dsmc_get_evaporated", "dsmc_get_cell_collisions",
     "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_loss_parts",
     "dsmc_adjoint_export", "dsmc_adjoint_export_spinors",
     "dsmc_sort_cells_noalloc", "dsmc_check_wait_timeout",
@@ -81,6 +81,8 @@ def load_library(path: str | None = None) -> C.CDLL:
                                           C.POINTER(C.c_double)]),
         "dsmc_adjoint_export_spinors": (i32, [vp, C.POINTER(C.c_double), i64]),
         "dsmc_set_recording": (i32, [vp, i32]),
+        "dsmc_autotune_table": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_double), i32, C.POINTER(i32),
+                                      C.POINTER(i32)]),
         "dsmc_get_evaporated": (i32, [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(i32),
                                       C.POINTER(i32), i64]),
         "dsmc_get_cell_collisions": (i32, [vp, C.POINTER(i32), i64, C.POINTER(i64)]),
@@ -326,3 +328,18 @@ class Simulation:
         ms = C.c_double()
         self._check(self.lib.dsmc_autotune(self._h, int(steps_per_candidate), C.byref(t), C.byref(ms)))
         return int(t.value), float(ms.value)
+
+    def autotune_table(self) -> dict:
+        """The last autotune's candidates: tile sizes, step-kernel blocks per SM, ms per step, and
+        the blocks per SM chosen."""
+        n, b = C.c_int32(), C.c_int32()
+        self._check(self.lib.dsmc_autotune_table(self._h, None, None, None, 0, C.byref(n), C.byref(b)))
+        T = np.zeros(max(n.value, 1), np.int32)
+        B = np.zeros(max(n.value, 1), np.int32)
+        ms = np.zeros(max(n.value, 1))
+        self._check(self.lib.dsmc_autotune_table(self._h, T.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 B.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 ms.ctypes.data_as(C.POINTER(C.c_double)), n.value, C.byref(n),
+                                                 C.byref(b)))
+        return {"tile_atoms": T[:n.value].tolist(), "blocks_per_sm": B[:n.value].tolist(),
+                "ms_per_step": ms[:n.value].tolist(), "chosen_blocks_per_sm": int(b.value)}

@@ -119,6 +119,8 @@ typedef struct dsmc_params {
     uint64_t seed;         /* Philox key for init (overridden by dsmc_init_cloud) and collisions */
     int32_t tile_atoms;    /* nominal atoms per tile (0 -> engine default) */
     int32_t use_graphs;    /* 1 -> replay captured CUDA graphs in dsmc_step (default), 0 -> plain launches */
+    int32_t step_blocks_per_sm; /* blocks of the step kernel per SM (0 -> as many as fit) */
+    int32_t reserved0;
 } dsmc_params;
 
 typedef struct dsmc_diag {
@@ -293,12 +295,18 @@ DSMC_API dsmc_status dsmc_adjoint_export(dsmc_handle* h, double* x0, double* v0,
                                          int64_t off_cap, int32_t* ij, double* nv, int64_t log_cap,
                                          int64_t* n_atoms, int64_t* n_log, int32_t* steps);
 
-/* Autotuner: times dsmc_step for each candidate tile size (atoms per tile, 128..CAP/2) over
- * steps_per_candidate steps and keeps the fastest; the simulation advances meanwhile (results do
- * not depend on the tiling).  Replaces no reference interface (the reference launches with
- * cudaOccupancyMaxPotentialBlockSize or 256*SMs x 512, CUDADSMC/src/main.cu:389-406). */
+/* Autotuner: times dsmc_step for each candidate launch shape -- nominal tile size (atoms per
+ * tile) x blocks of the step kernel per SM (how many warps walk tiles at once, which sets how much
+ * of the tiles' data is in flight in L2) -- over steps_per_candidate steps and keeps the fastest;
+ * the simulation advances meanwhile (results do not depend on the launch shape).  Replaces no
+ * reference interface (the reference launches with cudaOccupancyMaxPotentialBlockSize or
+ * 256*SMs x 512, CUDADSMC/src/main.cu:389-406). */
 DSMC_API dsmc_status dsmc_autotune(dsmc_handle* h, int32_t steps_per_candidate, int32_t* tile_atoms,
                                    double* ms_per_step);
+/* The last autotune's candidates and their ms per step (cap entries at most; *count receives the
+ * number of candidates timed) and the chosen blocks per SM. */
+DSMC_API dsmc_status dsmc_autotune_table(dsmc_handle* h, int32_t* tile_atoms, int32_t* blocks_per_sm, double* ms,
+                                         int32_t cap, int32_t* count, int32_t* chosen_blocks_per_sm);
 
 /* Sorts the n atoms of one cloud by cell without allocating any memory.  No counterpart in the
  * reference: it serves callers whose device memory is owned by another allocator (a PyTorch

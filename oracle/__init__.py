@@ -263,6 +263,9 @@ class Oracle:
     def step(self, n: int = 1):
         self._check(self.lib.oracle_step(self._h, int(n)))
 
+    def synchronize(self):
+        """The CPU steps complete before step() returns: nothing to wait for."""
+
     def diagnostics(self, cloud: int = -1) -> dict:
         d = Diag()
         self._check(self.lib.oracle_diag(self._h, int(cloud), C.byref(d)))

@@ -1,5 +1,8 @@
 """Replicas on CPU with world size 2 (gloo): clouds sharded over ranks evolve exactly as in one
-process, and the throughput aggregation takes the slowest rank and sums the work."""
+process, and the throughput aggregation takes the slowest rank and sums the work.  The sharded
+batched run (replicas.run_sharded_batch, the path of `bench.py --batched` under torchrun) is run
+with the oracle standing in for the engine's Python layer (it has the same interface), and every
+cloud's gathered diagnostics must equal a one-process run of the whole batch."""
 import os
 import socket
 
@@ -89,3 +92,40 @@ def test_two_rank_replicas_match_single_process():
             assert d[f] == r[f], (k, f)
         total += d["atom_steps"]
     assert steps == total
+
+
+def _sharded_worker(rank, world, port, q):
+    import torch.distributed as dist
+    import oracle
+    from cudadsmc_b200.replicas import run_sharded_batch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    run, cl = clouds(7)
+    ms, steps, table = run_sharded_batch(lambda r, c: oracle.Oracle(r, c), run, cl, steps=5, seed=77,
+                                         timer=lambda fn: (fn(), 3.0 * (rank + 1))[1])
+    q.put((rank, ms, steps, table))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_batch_gathers_every_cloud():
+    import oracle
+    from cudadsmc_b200.replicas import GATHERED_FIELDS, run_sharded_batch
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    run, cl = clouds(7)
+    ms1, steps1, ref = run_sharded_batch(lambda r, c: oracle.Oracle(r, c), run, cl, steps=5, seed=77)
+    for rank, ms, steps, table in got:
+        assert ms == 6.0  # the slowest rank
+        assert steps == steps1
+        for k in range(len(cl)):
+            for f in GATHERED_FIELDS:
+                assert table[k][f] == ref[k][f], (rank, k, f)
