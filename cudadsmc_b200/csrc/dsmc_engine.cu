@@ -63,17 +63,6 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #define DSMC_FP32_MINB 4
 #endif
 
-// the step kernel: one tile per warp (step_warp), or one tile per block staged in shared memory
-// (step_pass)
-#ifndef DSMC_STEP_WARP
-#define DSMC_STEP_WARP 1
-#endif
-// default nominal tile of step_warp (atoms): a little under a whole number of 32-atom passes
-#ifndef DSMC_WARP_TILE
-#define DSMC_WARP_TILE 240
-#endif
-constexpr int kMaxTileAtoms = 1 << 20;
-
 const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
 constexpr int kNumStepKernels = 4;
 
@@ -172,14 +161,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         // cell boundaries overshoots its nominal size by part of a cell
         // preferred nominal tile: three passes of the block, less a part of a cell for the snap
         // to cell boundaries (each step's scan lowers it where a cell is fuller than CAP - T + 1)
-#if DSMC_STEP_WARP
-        tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : DSMC_WARP_TILE;
-        if (tile_nominal > kMaxTileAtoms) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(kMaxTileAtoms)};
-#else
         tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP - BLOCK - 16;
         // a grid cell holds at most CAP - T + 1 atoms (DSMC_ERR_CELL_FULL beyond): T <= CAP - 128
         if (tile_nominal > CAP - 128) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP - 128)};
-#endif
         if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
         allocate();
@@ -189,17 +173,12 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         int dev = 0, nsm = 0, occ = 0;
         CU(cudaGetDevice(&dev));
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-#if DSMC_STEP_WARP
-        smem_tile = 0;
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_warp<R, BLOCK, MINB, false>, BLOCK, 0));
-#else
         smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int) + sizeof(uint16_t));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_pass<R, BLOCK, CAP, MINB, false>, BLOCK, smem_tile));
-#endif
         num_sms = nsm;
         step_occ = std::max(occ, 1);
         step_bps = (r.step_blocks_per_sm > 0 && r.step_blocks_per_sm < step_occ) ? r.step_blocks_per_sm : step_occ;
@@ -221,17 +200,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     }
 
     // blocks of the step kernel: no more than the tiles of the smallest tiling the scan may build
-    // need (one per warp for step_warp) nor than fit on the device at once
-    int step_grid() const {
-#if DSMC_STEP_WARP
-        const int tmin = args[0].tile_fill > 0 ? kMinTile : tile_nominal;
-        const long long tiles = (long long)capacity / tmin + nclouds + 2;
-        const long long blocks = (tiles + BLOCK / 32 - 1) / (BLOCK / 32);
-        return (int)std::max(1ll, std::min(blocks, (long long)resident_step));
-#else
-        return tile_grid(resident_step);
-#endif
-    }
+    // nor than the chosen number that run at once
+    int step_grid() const { return tile_grid(resident_step); }
 
     ~Engine() override {
         drop_graphs();
@@ -351,16 +321,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.scan_blk = scan_blk.p;
             A.cloud_first_blk = cloud_first_blk.p;
             A.nclouds = nclouds; A.total_cells = total_cells; A.nscan_blocks = nscan_blocks;
-            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal;
-#if DSMC_STEP_WARP
-            A.tile_cap = 1 << 29;  // nothing is staged: a tile holds cells of any size
-            A.tile_pass = 32;
-            A.tile_fill = run.tile_atoms > 0 ? 0 : resident_step * (BLOCK / 32);  // an explicit size is kept as given
-#else
-            A.tile_cap = CAP;
+            A.max_tiles = max_tiles; A.tile_nominal = tile_nominal; A.tile_cap = CAP;
             A.tile_pass = BLOCK;
             A.tile_fill = run.tile_atoms > 0 ? 0 : resident_step;  // an explicit size is kept as given
-#endif
             A.collide_every = run.collide_every; A.parity = p; A.init_mode = 0;
             A.seed = run.seed;
             A.capacity = capacity;
@@ -371,15 +334,10 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
         case 0:
-#if DSMC_STEP_WARP
-            if (nclouds == 1) step_warp<R, BLOCK, MINB, true><<<step_grid(), BLOCK, 0, stream>>>(A);
-            else step_warp<R, BLOCK, MINB, false><<<step_grid(), BLOCK, 0, stream>>>(A);
-#else
             if (nclouds == 1)
                 step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
-#endif
             break;
         case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
         case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
@@ -755,11 +713,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     void autotune(int steps_per_candidate, int32_t* chosen, double* ms_per_step) override {
         if (!initialised) throw Fail{DSMC_ERR_STATE, "autotune before init"};
         if (steps_per_candidate < 1) throw Fail{DSMC_ERR_INVALID, "steps_per_candidate must be >= 1"};
-#if DSMC_STEP_WARP
-        const int cands[] = {48, 80, 112, 144, 176, 208, 240, 304, 368, 496, 624, 752, 1008};
-#else
         const int cands[] = {128, 192, 240, 256, 384, 448, 480, 496, 512, CAP - BLOCK - 16, 768, 960, 1024};
-#endif
         int best = tile_nominal, best_b = step_bps;
         double best_ms = 1e300;
         const bool prof = profiling;
@@ -767,7 +721,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         tune_T.clear(); tune_B.clear(); tune_ms.clear();
         for (int bps = step_occ; bps >= 1 && bps >= step_occ - 2; --bps) {
             for (int T : cands) {
-                if (!DSMC_STEP_WARP && T > CAP - 128) continue;
+                if (T > CAP - 128) continue;
                 set_shape(T, bps);
                 step(1);  // builds the tiling of size T
                 CU(cudaEventRecord(ev[0], stream));

@@ -66,7 +66,7 @@ struct __align__(16) TilePartial {
 constexpr int ACC_BUCKETS = 16;
 
 // smallest nominal tile (sizes the tile tables: at most capacity / MIN_TILE + clouds + 2 tiles)
-constexpr int MIN_TILE = 32;
+constexpr int MIN_TILE = 128;
 struct __align__(16) CloudAccum {
     unsigned long long v2[3], B[3], ev2[3], eB[3];
     unsigned long long n_alive, n_maj, n_knife, coll, cand, pad[3];
@@ -592,6 +592,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 A.sigvrmax[c] = svm;
                 acc.coll += (unsigned)cr.accepted;
                 acc.cand += (unsigned)cr.candidates;
+                if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
             }
             __syncthreads();
         }
@@ -709,6 +710,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     add_limbs(s_lost.eB, fx_from(o.absB));
                     atomicAdd(o.fate == FATE_MAJORANA ? &s_lost.n_maj : &s_lost.n_knife, 1ull);
                     A.keys[j] = make_int2(-1, KIND_LOST);
+                    const unsigned id = lane_to_u32(q.w);
+                    if (A.rec_evap_pos && id < (unsigned)P.id_cap) {  // the snapshot record of a lost atom
+                        R4 ep, ev;
+                        ep.x = a.x; ep.y = a.y; ep.z = a.z; ep.w = lane_from_u32((uint32_t)step, R(0));
+                        ev.x = a.vx; ev.y = a.vy; ev.z = a.vz; ev.w = lane_from_u32((uint32_t)o.fate, R(0));
+                        A.rec_evap_pos[P.id_base + id] = ep;
+                        A.rec_evap_vel[P.id_base + id] = ev;
+                    }
                 }
             }
         }
@@ -738,356 +747,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         }
         __syncthreads();  // the staging arrays, red and s_lost are reused by the next tile
     }
-}
-
-// ---------------------------------------------------------------------------------------------
-// step_warp: the timestep of one tile per warp, with no shared-memory staging and no block
-// barriers.  Every warp walks its own tiles (grid-stride over warps), so the only
-// synchronisation is __syncwarp and the latency of one warp's loads is hidden by the other warps
-// of the SM rather than by a block-wide convoy.  Per tile:
-//   cell pass    the storage index of every atom (coalesced), its position (the gather's first
-//                round trip) and L2 prefetches of its velocity and spinor; the old cell of every
-//                atom, and the cells with two or more atoms (run starts of equal cells) listed in
-//                a small per-warp buffer, collided 32 at a time (one lane per cell) as it fills
-//   collisions   NTC in place on the velocities the previous step wrote, each atom reached
-//                through the permutation (the tile's cells are whole: no other warp touches them)
-//   motion       per 32 positions: Larmor + Verlet + Majorana + knife (+ MCWF) of each atom, its
-//                new cell, stayer / mover / lost, the new state written at its position, the sort
-//                key (a stayer's rank in its cell from warp ballots, with the run carried across
-//                the tile's passes in registers), leaver / incoming counts and mover records
-// Exact totals stay in registers until the warp's cloud changes or its last tile is done.
-// A tile holds whole cells however many atoms they have (nothing is staged), so no cell is too
-// full for the step.
-// ---------------------------------------------------------------------------------------------
-// the velocities of one cell's atoms, reached through the sorted order's permutation
-template <class R4> struct PermVel {
-    R4* vel;         // the state the previous step wrote (updated in place by the collisions)
-    const int* src;  // storage index of the cell's first sorted position
-    unsigned cap;    // storage slots (an index out of range, already flagged, reads slot 0)
-    __host__ __device__ __forceinline__ unsigned slot(uint32_t i) const {
-        const unsigned s = (unsigned)src[i];
-        return s < cap ? s : 0u;
-    }
-};
-template <class R4> __host__ __device__ __forceinline__ R4 vload(PermVel<R4> a, uint32_t i) { return a.vel[a.slot(i)]; }
-template <class R4> __host__ __device__ __forceinline__ void vstore(PermVel<R4> a, uint32_t i, const R4& v) {
-    a.vel[a.slot(i)] = v;
-}
-// records accepted collisions of one cell (adjoint runs): the atom ids of the pair and n^
-template <class R> struct PermCollisionLog {
-    typedef typename V4T<R>::type R4;
-    const R4* pos;
-    const int* src;  // storage index of the cell's first sorted position
-    unsigned cap_atoms;
-    int2* ij;
-    double* nv;
-    int* count;
-    int cap;
-    int* err;
-    template <class RR> __host__ __device__ void accept(uint32_t i, uint32_t j, RR nx, RR ny, RR nz) {
-#if defined(__CUDA_ARCH__)
-        const int slot = atomicAdd(count, 1);
-        if (slot < cap) {
-            ij[slot] = make_int2((int)lane_to_u32(pos[(unsigned)src[i] < cap_atoms ? src[i] : 0].w),
-                                 (int)lane_to_u32(pos[(unsigned)src[j] < cap_atoms ? src[j] : 0].w));
-            nv[3 * slot] = (double)nx;
-            nv[3 * slot + 1] = (double)ny;
-            nv[3 * slot + 2] = (double)nz;
-        } else {
-            atomicOr(err, EB_LOG_FULL);
-        }
-#endif
-    }
-};
-
-// a warp's totals into a bucket of its cloud (every lane calls; lane 0 adds), then cleared
-__device__ __forceinline__ void flush_warp_acc(StepAcc& acc, CloudAccum* bucket) {
-    warp_reduce_acc(acc);
-    if ((threadIdx.x & 31) == 0) {
-        TilePartial t;
-        zero_partial(t);
-        t.sum_v2 = acc.sum_v2;
-        t.sum_B = acc.sum_B;
-        t.n_alive = acc.n_alive;
-        t.coll = acc.coll;
-        t.cand = acc.cand;
-        accum_tile(bucket, t);
-    }
-    zero_acc(acc);
-}
-
-constexpr int WARP_HEADS = 64;  // per-warp list of cells to collide (flushed at 32)
-
-template <class R, int WBLOCK, int MINB, bool ONE>
-__global__ void __launch_bounds__(WBLOCK, MINB) step_warp(const __grid_constant__ Args<R> A) {
-    typedef typename V4T<R>::type R4;
-    constexpr int NW = WBLOCK / 32;
-    __shared__ int2 s_heads[NW][WARP_HEADS];  // (position in the tile, cell)
-    __shared__ CloudPhys<R> s_P[ONE ? 1 : NW];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    const CloudPhys<R>& P = ONE ? A.one : s_P[wl];
-    int2* const heads = s_heads[wl];
-
-    const int p = A.parity;
-    const int ntiles = A.ctl->ntiles[p];
-    const int nprev = A.ctl->n[p];
-    const int step = A.ctl->step[p];
-    const bool collide_now = (step % A.collide_every) == 0;
-    // MCWF phase of this step: bit 0 at the start of a collision period, bit 1 at its end
-    const uint32_t mcwf_phase = (collide_now ? 1u : 0u) | (((step + 1) % A.collide_every) == 0 ? 2u : 0u);
-    R4* const velw = const_cast<R4*>(A.vel_in);  // the collisions update it in place
-    const int gw = blockIdx.x * NW + wl;
-    const int nwarps = gridDim.x * NW;
-    const int bucket = gw & (ACC_BUCKETS - 1);
-    StepAcc acc;
-    zero_acc(acc);
-    int cur_cloud = -1;
-    R cut = R(0);
-
-    for (int b = gw; b < ntiles; b += nwarps) {
-        const int tb = A.tile_begin[b];
-        const int te = A.tile_begin[b + 1];
-        const int L = te - tb;
-        const int cloud = A.tile_cloud[b];
-        if (cloud != cur_cloud) {  // warp-uniform: the cloud's parameters and knife cut
-            if (cur_cloud >= 0) flush_warp_acc(acc, A.accum + cur_cloud * ACC_BUCKETS + bucket);
-            if (!ONE) {
-                __syncwarp();
-                const int* s = reinterpret_cast<const int*>(A.clouds + cloud);
-                int* d = reinterpret_cast<int*>(&s_P[wl]);
-                for (int i = lane; i < (int)(sizeof(CloudPhys<R>) / 4); i += 32) d[i] = s[i];
-                __syncwarp();
-            }
-            cut = knife_cut_for(P, A.cdyn[cloud].T_knife, step);
-            cur_cloud = cloud;
-        }
-        const bool box = (P.trap == TRAP_BOX);
-        CloudAccum* const bk = A.accum + cloud * ACC_BUCKETS + bucket;
-
-        if (L < 0 || te > nprev) {
-            // inconsistent tile tables: every atom in it leaves the simulation (flagged), so the
-            // cell counts stay consistent and every later kernel only touches indices it computed
-            if (lane == 0) atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            for (int t = lane; t < L && tb + t < nprev; t += 32) {
-                int s = A.src_in[tb + t];
-                s = (s >= 0 && s < A.capacity) ? s : 0;
-                const R4 q = A.pos_in[s];
-                atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
-                A.keys[tb + t] = make_int2(-1, KIND_LOST);
-            }
-            if (lane == 0) A.tile_ovf[b] = 0;
-            continue;
-        }
-        const bool split = L > 0 && A.tile_split[b] != 0;
-        const int* const src_t = A.src_in + tb;
-
-        // ---- cell pass: old cells, the cells to collide, the tile's data into L2
-        const bool do_coll = (P.flags & F_COLLIDE) && collide_now;
-        int nh = 0;           // cells listed (warp-uniform)
-        int prev_c = -1;      // cell at the previous pass's last position
-        int pend = -1;        // a run that starts at the previous pass's last position
-        int c_first = -1;
-        // collide the first `cnt` listed cells (one lane each), then drop them from the list
-        auto collide_listed = [&](int cnt) {
-            __syncwarp();
-            if (lane < cnt) {
-                const int2 h = heads[lane];
-                const int t = h.x, c = h.y;
-                const int c_beg = A.old_start[c], c_end = A.old_start[c + 1];
-                R svm = A.sigvrmax[c];
-                const int n = c_end - c_beg;
-                if (c_beg != tb + t || n > L - t) {  // cell not wholly inside this tile
-                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                } else if (n >= 2) {
-                    const PermVel<R4> va{velw, src_t + t, (unsigned)A.capacity};
-                    CollideResult<R> cr;
-                    if (A.clog_ij) {
-                        PermCollisionLog<R> lg{A.pos_in, src_t + t, (unsigned)A.capacity, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap,
-                                               &A.ctl->err};
-                        cr = collide_cell<R, PermVel<R4>, PermCollisionLog<R>>(va, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                                               (uint32_t)step, A.seed, &lg);
-                    } else {
-                        cr = collide_cell<R>(va, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
-                    }
-                    A.sigvrmax[c] = svm;
-                    acc.coll += (unsigned)cr.accepted;
-                    acc.cand += (unsigned)cr.candidates;
-                    if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
-                }
-            }
-            __syncwarp();
-            // move the rest of the list to its front
-            const int rest = nh - cnt;
-            int2 moved = make_int2(0, 0);
-            if (lane < rest) moved = heads[cnt + lane];
-            __syncwarp();
-            if (lane < rest) heads[lane] = moved;
-            nh = rest;
-        };
-        for (int base = 0; base < L; base += 32) {
-            const int t = base + lane;
-            const bool valid = t < L;
-            int c = -1;
-            if (valid) {
-                int s = src_t[t];
-                if (s < 0 || s >= A.capacity) {
-                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                    s = 0;
-                }
-                prefetch_l2(A.vel_in + s);
-                prefetch_l2(A.psi_in + s);
-                const R4 q = A.pos_in[s];
-                c = cell_of(P, q.x, q.y, q.z, box);
-            }
-            if (base == 0) c_first = __shfl_sync(FULL, c, 0);
-            if (do_coll) {
-                // a cell to collide begins where its run of equal cells starts and the next
-                // position is in the same cell (the overflow cell never collides)
-                int cp = __shfl_up_sync(FULL, c, 1);
-                const int cn = __shfl_down_sync(FULL, c, 1);
-                if (lane == 0) cp = prev_c;
-                const int c0 = __shfl_sync(FULL, c, 0);
-                if (pend >= 0 && c0 == prev_c) {  // the run from the previous pass's last position continues
-                    if (lane == 0) heads[nh] = make_int2(pend, prev_c);
-                    ++nh;
-                }
-                const bool start = valid && c != cp && c != P.ovf_cell;
-                const bool head = start && lane < 31 && cn == c;
-                const unsigned hm = __ballot_sync(FULL, head);
-                if (head) heads[nh + __popc(hm & lt)] = make_int2(t, c);
-                nh += __popc(hm);
-                pend = __shfl_sync(FULL, start ? t : -1, 31);
-                prev_c = __shfl_sync(FULL, c, 31);
-                if (nh >= 32) collide_listed(32);
-            }
-        }
-        while (nh > 0) collide_listed(nh < 32 ? nh : 32);
-        __syncwarp();  // the collisions' velocities are visible to every lane
-
-        // ---- motion: move, spin, evaporate and classify every atom once
-        int rc_cell = -1, rc_cnt = 0;  // the run at the previous pass's end: its cell, stayers so far
-        int n_ovf = 0;                 // stayers of the overflow cell in this tile
-        for (int base = 0; base < L; base += 32) {
-            const int t = base + lane;
-            const bool valid = t < L;
-            Atom<R> a;
-            AtomOut<R> o;
-            o.fate = FATE_ALIVE;
-            o.cell = 0;
-            bool stayer = false, mover = false;
-            int c_old = -1;
-            R4 q;
-            if (valid) {
-                int s = src_t[t];
-                s = (s >= 0 && s < A.capacity) ? s : 0;
-                q = A.pos_in[s];
-                const R4 v = velw[s];
-                const R4 w = A.psi_in[s];
-                a.x = q.x; a.y = q.y; a.z = q.z;
-                a.vx = v.x; a.vy = v.y; a.vz = v.z;
-                a.ur = w.x; a.ui = w.y; a.dr = w.z; a.di = w.w;
-                a.flags = lane_to_u32(v.w);
-                c_old = cell_of(P, q.x, q.y, q.z, box);
-                StepCtx sc;
-                sc.id = lane_to_u32(q.w);
-                sc.step = (uint32_t)step;
-                sc.cloud = (uint32_t)P.cloud_id;
-                sc.mcwf = mcwf_phase;
-                sc.seed = A.seed;
-                advance_atom(P, cut, a, o, sc);
-                const bool alive = (o.fate == FATE_ALIVE);
-                stayer = alive && (o.cell == c_old);
-                mover = alive && !stayer;
-                if (!(o.v2 == o.v2)) atomicOr(&A.ctl->err, EB_NAN);
-            }
-            // a stayer's rank among its cell's stayers in old order: cells are runs of consecutive
-            // positions, so it is the number of stayers since the start of its run in this pass,
-            // plus those of the run's earlier passes (carried)
-            const int cprev = __shfl_up_sync(FULL, c_old, 1);
-            const unsigned vmask = __ballot_sync(FULL, valid);
-            const unsigned hmask = __ballot_sync(FULL, valid && (lane == 0 || c_old != cprev));
-            const unsigned smask = __ballot_sync(FULL, stayer);
-            if (stayer) {
-                const unsigned le = lane == 31 ? FULL : ((2u << lane) - 1u);
-                const int run0 = 31 - __clz(hmask & le);
-                const int rank = __popc(smask & lt & (FULL << run0)) + ((run0 == 0 && c_old == rc_cell) ? rc_cnt : 0);
-                A.keys[tb + t] = stayer_key(split && c_old == c_first, b, c_old, rank, c_old == P.ovf_cell);
-            }
-            {
-                const int last = 31 - __clz(vmask);
-                const int r = 31 - __clz(hmask);
-                const int lc = __shfl_sync(FULL, c_old, last);
-                rc_cnt = __popc(smask & (FULL << r)) + ((r == 0 && lc == rc_cell) ? rc_cnt : 0);
-                rc_cell = lc;
-            }
-            n_ovf += __popc(__ballot_sync(FULL, stayer && c_old == P.ovf_cell));
-            // leavers of the old cell (movers and lost atoms), warp-aggregated
-            const bool leaver = valid && !stayer;
-            const unsigned lm = __ballot_sync(FULL, leaver);
-            if (leaver) {
-                const unsigned peers = __match_any_sync(lm, c_old);
-                if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
-            }
-            // movers: a slot in the step's mover list and a ticket in the target cell
-            const unsigned mm = __ballot_sync(FULL, mover);
-            int slot = 0;
-            if (mm) {
-                const int leader = __ffs(mm) - 1;
-                int sbase = 0;
-                if (lane == leader) sbase = atomicAdd(&A.ctl->movers[p], __popc(mm));
-                sbase = __shfl_sync(FULL, sbase, leader);
-                slot = sbase + __popc(mm & lt);
-            }
-            if (mover) {
-                const unsigned peers = __match_any_sync(mm, o.cell);
-                const int leader = __ffs(peers) - 1;
-                int tbase = 0;
-                if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
-                tbase = __shfl_sync(peers, tbase, leader);
-                const int ticket = tbase + __popc(peers & lt);
-                A.mrec[slot] = make_int4(o.cell, tb + t, ticket, cloud | (o.cell == P.ovf_cell ? MREC_OVF_CELL : 0));
-            }
-            if (valid) {
-                const int j = tb + t;
-                if (stayer || mover) {
-                    R4 qo, vo, so;
-                    qo.x = a.x; qo.y = a.y; qo.z = a.z; qo.w = q.w;
-                    vo.x = a.vx; vo.y = a.vy; vo.z = a.vz; vo.w = lane_from_u32(a.flags, R(0));
-                    so.x = a.ur; so.y = a.ui; so.z = a.dr; so.w = a.di;
-                    A.pos_out[j] = qo;
-                    A.vel_out[j] = vo;
-                    A.psi_out[j] = so;
-                    acc.n_alive += 1u;
-                    acc.sum_v2 += fx_from(o.v2);
-                    acc.sum_B += fx_from(o.absB);
-                    if (mover) A.keys[j] = make_int2(slot, KIND_MOVE);
-                } else {
-                    add_limbs(bk->ev2, fx_from(o.v2));
-                    add_limbs(bk->eB, fx_from(o.absB));
-                    atomicAdd(o.fate == FATE_MAJORANA ? &bk->n_maj : &bk->n_knife, 1ull);
-                    A.keys[j] = make_int2(-1, KIND_LOST);
-                    const unsigned id = lane_to_u32(q.w);
-                    if (A.rec_evap_pos && id < (unsigned)P.id_cap) {
-                        R4 ep, ev;
-                        ep.x = a.x; ep.y = a.y; ep.z = a.z; ep.w = lane_from_u32((uint32_t)step, R(0));
-                        ev.x = a.vx; ev.y = a.vy; ev.z = a.vz; ev.w = lane_from_u32((uint32_t)o.fate, R(0));
-                        A.rec_evap_pos[P.id_base + id] = ep;
-                        A.rec_evap_vel[P.id_base + id] = ev;
-                    }
-                }
-            }
-        }
-        if (lane == 0) {
-            A.tile_ovf[b] = n_ovf;
-            if (n_ovf > 0) {
-                const int i = atomicAdd(&A.ctl->novf[p], 1);
-                if (i < A.max_tiles) A.ovf_list[i] = b;
-            }
-        }
-    }
-    if (cur_cloud >= 0) flush_warp_acc(acc, A.accum + cur_cloud * ACC_BUCKETS + bucket);
 }
 
 // ---------------------------------------------------------------------------------------------
