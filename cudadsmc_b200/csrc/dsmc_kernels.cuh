@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     A.vel_out[j] = vo;
                     A.psi_out[j] = so;
                     acc.n_alive += 1u;
-                    acc.sum_v2 += fx_from(o.v2);
+                    acc.sum_v2 += fx_from_magnitude(o.v2);  // v^2 >= 0: fx_from without the sign
                     acc.sum_B += fx_from(o.absB);
                     if (stayer) {
                         if (c_old == P.ovf_cell) atomicAdd(&s_ovf, 1);
