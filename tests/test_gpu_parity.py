@@ -296,6 +296,12 @@ def test_autotune_changes_speed_not_results():
     orc.init_cloud(17)
     tile, ms = sim.autotune(2)
     assert 128 <= tile <= 1024 and ms > 0
+    # the table holds every (tile size, blocks per SM) candidate timed; the choice is its fastest
+    table = sim.autotune_table()
+    assert len(table["tile_atoms"]) >= 20 and len(set(table["blocks_per_sm"])) >= 2
+    best = int(np.argmin(table["ms_per_step"]))
+    assert table["tile_atoms"][best] == tile and table["blocks_per_sm"][best] == table["chosen_blocks_per_sm"]
+    assert table["ms_per_step"][best] == ms
     orc.step(sim.diagnostics()["step"])
     assert_same(sim, orc)
     sim.step(3)
