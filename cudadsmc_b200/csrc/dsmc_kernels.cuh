@@ -1488,13 +1488,22 @@ __device__ __forceinline__ int find_cloud(const int* off, int nclouds, int i) {
 template <class R>
 __global__ void __launch_bounds__(256) fs_cells(SortArgs<R> S, Args<R> A) {
     const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= S.n) return;
-    const int k = find_cloud<R>(S.cloud_atom_off, S.nclouds, i);
-    const CloudPhys<R>& P = A.clouds[k];
-    const auto q = S.pos_src[i];
-    const int c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);
-    S.cell[i] = c;
-    atomicAdd(&A.Ic[c], 1);
+    const bool valid = i < S.n;
+    int c = -1;
+    if (valid) {
+        const int k = find_cloud<R>(S.cloud_atom_off, S.nclouds, i);
+        const CloudPhys<R>& P = A.clouds[k];
+        const auto q = S.pos_src[i];
+        c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);
+        S.cell[i] = c;
+    }
+    // one atomic per cell and warp: input that is already nearly sorted (a state read back from
+    // the engine) has runs of equal cells
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+        const unsigned peers = __match_any_sync(vm, c);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&A.Ic[c], __popc(peers));
+    }
 }
 
 template <class R>

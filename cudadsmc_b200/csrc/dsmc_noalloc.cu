@@ -137,11 +137,19 @@ __global__ void k_zero(int* a, int n) {
 template <class R4, class R>
 __global__ void k_cells(const R4* pos, int n, CloudPhys<R> P, int* scratch) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n) return;
-    const R4 q = pos[i];
-    const int c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);  // ids start at 0 (cell_base 0)
-    scratch[kOffKeyA + i] = c;
-    atomicAdd(&scratch[kOffCounts + c], 1);
+    const bool valid = i < n;
+    int c = -1;
+    if (valid) {
+        const R4 q = pos[i];
+        c = cell_of(P, q.x, q.y, q.z, P.trap == TRAP_BOX);  // ids start at 0 (cell_base 0)
+        scratch[kOffKeyA + i] = c;
+    }
+    // one atomic per cell and warp (runs of equal cells in nearly sorted input)
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+        const unsigned peers = __match_any_sync(vm, c);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&scratch[kOffCounts + c], __popc(peers));
+    }
 }
 
 // exclusive scan of in[0..n) into out[0..n) (3 kernels, block sums in the scratch)
