@@ -44,6 +44,8 @@ DSMC_HD float xfma(float a, float b, float c) { return fmaf(a, b, c); }
 DSMC_HD double xfma(double a, double b, double c) { return fma(a, b, c); }
 DSMC_HD float xsqrt(float x) { return sqrtf(x); }
 DSMC_HD double xsqrt(double x) { return sqrt(x); }
+DSMC_HD float xabs(float x) { return fabsf(x); }
+DSMC_HD double xabs(double x) { return fabs(x); }
 DSMC_HD float xfloor(float x) { return floorf(x); }
 DSMC_HD double xfloor(double x) { return floor(x); }
 DSMC_HD float xceil(float x) { return ceilf(x); }
@@ -199,7 +201,19 @@ DSMC_HD uint32_t index_below(uint32_t r, uint32_t n) {
 DSMC_HD void xsincos(float x, float* s, float* c) {
     const float two_over_pi = 0x1.45f306p-1f;
     const float p1 = 0x1.922p+0f, p2 = -0x1.2aep-18f, p3 = -0x1.de973ep-31f;
-    float k = xrint(x * two_over_pi);
+    // k = x 2/pi rounded to the nearest integer (ties to even) by adding and removing 1.5 * 2^23:
+    // exact for |x 2/pi| < 2^22, and the sum's low mantissa bits are then k modulo 4 (1.5 * 2^23
+    // is a multiple of 4) -- two adds instead of a rounding and a conversion on the slow pipe
+    const float t = x * two_over_pi;
+    const float shifter = 12582912.0f;
+    float k, km;
+    if (xabs(t) < 4194304.0f) {
+        km = t + shifter;
+        k = km - shifter;
+    } else {
+        k = xrint(t);
+        km = 0.0f;
+    }
     float r = xfma(-k, p1, x);
     r = xfma(-k, p2, r);
     r = xfma(-k, p3, r);
@@ -214,7 +228,7 @@ DSMC_HD void xsincos(float x, float* s, float* c) {
     p = fma2(rr, p, v2(-1.66666667e-1f, -0.5f));
     const V2<float> sc = fma2(v2(r * r2, r2), p, v2(r, 1.0f));
     const float sr = sc.x, cr = sc.y;
-    int q = ((int)k) & 3;
+    int q = xabs(t) < 4194304.0f ? (int)(f2u(km) & 3u) : (((int)k) & 3);
     float ss = (q & 1) ? cr : sr;
     float cc = (q & 1) ? sr : cr;
     if (q == 1 || q == 2) cc = -cc;
@@ -226,7 +240,18 @@ DSMC_HD void xsincos(float x, float* s, float* c) {
 DSMC_HD void xsincos(double x, double* s, double* c) {
     const double two_over_pi = 0x1.45f306dc9c883p-1;
     const double p1 = 0x1.921fb58p+0, p2 = -0x1.dde974p-27, p3 = 0x1.1a62633145c07p-54;
-    double k = xrint(x * two_over_pi);
+    // nearest integer by adding and removing 1.5 * 2^52 (exact for |x 2/pi| < 2^51; the sum's low
+    // mantissa bits are k modulo 4), as in the float version
+    const double t = x * two_over_pi;
+    const double shifter = 6755399441055744.0;
+    double k, km;
+    if (xabs(t) < 2251799813685248.0) {
+        km = t + shifter;
+        k = km - shifter;
+    } else {
+        k = xrint(t);
+        km = 0.0;
+    }
     double r = xfma(-k, p1, x);
     r = xfma(-k, p2, r);
     r = xfma(-k, p3, r);
@@ -249,7 +274,7 @@ DSMC_HD void xsincos(double x, double* s, double* c) {
     pc = xfma(r2, pc, -4.1666666666666667e-2);                                // -1/4!
     pc = xfma(r2, pc, 0.5);                                                   // 1/2!
     double cr = xfma(-r2, pc, 1.0);
-    int q = ((int)(long long)k) & 3;
+    int q = xabs(t) < 2251799813685248.0 ? (int)(d2u(km) & 3ull) : (((int)(long long)k) & 3);
     double ss = (q & 1) ? cr : sr;
     double cc = (q & 1) ? sr : cr;
     if (q == 1 || q == 2) cc = -cc;
@@ -278,6 +303,22 @@ DSMC_HD double xrsqrt(double x) {
     y = y * xfma(-(hx * y), y, 1.5);
     y = y * xfma(-(hx * y), y, 1.5);
     return y;
+}
+
+// 1/sqrt(n2) for the squared norm of a spinor the step keeps normalised: a unitary rotation moves
+// n2 from 1 only by rounding, so with d = 1 - n2 (exact for n2 near 1) the series
+// 1/sqrt(1 - d) = 1 + d/2 + 3 d^2/8 + ..., cut after d^2, is exact to well under an ulp when
+// |d| < 2^-12 (float; 2^-18 for double); anything further from 1 takes the Newton rsqrt.  Two
+// dependent multiply-adds in place of the rsqrt's chain on the step's critical path.
+DSMC_HD float inv_norm(float n2) {
+    const float d = 1.0f - n2;
+    if (xabs(d) < 0x1p-12f) return xfma(d, xfma(d, 0.375f, 0.5f), 1.0f);
+    return xrsqrt(n2);
+}
+DSMC_HD double inv_norm(double n2) {
+    const double d = 1.0 - n2;
+    if (xabs(d) < 0x1p-18) return xfma(d, xfma(d, 0.375, 0.5), 1.0);
+    return xrsqrt(n2);
 }
 
 // natural log for normal positive x
@@ -661,7 +702,7 @@ DSMC_HD void advance_atom(const CloudPhys<R>& P, R cut_v2, Atom<R>& a, AtomOut<R
         V2<R> nd = fma2(td, v2s(s), mul2(d, v2s(c)));
         if (P.flags & F_NORMALISE) {
             const V2<R> q = fma2(nd, nd, mul2(nu, nu));
-            const R inv = xrsqrt(q.x + q.y);
+            const R inv = inv_norm(q.x + q.y);
             nu = mul2(nu, v2s(inv));
             nd = mul2(nd, v2s(inv));
         }
