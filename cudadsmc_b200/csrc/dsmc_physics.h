@@ -286,21 +286,27 @@ DSMC_HD void xsincos(double x, double* s, double* c) {
 // 1/sqrt(x) for positive normal x by Newton's iteration y <- y (3/2 - x y^2 / 2) from the
 // bit-level initial guess of Lomont, "Fast inverse square root" (2003): 3 iterations in float,
 // 5 in double reach the working precision (within ~2 ulp; deterministic, not correctly rounded).
+// Newton steps y <- y (3/2 - x y^2 / 2) from Lomont's initial guess.  The early steps are written
+// as 1.5 y - (x/2 y) y^2, whose three products are independent and joined by one multiply-add (two
+// dependent operations instead of three: the field's rsqrt is on the step's critical path); the
+// last keeps the form y (1.5 - (x/2 y) y), which rounds less.
+DSMC_HD float rsqrt_step(float y, float hx) { return xfma(-(hx * y), y * y, 1.5f * y); }
+DSMC_HD double rsqrt_step(double y, double hx) { return xfma(-(hx * y), y * y, 1.5 * y); }
 DSMC_HD float xrsqrt(float x) {
     float y = u2f(0x5f375a86u - (f2u(x) >> 1));
     const float hx = 0.5f * x;
-    y = y * xfma(-(hx * y), y, 1.5f);
-    y = y * xfma(-(hx * y), y, 1.5f);
+    y = rsqrt_step(y, hx);
+    y = rsqrt_step(y, hx);
     y = y * xfma(-(hx * y), y, 1.5f);
     return y;
 }
 DSMC_HD double xrsqrt(double x) {
     double y = u2d(0x5fe6eb50c7b537a9ull - (d2u(x) >> 1));
     const double hx = 0.5 * x;
-    y = y * xfma(-(hx * y), y, 1.5);
-    y = y * xfma(-(hx * y), y, 1.5);
-    y = y * xfma(-(hx * y), y, 1.5);
-    y = y * xfma(-(hx * y), y, 1.5);
+    y = rsqrt_step(y, hx);
+    y = rsqrt_step(y, hx);
+    y = rsqrt_step(y, hx);
+    y = rsqrt_step(y, hx);
     y = y * xfma(-(hx * y), y, 1.5);
     return y;
 }
