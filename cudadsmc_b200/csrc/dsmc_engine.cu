@@ -199,6 +199,12 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         return std::max(1, std::min(bound, resident));
     }
 
+    // mover-list entries beyond the capacity: each resident step_pass warp (at most 64 per SM) may
+    // leave up to MV_CHUNK - 1 slots of its last chunk unused
+    int num_sms_dev = 0;
+    int mover_slack() const { return num_sms_dev * 64 * MV_CHUNK; }
+    int mover_list_size() const { return (int)std::min<int64_t>((int64_t)capacity + mover_slack(), INT32_MAX); }
+
     // blocks of the step kernel: no more than the tiles of the smallest tiling the scan may build
     // nor than the chosen number that run at once
     int step_grid() const { return tile_grid(resident_step); }
@@ -238,6 +244,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     }
 
     void allocate() {
+        {
+            int dev = 0;
+            CU(cudaGetDevice(&dev));
+            CU(cudaDeviceGetAttribute(&num_sms_dev, cudaDevAttrMultiProcessorCount, dev));
+        }
         for (int i = 0; i < 2; ++i) {
             pos[i].alloc(capacity); vel[i].alloc(capacity); psi[i].alloc(capacity);
             src[i].alloc(capacity);
@@ -254,7 +265,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(Lc.p, 0, total_cells * sizeof(int)));
         CU(cudaMemset(Ic.p, 0, total_cells * sizeof(int)));
         in_list.alloc(capacity);
-        mrec.alloc(capacity);
+        mrec.alloc(mover_list_size());
         keys.alloc(std::max(capacity, 2048));  // >= 4096 ints: the full sort's count table
         tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles); ovf_list.alloc(max_tiles);
         sigvrmax.alloc(total_cells);
@@ -309,7 +320,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.old_start = start[p].p; A.new_start = start[q].p;
             A.Lc = Lc.p; A.Ic = Ic.p; A.mover_base = mover_base.p;
             A.sigvrmax = sigvrmax.p;
-            A.mrec = mrec.p; A.in_list = in_list.p;
+            A.mrec = mrec.p; A.mrec_cap = mover_list_size(); A.in_list = in_list.p;
             A.tile_begin = tile_begin[p].p; A.tile_cloud = tile_cloud[p].p; A.tile_split = tile_split[p].p;
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
             A.tile_split_next = tile_split[q].p;

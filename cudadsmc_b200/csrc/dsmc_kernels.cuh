@@ -52,7 +52,12 @@ enum : int {
     EB_LOG_FULL = 128
 };
 
-constexpr int MOVER_GRID = 148 * 8;  // grid-stride kernels over the mover list
+constexpr int MOVER_GRID = 148 * 8;
+// step_pass hands out mover-list slots from per-warp chunks of MV_CHUNK, each reserved with one
+// atomic on the step's mover counter (one contended atomic per 64 movers instead of one per warp
+// pass with a mover); a warp's last chunk leaves up to MV_CHUNK - 1 unused slots, marked as holes
+// (cell -1), so the list holds up to capacity + MV_CHUNK x (resident step_pass warps) entries
+constexpr int MV_CHUNK = 64;  // grid-stride kernels over the mover list
 
 struct __align__(16) TilePartial {
     i128 sum_v2, sum_B, evap_v2, evap_B;
@@ -138,6 +143,7 @@ template <class R> struct Args {
     int* mover_base;
     R* sigvrmax;
     int4* mrec;
+    int mrec_cap;  // entries of the mover list (atoms of capacity + the warps' chunk slack)
     int* in_list;
     const int* tile_begin;
     const int* tile_cloud;
@@ -465,6 +471,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         s_lost = z;  // ordered before first use by the barrier after the first load_cloud
     }
 
+    // this warp's chunk of mover-list slots: the next free one and the chunk's end
+    int mv_next = 0, mv_end = 0;
     // tiles in a grid-stride loop: the launch size only sets how many tiles run at once
     for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
         const int tb = A.tile_begin[b];
@@ -668,24 +676,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 const unsigned peers = __match_any_sync(lm, c_old);
                 if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
             }
-            // movers: a slot in the step's mover list and a ticket in the target cell
+            // movers: a slot in the step's mover list from the warp's chunk (the chunk's last slots, then
+            // a new chunk when this pass's movers do not fit), and one more incoming atom for the
+            // target cell, counted without waiting for the result (permute_pass hands out the
+            // cells' incoming slots)
             const unsigned mm = __ballot_sync(0xffffffffu, mover);
             int slot = 0;
             if (mm) {
-                const int leader = __ffs(mm) - 1;
-                int sbase = 0;
-                if (lane == leader) sbase = atomicAdd(&A.ctl->movers[p], __popc(mm));
-                sbase = __shfl_sync(0xffffffffu, sbase, leader);
-                slot = sbase + __popc(mm & ((1u << lane) - 1u));
+                const int need = __popc(mm);
+                const int rank = __popc(mm & ((1u << lane) - 1u));
+                const int left = mv_end - mv_next;
+                if (need <= left) {
+                    slot = mv_next + rank;
+                    mv_next += need;
+                } else {
+                    int nb = 0;
+                    if (lane == 0) nb = atomicAdd(&A.ctl->movers[p], MV_CHUNK);
+                    nb = __shfl_sync(0xffffffffu, nb, 0);
+                    slot = rank < left ? mv_next + rank : nb + (rank - left);
+                    mv_next = nb + (need - left);
+                    mv_end = nb + MV_CHUNK;
+                }
             }
             if (mover) {
-                const unsigned peers = __match_any_sync(mm, o.cell);
-                const int leader = __ffs(peers) - 1;
-                int tbase = 0;
-                if (lane == leader) tbase = atomicAdd(&A.Ic[o.cell], __popc(peers));
-                tbase = __shfl_sync(peers, tbase, leader);
-                const int ticket = tbase + __popc(peers & ((1u << lane) - 1u));
-                A.mrec[slot] = make_int4(o.cell, tb + t, ticket, cloud | (o.cell == P.ovf_cell ? MREC_OVF_CELL : 0));
+                atomicAdd(&A.Ic[o.cell], 1);
+                if (slot < A.mrec_cap)
+                    A.mrec[slot] = make_int4(o.cell, tb + t, 0, cloud | (o.cell == P.ovf_cell ? MREC_OVF_CELL : 0));
+                else
+                    atomicOr(&A.ctl->err, EB_CAPACITY);
             }
             if (valid) {
                 const int j = tb + t;
@@ -747,6 +765,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         }
         __syncthreads();  // the staging arrays, red and s_lost are reused by the next tile
     }
+    for (int i = mv_next + lane; i < mv_end; i += 32)  // the last chunk's unused slots
+        if (i < A.mrec_cap) A.mrec[i] = make_int4(-1, -1, -1, -1);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -884,11 +904,13 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             }
         }
     }
-    // incoming movers: each writes its old position into its cell's incoming slots (ticket order)
-    const int m = A.ctl->movers[p];
+    // incoming movers: each takes a slot in its cell's incoming list (the scan cleared the cell's
+    // incoming count, which now counts the slots handed out) and writes its old position there
+    const int m = min(A.ctl->movers[p], A.mrec_cap);
     for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
         const int4 r = A.mrec[i];
-        const int slot = A.mover_base[r.x] + r.z;
+        if (r.x < 0) continue;  // an unused slot of a warp's chunk
+        const int slot = A.mover_base[r.x] + atomicAdd(&A.Ic[r.x], 1);
         if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
         else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
@@ -1395,10 +1417,12 @@ __global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
 // starts, every overflow-cell mover checks its own position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
-    const int m = A.ctl->movers[A.parity];
+    const int m = min(A.ctl->movers[A.parity], A.mrec_cap);
     const bool tiles = A.ctl->tiles_built[1 - A.parity] == 0;  // the coming tiling is built here
     for (int i = blockIdx.x * 256 + threadIdx.x; i < m; i += gridDim.x * 256) {
         const int4 r = A.mrec[i];
+        if (r.x < 0) continue;  // an unused slot of a warp's chunk
+        A.Ic[r.x] = 0;  // the next step's incoming count starts at zero (every mover of the cell writes it)
         const int lo = A.mover_base[r.x];
         const int hi = A.new_start[r.x + 1];
         if (lo < 0 || hi > A.capacity || lo > hi) {
