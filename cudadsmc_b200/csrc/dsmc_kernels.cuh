@@ -669,13 +669,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     }
                 }
             }
-            // leavers of the old cell (movers and lost atoms), warp-aggregated
-            const bool leaver = valid && !stayer;
-            const unsigned lm = __ballot_sync(0xffffffffu, leaver);
-            if (leaver) {
-                const unsigned peers = __match_any_sync(lm, c_old);
-                if (lane == __ffs(peers) - 1) atomicAdd(&A.Lc[c_old], __popc(peers));
-            }
+            // leavers of the old cell (movers and lost atoms): one fire-and-forget atomic each (a
+            // warp pass rarely has two leavers of one cell, so aggregating them costs more than it saves)
+            if (valid && !stayer) atomicAdd(&A.Lc[c_old], 1);
             // movers: a slot in the step's mover list from the warp's chunk (the chunk's last slots, then
             // a new chunk when this pass's movers do not fit), and one more incoming atom for the
             // target cell, counted without waiting for the result (permute_pass hands out the
