@@ -669,6 +669,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     }
                 }
             }
+            // stayers of the overflow cell in this tile (one shared atomic per warp pass)
+            const unsigned om = __ballot_sync(FULL, stayer && c_old == P.ovf_cell);
+            if (om && lane == 0) atomicAdd(&s_ovf, __popc(om));
             // leavers of the old cell (movers and lost atoms): one fire-and-forget atomic each (a
             // warp pass rarely has two leavers of one cell, so aggregating them costs more than it saves)
             if (valid && !stayer) atomicAdd(&A.Lc[c_old], 1);
@@ -714,11 +717,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     acc.n_alive += 1u;
                     acc.sum_v2 += fx_from_magnitude(o.v2);  // v^2 >= 0: fx_from without the sign
                     acc.sum_B += fx_from(o.absB);
-                    if (stayer) {
-                        if (c_old == P.ovf_cell) atomicAdd(&s_ovf, 1);
-                    } else {
-                        A.keys[j] = make_int2(slot, KIND_MOVE);
-                    }
+                    if (!stayer) A.keys[j] = make_int2(slot, KIND_MOVE);
                 } else {
                     add_limbs(s_lost.ev2, fx_from(o.v2));
                     add_limbs(s_lost.eB, fx_from(o.absB));
