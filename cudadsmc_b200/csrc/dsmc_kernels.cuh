@@ -12,7 +12,8 @@
 //                    tile's cells in shared memory, then move + spin + evaporate every atom once,
 //                    write the new state at its current position j (coalesced) with an 8-byte
 //                    sort key (stayers ranked in their cell by warp ballots), count leavers L[c] /
-//                    incoming movers I[c], list movers, and add exact totals into per-cloud
+//                    incoming movers I[c] (fire-and-forget atomics), list movers in per-warp
+//                    chunks of the step's mover list, and add exact totals into per-cloud
 //                    buckets.  The only heavy pass: the step is computed once.
 //   scan_cells       one-pass scan (decoupled look-back) of the per-cell counts n_c - L_c + I_c:
 //                    new start[], movers' base slots, largest cell, the next tiling of a single
@@ -116,8 +117,8 @@ struct Ctl {
 enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2, KIND_OVF = 3 };
 constexpr int KEY_OVF_CELL = 4;
 constexpr int KEY_RANK_SHIFT = 3;
-// mover records written by step_pass: .x = target cell, .y = old position, .z = ticket in the
-// target cell, .w = cloud | MREC_OVF_CELL when the target is the cloud's overflow cell
+// mover records written by step_pass: .x = target cell (-1: an unused slot of a warp's chunk),
+// .y = old position, .z unused, .w = cloud | MREC_OVF_CELL when the target is the cloud's overflow cell
 constexpr int MREC_OVF_CELL = 1 << 30;
 
 __device__ __forceinline__ int2 stayer_key(bool split_ovf, int tile, int cell, int rank, bool ovf_cell) {
