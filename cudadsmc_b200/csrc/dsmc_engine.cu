@@ -1151,6 +1151,10 @@ DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params
         g_create_error = "dsmc_create: null argument or nclouds < 1";
         return DSMC_ERR_INVALID;
     }
+    if (nclouds > KEY_MAX_CLOUDS) {
+        g_create_error = "dsmc_create: at most " + std::to_string(KEY_MAX_CLOUDS) + " clouds per handle";
+        return DSMC_ERR_INVALID;
+    }
     *out = nullptr;
     try {
         int dev_count = 0;

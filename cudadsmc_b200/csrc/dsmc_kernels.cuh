@@ -108,22 +108,30 @@ struct Ctl {
     unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
 };
 
-// keys written by step_pass, one per atom position: .y = kind | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT)
+// keys written by step_pass, one per atom position:
+//   .y = kind | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT) | (cloud << KEY_CLOUD_SHIFT)
 //   KIND_STAY  .x = cell, rank among the cell's stayers before it (the cell starts in this tile)
 //   KIND_OVF   .x = tile, rank among the tile's stayers of the cloud's overflow cell, which
 //              started in an earlier tile (the only cell that may be split across tiles)
 //   KIND_MOVE  .x = slot in the step's mover list;  KIND_LOST  .x = -1
 //   KEY_OVF_CELL: the stayer's cell is its cloud's overflow cell (always set with KIND_OVF)
+// A stayer's rank counts positions of its tile, so it is below the staging capacity (< 2^11); the
+// cloud rides along so that permute_pass need not search for the cell's cloud.
 enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2, KIND_OVF = 3 };
 constexpr int KEY_OVF_CELL = 4;
 constexpr int KEY_RANK_SHIFT = 3;
+constexpr int KEY_RANK_BITS = 11;
+constexpr int KEY_RANK_MASK = (1 << KEY_RANK_BITS) - 1;
+constexpr int KEY_CLOUD_SHIFT = KEY_RANK_SHIFT + KEY_RANK_BITS;
+constexpr int KEY_MAX_CLOUDS = 1 << (31 - KEY_CLOUD_SHIFT);  // clouds a handle may hold
 // mover records written by step_pass: .x = target cell (-1: an unused slot of a warp's chunk),
 // .y = old position, .z unused, .w = cloud | MREC_OVF_CELL when the target is the cloud's overflow cell
 constexpr int MREC_OVF_CELL = 1 << 30;
 
-__device__ __forceinline__ int2 stayer_key(bool split_ovf, int tile, int cell, int rank, bool ovf_cell) {
-    return split_ovf ? make_int2(tile, KIND_OVF | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT))
-                     : make_int2(cell, KIND_STAY | (ovf_cell ? KEY_OVF_CELL : 0) | (rank << KEY_RANK_SHIFT));
+__device__ __forceinline__ int2 stayer_key(bool split_ovf, int tile, int cell, int rank, bool ovf_cell, int cloud) {
+    const int tail = (rank << KEY_RANK_SHIFT) | (cloud << KEY_CLOUD_SHIFT);
+    return split_ovf ? make_int2(tile, KIND_OVF | KEY_OVF_CELL | tail)
+                     : make_int2(cell, KIND_STAY | (ovf_cell ? KEY_OVF_CELL : 0) | tail);
 }
 
 template <class R> struct Args {
@@ -445,6 +453,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     int* s_cell = s_src + CAP;
     uint16_t* s_head = reinterpret_cast<uint16_t*>(s_cell + CAP);  // first positions of cells to collide
     static_assert(CAP <= 65536, "head positions are 16-bit");
+    static_assert(CAP <= (1 << KEY_RANK_BITS), "a stayer's rank (below CAP) must fit its key");
     __shared__ CloudPhys<R> P_sh;
     const CloudPhys<R>& P = ONE ? A.one : P_sh;
     __shared__ StepAcc red[BLOCK / 32];
@@ -666,7 +675,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                         reinterpret_cast<int*>(s_pos + t)[0] = rank;
                         s_cell[t] = (int)((unsigned)c_old | 0x80000000u);
                     } else {
-                        A.keys[tb + t] = stayer_key(split && c_old == c_first, b, c_old, rank, c_old == P.ovf_cell);
+                        A.keys[tb + t] = stayer_key(split && c_old == c_first, b, c_old, rank, c_old == P.ovf_cell, cloud);
                     }
                 }
             }
@@ -757,7 +766,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 rank += s_tcnt[qq];
                 if (!s_twhole[qq]) break;
             }
-            A.keys[tb + t] = stayer_key(split && c == c_first, b, c, rank, c == P.ovf_cell);
+            A.keys[tb + t] = stayer_key(split && c == c_first, b, c, rank, c == P.ovf_cell, cloud);
         }
         __syncthreads();  // the staging arrays, red and s_lost are reused by the next tile
     }
@@ -772,18 +781,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 // except one exactly at st; the overflow cell, which never collides, begins a tile at each
 // nominal start inside it (the only cell split across tiles).
 // ---------------------------------------------------------------------------------------------
-template <class R>
-__device__ __forceinline__ int cloud_of_cell(const Args<R>& A, int c) {
-    if (A.nclouds == 1) return 0;
-    int lo = 0, hi = A.nclouds - 1;  // the last cloud whose first cell is <= c
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (A.cloud_cell_base[mid] <= c) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // every tile start in the non-empty cell [st, e) of cloud k
 template <class R>
 __device__ void cell_tile_starts(const Args<R>& A, int k, int st, int e, bool ovf) {
@@ -851,7 +848,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 #pragma unroll
             for (int i = 0; i < G; ++i) key[i] = j0 + i < n ? A.keys[j0 + i] : make_int2(-1, KIND_LOST);
         }
-        int c[G], base[G], kc[G];
+        int c[G], base[G];
         bool ok[G];
 #pragma unroll
         for (int i = 0; i < G; ++i) {
@@ -859,7 +856,6 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             ok[i] = kind == KIND_STAY || kind == KIND_OVF;
             c[i] = key[i].x;
             base[i] = 0;
-            kc[i] = -1;
             if (kind == KIND_OVF) {
                 const int b = key[i].x;
                 if (b < 0 || b >= ntiles) {
@@ -868,7 +864,6 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
                     continue;
                 }
                 const int cloud = A.tile_cloud[b];
-                kc[i] = cloud;
                 c[i] = A.clouds[cloud].ovf_cell;
                 const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
                 base[i] = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
@@ -887,13 +882,14 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
 #pragma unroll
         for (int i = 0; i < G; ++i) {
             if (!ok[i]) continue;
-            const int r = base[i] + (key[i].y >> KEY_RANK_SHIFT);
+            const int r = base[i] + ((key[i].y >> KEY_RANK_SHIFT) & KEY_RANK_MASK);
             const int dest = lo[i] + r;
             if (dest >= lo[i] && dest < hi[i]) {
                 A.src_out[dest] = j0 + i;
                 if (tiles) {
-                    if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kc[i] >= 0 ? kc[i] : cloud_of_cell(A, c[i]), lo[i], dest);
-                    else if (r == 0) cell_tile_starts(A, cloud_of_cell(A, c[i]), lo[i], hi[i], false);
+                    const int kcl = key[i].y >> KEY_CLOUD_SHIFT;  // the cell's cloud
+                    if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kcl, lo[i], dest);
+                    else if (r == 0) cell_tile_starts(A, kcl, lo[i], hi[i], false);
                 }
             } else {
                 atomicOr(&A.ctl->err, EB_INCONSISTENT);
