@@ -63,8 +63,9 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #define DSMC_FP32_MINB 4
 #endif
 
-const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
-constexpr int kNumStepKernels = 4;
+// the kernels of one step, in launch order
+const char* kKernelNames[] = {"dense_collide", "step_pass", "scan_cells", "permute_pass", "mover_rank"};
+constexpr int kNumStepKernels = 5;
 
 }  // namespace
 
@@ -118,7 +119,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<R4> pos[2], vel[2], psi[2];
     DevBuf<int> start[2], tile_begin[2], tile_cloud[2], tile_split[2];
     DevBuf<int> src[2];
-    DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry, ovf_list;
+    DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry, ovf_list, tile_cell;
+    DevBuf<int2> dense_list;
+    int dense_cap = 0;  // dense cells a step can hold: each has more than dense_threshold(CAP) atoms
     DevBuf<int4> mrec;
     DevBuf<int2> keys;
     DevBuf<R> sigvrmax;
@@ -157,12 +160,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         nclouds = n;
         cp.assign(clouds, clouds + n);
         use_graphs = r.use_graphs != 0;
-        // default nominal tile: a little under two passes of the block, since a tile snapped to
-        // cell boundaries overshoots its nominal size by part of a cell
         // preferred nominal tile: three passes of the block, less a part of a cell for the snap
-        // to cell boundaries (each step's scan lowers it where a cell is fuller than CAP - T + 1)
+        // to cell boundaries (each step's scan lowers it where a cell that is not split across
+        // tiles is fuller than CAP - T + 1)
         tile_nominal = r.tile_atoms > 0 ? r.tile_atoms : CAP - BLOCK - 16;
-        // a grid cell holds at most CAP - T + 1 atoms (DSMC_ERR_CELL_FULL beyond): T <= CAP - 128
+        // a tile of nominal size T fits every cell of up to CAP - T + 1 atoms beside it
         if (tile_nominal > CAP - 128) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be <= " + std::to_string(CAP - 128)};
         if (tile_nominal < kMinTile) throw Fail{DSMC_ERR_INVALID, "tile_atoms must be >= " + std::to_string(kMinTile)};
         build_phys();
@@ -268,6 +270,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         mrec.alloc(mover_list_size());
         keys.alloc(std::max(capacity, 2048));  // >= 4096 ints: the full sort's count table
         tile_ovf.alloc(max_tiles); tile_ovf_carry.alloc(max_tiles); ovf_list.alloc(max_tiles);
+        tile_cell.alloc(max_tiles);
+        dense_cap = capacity / (dense_threshold(CAP) + 1) + 1;
+        dense_list.alloc(dense_cap);
         sigvrmax.alloc(total_cells);
         accum.alloc((size_t)nclouds * ACC_BUCKETS);
         CU(cudaMemset(accum.p, 0, (size_t)nclouds * ACC_BUCKETS * sizeof(CloudAccum)));
@@ -325,6 +330,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.tile_begin_next = tile_begin[q].p; A.tile_cloud_next = tile_cloud[q].p;
             A.tile_split_next = tile_split[q].p;
             A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p; A.ovf_list = ovf_list.p;
+            A.tile_cell = tile_cell.p; A.dense_list = dense_list.p; A.dense_cap = dense_cap;
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.one = phys[0];
@@ -344,15 +350,16 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0:
+        case 0: dense_collide<R><<<DENSE_GRID, DENSE_BLOCK, 0, stream>>>(A); break;
+        case 1:
             if (nclouds == 1)
                 step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
-        case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
-        case 3: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 2: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
+        case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
+        case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
     }
 
@@ -556,7 +563,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (h.err) {
             std::string m = "device error bits 0x" + std::to_string(h.err) + ":";
             dsmc_status st = DSMC_ERR_CUDA;
-            if (h.err & EB_CELL_FULL) { m += " a cell holds more atoms than a tile can stage;"; st = DSMC_ERR_CELL_FULL; }
+            if (h.err & EB_CELL_FULL) { m += " a tile holds more atoms than it can stage;"; st = DSMC_ERR_CELL_FULL; }
             if (h.err & EB_NAN) { m += " non-finite velocity;"; st = DSMC_ERR_NAN; }
             if (h.err & EB_INIT_REJECT) { m += " initial rejection sampling gave up;"; st = DSMC_ERR_INVALID; }
             if (h.err & EB_TILE_OVERFLOW) { m += " tile table overflow;"; st = DSMC_ERR_CAPACITY; }
@@ -699,6 +706,11 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (nscan_blocks < 2) throw Fail{DSMC_ERR_INVALID, "the wait check needs more than one scan block of cells"};
         sync();
         check_err();
+        // the dense-cell lists: the scan lists into one and clears the other, which the coming
+        // step's dense_collide still reads, so both are put back afterwards
+        int nd[2] = {0, 0};
+        CU(cudaMemcpyAsync(nd, ctl.p->ndense, sizeof(nd), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
         const int one = 1;
         CU(cudaMemcpyAsync(&ctl.p->scan_ticket, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
         launch_scan(args[parity], 0);
@@ -707,6 +719,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemcpyAsync(&bits, &ctl.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
         CU(cudaMemsetAsync(&ctl.p->err, 0, sizeof(int), stream));
+        CU(cudaMemcpyAsync(ctl.p->ndense, nd, sizeof(nd), cudaMemcpyHostToDevice, stream));
         CU(cudaStreamSynchronize(stream));
         return bits;
     }
@@ -1126,7 +1139,7 @@ DSMC_API const char* dsmc_status_string(dsmc_status s) {
     case DSMC_ERR_CUDA: return "CUDA error";
     case DSMC_ERR_ALLOC: return "allocation failed";
     case DSMC_ERR_CAPACITY: return "capacity exceeded";
-    case DSMC_ERR_CELL_FULL: return "cell too full for one tile";
+    case DSMC_ERR_CELL_FULL: return "tile too full to stage";
     case DSMC_ERR_NAN: return "non-finite state";
     case DSMC_ERR_STATE: return "call out of order";
     case DSMC_ERR_UNSUPPORTED: return "unsupported";

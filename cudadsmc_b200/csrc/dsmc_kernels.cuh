@@ -73,6 +73,15 @@ constexpr int ACC_BUCKETS = 16;
 
 // smallest nominal tile (sizes the tile tables: at most capacity / MIN_TILE + clouds + 2 tiles)
 constexpr int MIN_TILE = 128;
+// A grid cell of more than dense_threshold(CAP) atoms is dense: like the overflow cell it is split
+// across tiles (a tile begins at each nominal start inside it), and dense_collide collides it
+// before step_pass, reaching its atoms through the sorted order.  Every other grid cell fits a
+// tile, so a tiling of nominal size T >= MIN_TILE (tiles of at most T - 1 + dense_threshold
+// atoms) always fits the staging capacity.
+__host__ __device__ constexpr int dense_threshold(int cap) { return cap - MIN_TILE + 1; }
+// tile_ovf word of a tile: the stayers of its last cell when that cell continues into the next
+// tile, and TILE_WHOLE when the tile lies inside that cell (it also began inside it)
+constexpr int TILE_WHOLE = 1 << 30;
 struct __align__(16) CloudAccum {
     unsigned long long v2[3], B[3], ev2[3], eB[3];
     unsigned long long n_alive, n_maj, n_knife, coll, cand, pad[3];
@@ -98,14 +107,15 @@ struct Ctl {
     int step[2];
     int err;
     int movers[2];  // movers listed by the step of each parity (the other parity's is cleared by the scan)
-    int novf[2];    // tiles with overflow-cell stayers listed by the step of each parity
-    int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds prefixes from there on
+    int novf[2];    // tiles listed in ovf_list by the step of each parity
+    int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds the carries from there on
     int scan_done;    // scan_cells blocks finished (the last one runs the top level and clears it)
     int max_cell;     // largest coming grid-cell count, gathered by scan_cells (cleared by its top level)
     int tile_T[2];    // nominal tile size of the tiling built for each parity
     int scan_ticket;  // scan_cells blocks started: a block's ticket is the scan block it processes
     int tiles_built[2];  // 1: scan_cells wrote the tiling of that parity (else the atoms' placement does)
     unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
+    int ndense[2];  // dense grid cells listed for the step of each parity (dense_collide collides them)
 };
 
 // keys written by step_pass, one per atom position:
@@ -156,13 +166,16 @@ template <class R> struct Args {
     int* in_list;
     const int* tile_begin;
     const int* tile_cloud;
-    const int* tile_split;  // 1: the tile begins inside a cell (the overflow cell) that began earlier
+    const int* tile_split;  // 1: the tile begins inside a cell (overflow or dense) that began earlier
     int* tile_begin_next;
     int* tile_cloud_next;
     int* tile_split_next;
     int* tile_ovf;
     int* tile_ovf_carry;
-    int* ovf_list;  // tiles holding stayers of an overflow cell, in any order (ctl->novf[parity])
+    int* ovf_list;  // split tiles and tiles whose last cell continues, in any order (ctl->novf[parity])
+    int* tile_cell;  // per split tile: the cell it begins inside (written by step_pass)
+    int2* dense_list;  // (cell, cloud) of each dense grid cell of the coming step (ctl->ndense)
+    int dense_cap;
     CloudAccum* accum;  // nclouds x ACC_BUCKETS
     const CloudPhys<R>* clouds;
     CloudPhys<R> one;   // the parameters of cloud 0, read from the kernel parameters by one-cloud runs
@@ -417,6 +430,62 @@ template <class R> struct TileCollisionLog {
     }
 };
 
+// The velocities of a dense cell in global memory: element i of the cell is the atom at sorted
+// position first + i, stored at src[first + i] (an index outside the state flags the step
+// inconsistent and reads atom 0 without writing it)
+template <class R> struct GatherVel {
+    typedef typename V4T<R>::type R4;
+    R4* vel;
+    const int* src;  // the cell's entries of the gather permutation
+    int capacity;
+    int* err;
+    __device__ __forceinline__ int at(uint32_t i) const {
+        const int s = src[i];
+        if (s < 0 || s >= capacity) {
+            atomicOr(err, EB_INCONSISTENT);
+            return -1;
+        }
+        return s;
+    }
+};
+template <class R> __device__ __forceinline__ typename V4T<R>::type vload(const GatherVel<R>& g, uint32_t i) {
+    const int s = g.at(i);
+    return g.vel[s < 0 ? 0 : s];
+}
+template <class R>
+__device__ __forceinline__ void vstore(const GatherVel<R>& g, uint32_t i, const typename V4T<R>::type& v) {
+    const int s = g.at(i);
+    if (s >= 0) g.vel[s] = v;
+}
+
+// the collision record of a dense cell: atom ids read through the same permutation
+template <class R> struct GatherCollisionLog {
+    typedef typename V4T<R>::type R4;
+    const R4* pos;
+    const int* src;
+    int capacity;
+    int2* ij;
+    double* nv;
+    int* count;
+    int cap;
+    int* err;
+    __device__ __forceinline__ int id(uint32_t i) const {
+        const int s = src[i];
+        return (s >= 0 && s < capacity) ? (int)lane_to_u32(pos[s].w) : -1;
+    }
+    template <class RR> __device__ void accept(uint32_t i, uint32_t j, RR nx, RR ny, RR nz) {
+        const int slot = atomicAdd(count, 1);
+        if (slot < cap) {
+            ij[slot] = make_int2(id(i), id(j));
+            nv[3 * slot] = (double)nx;
+            nv[3 * slot + 1] = (double)ny;
+            nv[3 * slot + 2] = (double)nz;
+        } else {
+            atomicOr(err, EB_LOG_FULL);
+        }
+    }
+};
+
 // 16-byte asynchronous global -> shared copies (cp.async, L2 only); a gather, unlike TMA
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -430,6 +499,58 @@ template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src
 #pragma unroll
     for (int o = 0; o < (int)sizeof(R4); o += 16)
         cp_async16(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o);
+}
+
+// ---------------------------------------------------------------------------------------------
+// dense_collide: the NTC collisions of this step's dense grid cells (more atoms than a tile can
+// stage beside a minimal tile), which step_pass leaves out.  One thread per cell runs the same
+// serial loop as a cell inside a tile -- same Philox words, same order, so the same result bit for
+// bit -- on the velocities in global memory, reached through the sorted order's permutation, and
+// adds its counts to the cloud's totals.  Runs before step_pass, which then gathers the collided
+// velocities; cells are independent, so colliding them here or inside a tile is the same.
+// ---------------------------------------------------------------------------------------------
+constexpr int DENSE_BLOCK = 128;
+constexpr int DENSE_GRID = 148;
+template <class R>
+__global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
+    typedef typename V4T<R>::type R4;
+    const int p = A.parity;
+    const int nd = min(A.ctl->ndense[p], A.dense_cap);
+    if (nd == 0) return;
+    const int step = A.ctl->step[p];
+    if (step % A.collide_every != 0) return;
+    const int n_now = A.ctl->n[p];
+    for (int i = blockIdx.x * DENSE_BLOCK + threadIdx.x; i < nd; i += gridDim.x * DENSE_BLOCK) {
+        const int2 d = A.dense_list[i];
+        const int c = d.x, k = d.y;
+        if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            continue;
+        }
+        const CloudPhys<R>& P = A.clouds[k];
+        if (!(P.flags & F_COLLIDE)) continue;
+        const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
+        if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            continue;
+        }
+        R svm = A.sigvrmax[c];
+        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
+        CollideResult<R> cr;
+        if (A.clog_ij) {
+            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n, A.clog_count,
+                                     A.clog_cap, &A.ctl->err};
+            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                                     (uint32_t)step, A.seed, &lg);
+        } else {
+            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
+        }
+        A.sigvrmax[c] = svm;
+        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
+        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
+        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
+        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -454,6 +575,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     uint16_t* s_head = reinterpret_cast<uint16_t*>(s_cell + CAP);  // first positions of cells to collide
     static_assert(CAP <= 65536, "head positions are 16-bit");
     static_assert(CAP <= (1 << KEY_RANK_BITS), "a stayer's rank (below CAP) must fit its key");
+    constexpr int DENSE = dense_threshold(CAP);
     __shared__ CloudPhys<R> P_sh;
     const CloudPhys<R>& P = ONE ? A.one : P_sh;
     __shared__ StepAcc red[BLOCK / 32];
@@ -464,7 +586,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     __shared__ int s_tcell[NCH];
     __shared__ int s_tcnt[NCH];
     __shared__ int s_twhole[NCH];
-    __shared__ int s_ovf;  // stayers of the overflow cell in the current tile
+    __shared__ int s_ovf;   // stayers of the tile's last cell, when that cell continues into the next tile
+    __shared__ int s_cont;  // that cell (-1: the last cell ends with the tile)
     __shared__ LostAcc s_lost;
 
     const int p = A.parity;
@@ -559,6 +682,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             const R4 q = s_pos[t];
             const int c = cell_of(P, q.x, q.y, q.z, box);
             s_cell[t] = c;
+            // the last cell when it continues into the next tile (a split cell; else -1): its
+            // stayers here are counted for the ranks of its stayers there
+            if (t == L - 1) s_cont = (c < A.total_cells && A.old_start[c + 1] > te) ? c : -1;
         }
         __syncthreads();
         const int c_first = L > 0 ? s_cell[0] : -1;
@@ -566,8 +692,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 
         StepAcc acc;
         zero_acc(acc);
-        // phase 2: NTC collisions, one thread per grid cell (cells never straddle tiles).  The
-        // cells holding two or more atoms are listed first, so that every lane takes a cell.
+        // phase 2: NTC collisions, one thread per grid cell that fits a tile (dense cells, which
+        // dense_collide has collided, and the overflow cell are split across tiles).  The cells
+        // holding two or more atoms are listed first, so that every lane takes a cell.
         if ((P.flags & F_COLLIDE) && collide_now) {
             for (int base = 0; base < L; base += BLOCK) {
                 const int t = base + threadIdx.x;
@@ -593,6 +720,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 const int c_beg = A.old_start[c], c_end = A.old_start[c + 1];
                 R svm = A.sigvrmax[c];
                 const int n = c_end - c_beg;
+                if (n > DENSE) continue;  // a dense cell: collided by dense_collide
                 if (c_beg != tb + t || n > L - t) {  // cell not wholly inside this tile
                     atomicOr(&A.ctl->err, EB_INCONSISTENT);
                     continue;
@@ -679,8 +807,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     }
                 }
             }
-            // stayers of the overflow cell in this tile (one shared atomic per warp pass)
-            const unsigned om = __ballot_sync(FULL, stayer && c_old == P.ovf_cell);
+            // stayers of the tile's last cell when it continues into the next tile (one shared atomic
+            // per warp pass)
+            const unsigned om = __ballot_sync(FULL, stayer && c_old == s_cont);
             if (om && lane == 0) atomicAdd(&s_ovf, __popc(om));
             // leavers of the old cell (movers and lost atoms): one fire-and-forget atomic each (a
             // warp pass rarely has two leavers of one cell, so aggregating them costs more than it saves)
@@ -748,8 +877,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         block_reduce_acc<BLOCK>(acc, red, tot);  // its barrier also orders the chunk records, s_ovf and s_lost
         if (threadIdx.x == 0) {
             CloudAccum* bucket = A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1));
-            A.tile_ovf[b] = s_ovf;
-            if (s_ovf > 0) {
+            const bool whole = split && s_cont == c_first;
+            A.tile_ovf[b] = s_ovf | (whole ? TILE_WHOLE : 0);
+            if (split) A.tile_cell[b] = c_first;
+            if (s_ovf > 0 || split) {  // ovf_carries scans the tiles from the lowest to the highest listed
                 const int i = atomicAdd(&A.ctl->novf[p], 1);
                 if (i < A.max_tiles) A.ovf_list[i] = b;
             }
@@ -778,8 +909,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 // Tile starts of the coming step, written where the atoms are placed (permute_pass, mover_rank,
 // and init_tiles after a full sort).  The nominal starts S + j*T of cloud k (S its first sorted
 // position, T the coming nominal size) that fall inside a grid cell [st, e) snap to the cell's end,
-// except one exactly at st; the overflow cell, which never collides, begins a tile at each
-// nominal start inside it (the only cell split across tiles).
+// except one exactly at st; a split cell -- the overflow cell, which never collides, or a dense
+// cell, which dense_collide collides -- begins a tile at each nominal start inside it.
 // ---------------------------------------------------------------------------------------------
 // every tile start in the non-empty cell [st, e) of cloud k
 template <class R>
@@ -803,9 +934,9 @@ __device__ void cell_tile_starts(const Args<R>& A, int k, int st, int e, bool ov
     }
 }
 
-// the tile start at position x of cloud k's overflow cell (which begins at st), if x is a nominal start
+// the tile start at position x of a split cell of cloud k (the cell begins at st), if x is a nominal start
 template <class R>
-__device__ __forceinline__ void ovf_tile_start(const Args<R>& A, int k, int st, int x) {
+__device__ __forceinline__ void split_tile_start(const Args<R>& A, int k, int st, int x) {
     const int q = 1 - A.parity;
     const int S = A.cdyn[k].start[q];
     const int T = A.ctl->tile_T[q];
@@ -821,10 +952,11 @@ __device__ __forceinline__ void ovf_tile_start(const Args<R>& A, int k, int st, 
 
 // ---------------------------------------------------------------------------------------------
 // permute_pass: the stayers' part of the next step's gather permutation.  A stayer of cell c with
-// rank r goes to new_start[c] + r (+ the overflow-cell stayers of the cloud's earlier tiles for
+// rank r goes to new_start[c] + r (+ the stayers of its split cell in the cell's earlier tiles for
 // KIND_OVF); src_out[dest] = its position in the buffer step_pass wrote.  Unless scan_cells built
 // the coming tiling, the stayer placed at a grid cell's first position writes the cell's tile
-// starts; every stayer of an overflow cell checks its own position.  Movers are placed by
+// starts; every stayer of a split cell (the overflow cell, or a cell that will be dense) checks its
+// own position.  Movers are placed by
 // mover_rank, after this kernel has listed each cell's incoming movers.  Flat streams over the
 // keys and the mover records, no shared memory and no barriers.
 // ---------------------------------------------------------------------------------------------
@@ -834,6 +966,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
     const int n = A.ctl->n[p];
     const int ntiles = A.ctl->ntiles[p];
     const bool tiles = A.ctl->tiles_built[1 - p] == 0;  // the coming tiling is built here
+    const int dense = dense_threshold(A.tile_cap);     // larger cells are split like the overflow cell
     // four consecutive positions per thread and pass: two 16-byte key loads, then the cell
     // starts of all four, then the stores (the loads of one pass are independent)
     constexpr int G = 4;
@@ -863,10 +996,8 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
                     ok[i] = false;
                     continue;
                 }
-                const int cloud = A.tile_cloud[b];
-                c[i] = A.clouds[cloud].ovf_cell;
-                const int first = max(A.cdyn[cloud].tile_off[p], A.ctl->ovf_lo[p]);
-                base[i] = A.tile_ovf_carry[b] - A.tile_ovf_carry[first];
+                c[i] = A.tile_cell[b];  // the split cell the tile begins inside
+                base[i] = A.tile_ovf_carry[b];
             }
             if (ok[i] && (c[i] < 0 || c[i] >= A.total_cells)) {
                 atomicOr(&A.ctl->err, EB_INCONSISTENT);
@@ -888,7 +1019,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
                 A.src_out[dest] = j0 + i;
                 if (tiles) {
                     const int kcl = key[i].y >> KEY_CLOUD_SHIFT;  // the cell's cloud
-                    if (key[i].y & KEY_OVF_CELL) ovf_tile_start(A, kcl, lo[i], dest);
+                    if ((key[i].y & KEY_OVF_CELL) || hi[i] - lo[i] > dense) split_tile_start(A, kcl, lo[i], dest);
                     else if (r == 0) cell_tile_starts(A, kcl, lo[i], hi[i], false);
                 }
             } else {
@@ -1155,6 +1286,7 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
+        A.ctl->ndense[A.parity] = 0;  // consumed by this step's dense_collide; the next scan lists into it
         A.ctl->tiles_built[q] = (A.nclouds == 1 && !A.init_mode && T == A.ctl->tile_T[A.parity]) ? 1 : 0;
         A.ctl->tile_T[q] = T;
         A.ctl->max_cell = 0;
@@ -1163,19 +1295,25 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
     }
 }
 
-// Overflow-cell stayers, run by one block of a physics-step scan_cells launch beside the scan:
-// exclusive prefix of tile_ovf over the tiles from the lowest to the highest listed one (tile_ovf
-// is zero on every unlisted tile, so a listed tile's carry is its prefix minus the prefix at its
-// cloud's first tile, or at the lowest listed tile)
+// Stayers of split cells (overflow and dense cells), run by one block of a physics-step scan_cells
+// launch beside the scan.  A stayer in a tile that begins inside its cell (a KIND_OVF key) is
+// ranked after the cell's stayers in the cell's earlier tiles; that carry is, per tile b,
+//   carry[b + 1] = cnt[b] + (whole[b] ? carry[b] : 0)
+// with cnt[b] the stayers of tile b's last cell when that cell continues into tile b + 1, and
+// whole[b] when tile b lies inside it.  An affine recurrence: the block scans it over the tiles
+// from the lowest to the highest listed one (every split tile and every tile with cnt > 0 is
+// listed, so the lowest listed tile has carry 0 and every carry a KIND_OVF key needs is in range).
 template <class R, int BLOCK>
 __device__ void ovf_carries(const Args<R>& A) {
-    __shared__ uint32_t wsum[32];
-    __shared__ int s_carry, s_lo, s_hi;
+    constexpr int NW = BLOCK / 32;
+    __shared__ int s_lo, s_hi, s_x;
+    __shared__ int wa[NW], wc[NW], wx[NW];
     const int p = A.parity;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         s_lo = 0x7fffffff;
         s_hi = -1;
-        s_carry = 0;
+        s_x = 0;
     }
     __syncthreads();
     const int m = min(A.ctl->novf[p], A.max_tiles);
@@ -1190,23 +1328,56 @@ __device__ void ovf_carries(const Args<R>& A) {
     constexpr int IT = 16;
     for (int base = lo; base <= hi; base += BLOCK * IT) {
         const int i0 = base + threadIdx.x * IT;
-        int v[IT];
-        uint32_t s = 0;
+        int cnt[IT];
+        bool wh[IT];
+        // this thread's tiles as one map x -> (a ? x : 0) + c (beyond hi: the identity)
+        bool a = true;
+        int c = 0;
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
-            v[k] = (i0 + k <= hi) ? A.tile_ovf[i0 + k] : 0;
-            s += (uint32_t)v[k];
+            const int v = (i0 + k <= hi) ? A.tile_ovf[i0 + k] : TILE_WHOLE;
+            cnt[k] = v & (TILE_WHOLE - 1);
+            wh[k] = (v & TILE_WHOLE) != 0;
+            c = (wh[k] ? c : 0) + cnt[k];
+            a = a && wh[k];
         }
-        uint32_t tot;
-        uint32_t ex = block_excl_scan_u32<BLOCK>(s, wsum, tot) + (uint32_t)s_carry;
+        // inclusive scan of the maps over the warp (later after earlier), then the exclusive one
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int ap = __shfl_up_sync(0xffffffffu, a ? 1 : 0, off);
+            const int cp = __shfl_up_sync(0xffffffffu, c, off);
+            if (lane >= off) {
+                c = (a ? cp : 0) + c;
+                a = a && ap != 0;
+            }
+        }
+        int ae = __shfl_up_sync(0xffffffffu, a ? 1 : 0, 1);
+        int ce = __shfl_up_sync(0xffffffffu, c, 1);
+        if (lane == 0) {
+            ae = 1;
+            ce = 0;
+        }
+        if (lane == 31) {
+            wa[warp] = a ? 1 : 0;
+            wc[warp] = c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {  // the carry entering each warp's first tile, and the next chunk's
+            int x = s_x;
+            for (int w = 0; w < NW; ++w) {
+                wx[w] = x;
+                x = (wa[w] ? x : 0) + wc[w];
+            }
+            s_x = x;
+        }
+        __syncthreads();
+        int x = (ae ? wx[warp] : 0) + ce;
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
-            if (i0 + k <= hi) A.tile_ovf_carry[i0 + k] = (int)ex;
-            ex += (uint32_t)v[k];
+            if (i0 + k <= hi) A.tile_ovf_carry[i0 + k] = x;
+            x = (wh[k] ? x : 0) + cnt[k];
         }
-        __syncthreads();
-        if (threadIdx.x == 0) s_carry += (int)tot;
-        __syncthreads();
+        __syncthreads();  // wa / wc / wx are rewritten by the next chunk
     }
 }
 
@@ -1288,11 +1459,22 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
             }
         }
         uint32_t s = 0;
-        int m = 0;  // largest grid-cell count (the cloud's overflow cell, its last, is split across tiles)
+        // largest count of a grid cell that fits a tile (the overflow cell, the cloud's last, and the
+        // dense cells are split across tiles); the dense cells are listed for dense_collide
+        const int dense = dense_threshold(A.tile_cap);
+        int m = 0;
 #pragma unroll
         for (int k = 0; k < CELL_ITEMS; ++k) {
             s += (uint32_t)cnt[k];
-            if (cb + k < cend - 1) m = max(m, cnt[k]);
+            if (cb + k < cend - 1) {
+                if (cnt[k] <= dense) {
+                    m = max(m, cnt[k]);
+                } else {
+                    const int i = atomicAdd(&A.ctl->ndense[1 - A.parity], 1);
+                    if (i < A.dense_cap) A.dense_list[i] = make_int2(cb + k, hb.x);
+                    else atomicOr(&A.ctl->err, EB_CAPACITY);
+                }
+            }
         }
         m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
         if (lane == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
@@ -1336,13 +1518,15 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
                         s_ovf_end = e;
                         j = e / Ts + (e % Ts != 0);
                     }
-                    for (; j * Ts < e; ++j) {  // nominal starts inside this cell snap to its end
+                    // nominal starts inside this cell snap to its end, unless the cell is dense
+                    const bool spl = cnt[k] > dense && cb + k < cend - 1;
+                    for (; j * Ts < e; ++j) {
                         const int pnom = j * Ts;
-                        const int tbeg = pnom == st ? st : e;
+                        const int tbeg = (pnom == st || spl) ? pnom : e;
                         if (j < A.max_tiles) {
                             A.tile_begin_next[j] = tbeg;
                             A.tile_cloud_next[j] = 0;
-                            A.tile_split_next[j] = 0;
+                            A.tile_split_next[j] = tbeg != st && tbeg != e ? 1 : 0;
                         }
                     }
                 }
@@ -1400,13 +1584,13 @@ __global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
         const int c = c0 + threadIdx.x * CELL_ITEMS + k;
         if (c >= c1) break;
         const int st = A.new_start[c], e = A.new_start[c + 1];
-        if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1);
+        if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1 || e - st > dense_threshold(A.tile_cap));
     }
 }
 
 // rank = number of incoming movers of the same cell with a smaller old position; unless scan_cells
 // built the coming tiling, the mover placed at a grid cell's first position writes the cell's tile
-// starts, every overflow-cell mover checks its own position
+// starts, every mover into a split cell (overflow or dense) checks its own position
 template <class R>
 __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
     const int m = min(A.ctl->movers[A.parity], A.mrec_cap);
@@ -1428,10 +1612,10 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
             A.src_out[x] = r.y;
             const int k = r.w & (MREC_OVF_CELL - 1);
             if (tiles) {
-                if (r.w & MREC_OVF_CELL) {
-                    ovf_tile_start(A, k, A.new_start[r.x], x);
+                const int st = A.new_start[r.x];
+                if ((r.w & MREC_OVF_CELL) || hi - st > dense_threshold(A.tile_cap)) {
+                    split_tile_start(A, k, st, x);
                 } else if (rank == 0) {
-                    const int st = A.new_start[r.x];
                     if (st == lo) cell_tile_starts(A, k, st, hi, false);
                 }
             }

@@ -49,7 +49,8 @@ typedef enum dsmc_status {
     DSMC_ERR_CUDA = 2,        /* CUDA runtime error (no device, launch failure...) */
     DSMC_ERR_ALLOC = 3,       /* device or host allocation failed */
     DSMC_ERR_CAPACITY = 4,    /* atom capacity exceeded */
-    DSMC_ERR_CELL_FULL = 5,   /* a grid cell holds more atoms than one tile can stage */
+    DSMC_ERR_CELL_FULL = 5,   /* a tile holds more atoms than it can stage (an inconsistent tiling;
+                                 dense cells are split across tiles and never raise it) */
     DSMC_ERR_NAN = 6,         /* non-finite position or velocity met */
     DSMC_ERR_STATE = 7,       /* call out of order (e.g. step before init) */
     DSMC_ERR_UNSUPPORTED = 8, /* feature not available in this build / mode */

@@ -86,7 +86,7 @@ def test_presets():
 def test_status_strings():
     lib = dsmc.load_library()
     assert lib.dsmc_abi_version() == 2
-    assert lib.dsmc_status_string(5) == b"cell too full for one tile"
+    assert lib.dsmc_status_string(5) == b"tile too full to stage"
 
 
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device failure path")

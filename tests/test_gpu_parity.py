@@ -181,7 +181,7 @@ def test_profiling_mode_identical():
     orc.step(5)
     assert_same(a, orc)
     t = a.kernel_times()
-    assert len(t) == a.launches_per_step() == 4
+    assert len(t) == a.launches_per_step() == 5  # dense_collide, step_pass, scan_cells, permute_pass, mover_rank
     assert all(v[1] == 5 for v in t.values())
 
 
@@ -270,20 +270,41 @@ def test_dense_cells_and_tiny_clouds():
     assert occ[:-1].max() > 300
 
 
-def test_cell_too_full_fails_loudly():
-    # 4000 atoms in one cell cannot be staged by one tile: the step reports DSMC_ERR_CELL_FULL
-    run, c = scaled(2, n=4000, cells=1, flags=F_COLLIDE | F_LARMOR)
-    for a in range(3):
-        c.grid_min[a] *= 4
-        c.grid_max[a] *= 4
-    sim = Simulation(run, c)
-    sim.init_cloud(1)
-    sim.step(1)
-    with pytest.raises(DSMCError):
-        sim.synchronize()
-        d = sim.diagnostics()
-        if d["error"]:
-            raise DSMCError(5, "error bits set")
+DENSE_FP32 = 1280 - 128 + 1  # grid cells above this many atoms are split across tiles (FP32)
+
+
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_one_dense_cell_bit_exact(precision):
+    # 4000 atoms in one cell, more than a tile stages: the cell is split across tiles, its
+    # collisions run in dense_collide through the sorted order, and the result is the oracle's
+    run, c = scaled(2, n=4000, cells=1, flags=F_COLLIDE | F_LARMOR, precision=precision, alpha=2e7)
+    sim, orc = run_pair(run, c, 12, check_every=[1, 5, 6])
+    occ = np.diff(sim.cell_starts())
+    assert occ[0] > 3000
+    assert sim.diagnostics()["collisions"] > 50
+
+
+def test_dense_cells_split_across_small_tiles():
+    # a coarse grid: dozens of cells above the dense threshold, each split across several
+    # 256-atom tiles, beside ordinary cells and the overflow cell, with every step process on;
+    # two clouds in one handle so that the split cells of both carry their ranks separately
+    run, c = scaled(2, n=60000, cells=6, flags=ALL, tile_atoms=256, alpha=2e4)
+    run2, c1 = scaled(2, n=20000, cells=5, flags=ALL, alpha=1e4)
+    c1.stream_id = 1
+    sim, orc = run_pair(run, [c, c1], 16, check_every=[1, 1, 6, 8])
+    occ = np.diff(sim.cell_starts())
+    grid = np.delete(occ, [6 ** 3, 6 ** 3 + 1 + 5 ** 3])  # the two overflow cells left out
+    assert (grid > DENSE_FP32).sum() >= 6
+    assert sim.diagnostics(0)["collisions"] > 0 and sim.diagnostics(1)["collisions"] > 0
+
+
+def test_dense_cells_default_tiles_and_collide_every():
+    # the default (adaptive) tiling, collisions every third step, the MCWF flips at the
+    # collision periods' ends: dense cells only change which kernel collides them
+    run, c = scaled(2, n=80000, cells=8, flags=ALL | F_MCWF, collide_every=3, alpha=2e4)
+    sim, orc = run_pair(run, c, 12, check_every=[2, 10])
+    occ = np.diff(sim.cell_starts())
+    assert occ[:-1].max() > DENSE_FP32
 
 
 def test_autotune_changes_speed_not_results():
