@@ -64,8 +64,8 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #endif
 
 // the kernels of one step, in launch order
-const char* kKernelNames[] = {"dense_collide", "step_pass", "scan_cells", "permute_pass", "mover_rank"};
-constexpr int kNumStepKernels = 5;
+const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
+constexpr int kNumStepKernels = 4;
 
 }  // namespace
 
@@ -350,16 +350,15 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0: dense_collide<R><<<DENSE_GRID, DENSE_BLOCK, 0, stream>>>(A); break;
-        case 1:
+        case 0:
             if (nclouds == 1)
                 step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 2: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
-        case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
-        case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
+        case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
+        case 3: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
     }
 
@@ -567,6 +566,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             if (h.err & EB_NAN) { m += " non-finite velocity;"; st = DSMC_ERR_NAN; }
             if (h.err & EB_INIT_REJECT) { m += " initial rejection sampling gave up;"; st = DSMC_ERR_INVALID; }
             if (h.err & EB_TILE_OVERFLOW) { m += " tile table overflow;"; st = DSMC_ERR_CAPACITY; }
+            if (h.err & EB_CAPACITY) { m += " a mover or dense-cell list overflowed;"; st = DSMC_ERR_CAPACITY; }
+            if (h.err & EB_LOG_FULL) { m += " the collision record is full;"; st = DSMC_ERR_CAPACITY; }
             if (h.err & EB_TIMEOUT) { m += " a bounded device-side wait gave up;"; st = DSMC_ERR_TIMEOUT; }
             if (h.err & EB_INCONSISTENT) { m += " inconsistent cell bookkeeping (after an earlier error);"; }
             throw Fail{st, m};
@@ -707,7 +708,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         sync();
         check_err();
         // the dense-cell lists: the scan lists into one and clears the other, which the coming
-        // step's dense_collide still reads, so both are put back afterwards
+        // step's step_pass still reads, so both are put back afterwards
         int nd[2] = {0, 0};
         CU(cudaMemcpyAsync(nd, ctl.p->ndense, sizeof(nd), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));

@@ -74,8 +74,8 @@ constexpr int ACC_BUCKETS = 16;
 // smallest nominal tile (sizes the tile tables: at most capacity / MIN_TILE + clouds + 2 tiles)
 constexpr int MIN_TILE = 128;
 // A grid cell of more than dense_threshold(CAP) atoms is dense: like the overflow cell it is split
-// across tiles (a tile begins at each nominal start inside it), and dense_collide collides it
-// before step_pass, reaching its atoms through the sorted order.  Every other grid cell fits a
+// across tiles (a tile begins at each nominal start inside it), and step_pass collides it at its
+// head, before any tile, reaching its atoms through the sorted order.  Every other grid cell fits a
 // tile, so a tiling of nominal size T >= MIN_TILE (tiles of at most T - 1 + dense_threshold
 // atoms) always fits the staging capacity.
 __host__ __device__ constexpr int dense_threshold(int cap) { return cap - MIN_TILE + 1; }
@@ -115,16 +115,19 @@ struct Ctl {
     int scan_ticket;  // scan_cells blocks started: a block's ticket is the scan block it processes
     int tiles_built[2];  // 1: scan_cells wrote the tiling of that parity (else the atoms' placement does)
     unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
-    int ndense[2];  // dense grid cells listed for the step of each parity (dense_collide collides them)
+    int ndense[2];     // dense grid cells listed for the step of each parity (collided at the head of step_pass;
+                       // listed where the atoms are placed, the list of the coming step cleared by the scan)
+    int dense_ticket;  // dense cells taken by step_pass blocks in the current step (cleared by the scan)
+    int dense_done;    // dense cells collided in the current step (cleared by the scan)
 };
 
 // keys written by step_pass, one per atom position:
 //   .y = kind | KEY_OVF_CELL | (rank << KEY_RANK_SHIFT) | (cloud << KEY_CLOUD_SHIFT)
 //   KIND_STAY  .x = cell, rank among the cell's stayers before it (the cell starts in this tile)
-//   KIND_OVF   .x = tile, rank among the tile's stayers of the cloud's overflow cell, which
-//              started in an earlier tile (the only cell that may be split across tiles)
+//   KIND_OVF   .x = tile, rank among the tile's stayers of the split cell (overflow or dense)
+//              that the tile begins inside (tile_cell), which started in an earlier tile
 //   KIND_MOVE  .x = slot in the step's mover list;  KIND_LOST  .x = -1
-//   KEY_OVF_CELL: the stayer's cell is its cloud's overflow cell (always set with KIND_OVF)
+//   KEY_OVF_CELL: the stayer's cell is its cloud's overflow cell
 // A stayer's rank counts positions of its tile, so it is below the staging capacity (< 2^11); the
 // cloud rides along so that permute_pass need not search for the cell's cloud.
 enum : int { KIND_STAY = 0, KIND_MOVE = 1, KIND_LOST = 2, KIND_OVF = 3 };
@@ -140,8 +143,7 @@ constexpr int MREC_OVF_CELL = 1 << 30;
 
 __device__ __forceinline__ int2 stayer_key(bool split_ovf, int tile, int cell, int rank, bool ovf_cell, int cloud) {
     const int tail = (rank << KEY_RANK_SHIFT) | (cloud << KEY_CLOUD_SHIFT);
-    return split_ovf ? make_int2(tile, KIND_OVF | KEY_OVF_CELL | tail)
-                     : make_int2(cell, KIND_STAY | (ovf_cell ? KEY_OVF_CELL : 0) | tail);
+    return make_int2(split_ovf ? tile : cell, (split_ovf ? KIND_OVF : KIND_STAY) | (ovf_cell ? KEY_OVF_CELL : 0) | tail);
 }
 
 template <class R> struct Args {
@@ -501,56 +503,89 @@ template <class R4> __device__ __forceinline__ void stage(R4* dst, const R4* src
         cp_async16(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o);
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// a wait on other blocks that sees no progress for this long gives up with EB_TIMEOUT instead of
+// hanging (the scan's look-back, the dense-cell barrier of step_pass)
+constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
+
 // ---------------------------------------------------------------------------------------------
-// dense_collide: the NTC collisions of this step's dense grid cells (more atoms than a tile can
-// stage beside a minimal tile), which step_pass leaves out.  One thread per cell runs the same
-// serial loop as a cell inside a tile -- same Philox words, same order, so the same result bit for
-// bit -- on the velocities in global memory, reached through the sorted order's permutation, and
-// adds its counts to the cloud's totals.  Runs before step_pass, which then gathers the collided
-// velocities; cells are independent, so colliding them here or inside a tile is the same.
+// The NTC collisions of the step's dense grid cells (more atoms than a tile stages beside a
+// minimal tile), which the tiles leave out.  Run at the head of step_pass by every block before
+// its first tile: warp 0 takes 32 listed cells at a time from a ticket and each lane runs one
+// cell's serial loop -- the same collide_cell code, Philox words and order as inside a tile, so
+// the same result bit for bit -- on the velocities in global memory, reached through the sorted
+// order's permutation, then counts the cell done; the block then waits until every listed cell is
+// done, so that its tiles gather collided velocities.  Cells are independent, so colliding them
+// here or inside a tile is the same.  A block only waits on cells that blocks which have already
+// started took (tickets are taken at block start), so the wait ends whatever the scheduling; it is
+// also bounded in time (EB_TIMEOUT).  With no dense cell (the usual case) it costs one load.
 // ---------------------------------------------------------------------------------------------
-constexpr int DENSE_BLOCK = 128;
-constexpr int DENSE_GRID = 148;
 template <class R>
-__global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
+__device__ void collide_dense_cells(const Args<R>& A, int nd, int step) {
     typedef typename V4T<R>::type R4;
     const int p = A.parity;
-    const int nd = min(A.ctl->ndense[p], A.dense_cap);
-    if (nd == 0) return;
-    const int step = A.ctl->step[p];
-    if (step % A.collide_every != 0) return;
-    const int n_now = A.ctl->n[p];
-    for (int i = blockIdx.x * DENSE_BLOCK + threadIdx.x; i < nd; i += gridDim.x * DENSE_BLOCK) {
-        const int2 d = A.dense_list[i];
-        const int c = d.x, k = d.y;
-        if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
-            atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            continue;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const int n_now = A.ctl->n[p];
+        for (;;) {
+            int i0 = 0;
+            if (lane == 0) i0 = atomicAdd(&A.ctl->dense_ticket, 32);
+            i0 = __shfl_sync(0xffffffffu, i0, 0);
+            if (i0 >= nd) break;
+            const int i = i0 + lane;
+            if (i < nd) {
+                const int2 d = A.dense_list[i];
+                const int c = d.x, k = d.y;
+                if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
+                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                } else if (A.clouds[k].flags & F_COLLIDE) {
+                    const CloudPhys<R>& P = A.clouds[k];
+                    const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
+                    if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
+                        atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                    } else {
+                        R svm = A.sigvrmax[c];
+                        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
+                        CollideResult<R> cr;
+                        if (A.clog_ij) {
+                            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n,
+                                                     A.clog_count, A.clog_cap, &A.ctl->err};
+                            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(
+                                g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed, &lg);
+                        } else {
+                            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                               (uint32_t)step, A.seed);
+                        }
+                        A.sigvrmax[c] = svm;
+                        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
+                        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
+                        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
+                        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
+                    }
+                }
+                __threadfence();  // the cell's velocities before its done count
+                atomicAdd(&A.ctl->dense_done, 1);
+            }
         }
-        const CloudPhys<R>& P = A.clouds[k];
-        if (!(P.flags & F_COLLIDE)) continue;
-        const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
-        if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
-            atomicOr(&A.ctl->err, EB_INCONSISTENT);
-            continue;
+        if (lane == 0) {
+            const unsigned long long t0 = global_ns();
+            while (true) {
+                int done;
+                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(done) : "l"(&A.ctl->dense_done) : "memory");
+                if (done >= nd) break;
+                if (global_ns() - t0 > LB_TIMEOUT_NS) {
+                    atomicOr(&A.ctl->err, EB_TIMEOUT);
+                    break;
+                }
+                __nanosleep(256);
+            }
         }
-        R svm = A.sigvrmax[c];
-        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
-        CollideResult<R> cr;
-        if (A.clog_ij) {
-            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n, A.clog_count,
-                                     A.clog_cap, &A.ctl->err};
-            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                                     (uint32_t)step, A.seed, &lg);
-        } else {
-            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
-        }
-        A.sigvrmax[c] = svm;
-        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
-        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
-        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
-        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
     }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -581,13 +616,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
     __shared__ StepAcc red[BLOCK / 32];
     __shared__ R s_cut;
     __shared__ int s_nhead;
+    __shared__ int s_next_split;
     // the last run of cells in each 32-position chunk: its cell, its stayers, whether it spans the chunk
     constexpr int NCH = CAP / 32;
     __shared__ int s_tcell[NCH];
     __shared__ int s_tcnt[NCH];
     __shared__ int s_twhole[NCH];
-    __shared__ int s_ovf;   // stayers of the tile's last cell, when that cell continues into the next tile
-    __shared__ int s_cont;  // that cell (-1: the last cell ends with the tile)
     __shared__ LostAcc s_lost;
 
     const int p = A.parity;
@@ -603,6 +637,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         LostAcc z = {};
         s_lost = z;  // ordered before first use by the barrier after the first load_cloud
     }
+
+    if ((A.ctl->ndense[p] > 0) && collide_now) collide_dense_cells(A, min(A.ctl->ndense[p], A.dense_cap), step);
 
     // this warp's chunk of mover-list slots: the next free one and the chunk's end
     int mv_next = 0, mv_end = 0;
@@ -661,10 +697,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 prefetch_l2(A.psi_in + s);  // read in the motion phase: an L2 hit by then
             }
         }
-        if (threadIdx.x == 0) {
-            s_nhead = 0;
-            s_ovf = 0;
-        }
+        if (threadIdx.x == 0) s_nhead = 0;
         // the next tile's storage indices into L2 (its first DRAM round trip), while the
         // gathers of this one are in flight
         {
@@ -675,6 +708,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 if (x < nte) prefetch_l2(A.src_in + x);
             }
         }
+        // whether the next tile begins inside this tile's last cell (kept in shared memory for the
+        // tile's end, where thread 0 reads it; loaded while the gathers are in flight)
+        if (threadIdx.x == 0) s_next_split = b + 1 < ntiles && A.tile_split[b + 1] != 0 ? 1 : 0;
         // each thread's cell pass reads only the positions it staged itself: its own copies
         // suffice, the barrier after the pass publishes the cells and the staged tile
         cp_async_wait_all();
@@ -682,9 +718,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             const R4 q = s_pos[t];
             const int c = cell_of(P, q.x, q.y, q.z, box);
             s_cell[t] = c;
-            // the last cell when it continues into the next tile (a split cell; else -1): its
-            // stayers here are counted for the ranks of its stayers there
-            if (t == L - 1) s_cont = (c < A.total_cells && A.old_start[c + 1] > te) ? c : -1;
         }
         __syncthreads();
         const int c_first = L > 0 ? s_cell[0] : -1;
@@ -693,7 +726,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         StepAcc acc;
         zero_acc(acc);
         // phase 2: NTC collisions, one thread per grid cell that fits a tile (dense cells, which
-        // dense_collide has collided, and the overflow cell are split across tiles).  The cells
+        // were collided at the head of the kernel, and the overflow cell are split across tiles).  The cells
         // holding two or more atoms are listed first, so that every lane takes a cell.
         if ((P.flags & F_COLLIDE) && collide_now) {
             for (int base = 0; base < L; base += BLOCK) {
@@ -720,7 +753,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 const int c_beg = A.old_start[c], c_end = A.old_start[c + 1];
                 R svm = A.sigvrmax[c];
                 const int n = c_end - c_beg;
-                if (n > DENSE) continue;  // a dense cell: collided by dense_collide
+                if (n > DENSE) continue;  // a dense cell: collided at the head of the kernel
                 if (c_beg != tb + t || n > L - t) {  // cell not wholly inside this tile
                     atomicOr(&A.ctl->err, EB_INCONSISTENT);
                     continue;
@@ -807,10 +840,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                     }
                 }
             }
-            // stayers of the tile's last cell when it continues into the next tile (one shared atomic
-            // per warp pass)
-            const unsigned om = __ballot_sync(FULL, stayer && c_old == s_cont);
-            if (om && lane == 0) atomicAdd(&s_ovf, __popc(om));
             // leavers of the old cell (movers and lost atoms): one fire-and-forget atomic each (a
             // warp pass rarely has two leavers of one cell, so aggregating them costs more than it saves)
             if (valid && !stayer) atomicAdd(&A.Lc[c_old], 1);
@@ -874,13 +903,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
             }
         }
         TilePartial tot;
-        block_reduce_acc<BLOCK>(acc, red, tot);  // its barrier also orders the chunk records, s_ovf and s_lost
+        block_reduce_acc<BLOCK>(acc, red, tot);  // its barrier also orders the chunk records and s_lost
         if (threadIdx.x == 0) {
             CloudAccum* bucket = A.accum + cloud * ACC_BUCKETS + (b & (ACC_BUCKETS - 1));
-            const bool whole = split && s_cont == c_first;
-            A.tile_ovf[b] = s_ovf | (whole ? TILE_WHOLE : 0);
+            // when the next tile begins inside this tile's last cell (split): that cell's stayers here,
+            // from the chunk records of its run (counted for the ranks of its stayers there), and
+            // whether this tile lies wholly inside it
+            int cont = 0;
+            bool whole = false;
+            if (s_next_split && L > 0) {
+                const int lc = (L - 1) >> 5;
+                const int c_last = s_tcell[lc];
+                for (int qq = lc; qq >= 0 && s_tcell[qq] == c_last; --qq) {
+                    cont += s_tcnt[qq];
+                    if (!s_twhole[qq]) break;
+                }
+                whole = split && c_last == c_first;
+            }
+            A.tile_ovf[b] = cont | (whole ? TILE_WHOLE : 0);
             if (split) A.tile_cell[b] = c_first;
-            if (s_ovf > 0 || split) {  // ovf_carries scans the tiles from the lowest to the highest listed
+            if (cont > 0 || split) {  // ovf_carries scans the tiles from the lowest to the highest listed
                 const int i = atomicAdd(&A.ctl->novf[p], 1);
                 if (i < A.max_tiles) A.ovf_list[i] = b;
             }
@@ -910,7 +952,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 // and init_tiles after a full sort).  The nominal starts S + j*T of cloud k (S its first sorted
 // position, T the coming nominal size) that fall inside a grid cell [st, e) snap to the cell's end,
 // except one exactly at st; a split cell -- the overflow cell, which never collides, or a dense
-// cell, which dense_collide collides -- begins a tile at each nominal start inside it.
+// cell, which step_pass collides at its head -- begins a tile at each nominal start inside it.
 // ---------------------------------------------------------------------------------------------
 // every tile start in the non-empty cell [st, e) of cloud k
 template <class R>
@@ -932,6 +974,15 @@ __device__ void cell_tile_starts(const Args<R>& A, int k, int st, int e, bool ov
             A.tile_split_next[ti] = (tbeg != st && tbeg != e) ? 1 : 0;
         }
     }
+}
+
+// lists grid cell c of cloud k, dense in the coming step, for that step's step_pass (called once per
+// dense cell: by the atom placed at its first position, or by init_tiles after a full sort)
+template <class R>
+__device__ __forceinline__ void list_dense(const Args<R>& A, int c, int k) {
+    const int i = atomicAdd(&A.ctl->ndense[1 - A.parity], 1);
+    if (i < A.dense_cap) A.dense_list[i] = make_int2(c, k);
+    else atomicOr(&A.ctl->err, EB_CAPACITY);
 }
 
 // the tile start at position x of a split cell of cloud k (the cell begins at st), if x is a nominal start
@@ -1015,11 +1066,14 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
             if (!ok[i]) continue;
             const int r = base[i] + ((key[i].y >> KEY_RANK_SHIFT) & KEY_RANK_MASK);
             const int dest = lo[i] + r;
-            if (dest >= lo[i] && dest < hi[i]) {
+            if (dest >= lo[i] && dest < hi[i] && dest < A.capacity) {
                 A.src_out[dest] = j0 + i;
+                const int kcl = key[i].y >> KEY_CLOUD_SHIFT;  // the cell's cloud
+                const bool ovf = (key[i].y & KEY_OVF_CELL) != 0;
+                const bool dns = !ovf && hi[i] - lo[i] > dense;
+                if (dns && r == 0) list_dense(A, c[i], kcl);
                 if (tiles) {
-                    const int kcl = key[i].y >> KEY_CLOUD_SHIFT;  // the cell's cloud
-                    if ((key[i].y & KEY_OVF_CELL) || hi[i] - lo[i] > dense) split_tile_start(A, kcl, lo[i], dest);
+                    if (ovf || dns) split_tile_start(A, kcl, lo[i], dest);
                     else if (r == 0) cell_tile_starts(A, kcl, lo[i], hi[i], false);
                 }
             } else {
@@ -1034,7 +1088,7 @@ __global__ void __launch_bounds__(256) permute_pass(Args<R> A) {
         const int4 r = A.mrec[i];
         if (r.x < 0) continue;  // an unused slot of a warp's chunk
         const int slot = A.mover_base[r.x] + atomicAdd(&A.Ic[r.x], 1);
-        if (slot >= 0 && slot < A.new_start[r.x + 1]) A.in_list[slot] = r.y;
+        if (slot >= 0 && slot < A.new_start[r.x + 1] && slot < A.capacity) A.in_list[slot] = r.y;
         else atomicOr(&A.ctl->err, EB_INCONSISTENT);
     }
 }
@@ -1074,8 +1128,6 @@ inline int scan_extra_blocks(int nclouds, int cb) { return 1 + (nclouds + cb / 3
 // and the value is the block's sum (LB_AGG) or its inclusive prefix (LB_INC)
 enum : unsigned { LB_NONE = 0, LB_AGG = 1, LB_INC = 2 };
 constexpr unsigned LB_EPOCH_MASK = 0x3fffffffu;
-// a look-back that sees no progress for this long gives up with EB_TIMEOUT instead of hanging
-constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
 
 __device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned status, unsigned v) {
     return ((unsigned long long)(epoch & LB_EPOCH_MASK) << 34) | ((unsigned long long)status << 32) | v;
@@ -1093,11 +1145,6 @@ __device__ __forceinline__ unsigned long long lb_load(const unsigned long long* 
     unsigned long long w;
     asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
     return w;
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
 }
 
 // Exclusive prefix of scan block blk (one full warp; the result is the same in every lane).  The
@@ -1230,7 +1277,11 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
     __shared__ uint32_t wsum[32];
     __shared__ int s_tcarry;
     const int q = 1 - A.parity;
-    const int total = (int)(unsigned)lb_load(A.scan_desc, A.nscan_blocks - 1);
+    int total = (int)(unsigned)lb_load(A.scan_desc, A.nscan_blocks - 1);
+    if (total < 0 || total > A.capacity) {  // only after an inconsistent step: keep every later index in range
+        if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_INCONSISTENT);
+        total = total < 0 ? 0 : A.capacity;
+    }
     // the coming tiling's nominal size: the preferred size, or less where a cell holds so many
     // atoms that a tile snapped to cell boundaries could outgrow the staging capacity
     const int mc = __ldcg(&A.ctl->max_cell);
@@ -1286,7 +1337,9 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
         A.tile_begin_next[ntiles_next <= A.max_tiles ? ntiles_next : A.max_tiles] = total;
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
-        A.ctl->ndense[A.parity] = 0;  // consumed by this step's dense_collide; the next scan lists into it
+        A.ctl->ndense[q] = 0;  // the coming step's dense cells are listed where its atoms are placed
+        A.ctl->dense_ticket = 0;
+        A.ctl->dense_done = 0;
         A.ctl->tiles_built[q] = (A.nclouds == 1 && !A.init_mode && T == A.ctl->tile_T[A.parity]) ? 1 : 0;
         A.ctl->tile_T[q] = T;
         A.ctl->max_cell = 0;
@@ -1460,21 +1513,13 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
         }
         uint32_t s = 0;
         // largest count of a grid cell that fits a tile (the overflow cell, the cloud's last, and the
-        // dense cells are split across tiles); the dense cells are listed for dense_collide
+        // dense cells are split across tiles)
         const int dense = dense_threshold(A.tile_cap);
         int m = 0;
 #pragma unroll
         for (int k = 0; k < CELL_ITEMS; ++k) {
             s += (uint32_t)cnt[k];
-            if (cb + k < cend - 1) {
-                if (cnt[k] <= dense) {
-                    m = max(m, cnt[k]);
-                } else {
-                    const int i = atomicAdd(&A.ctl->ndense[1 - A.parity], 1);
-                    if (i < A.dense_cap) A.dense_list[i] = make_int2(cb + k, hb.x);
-                    else atomicOr(&A.ctl->err, EB_CAPACITY);
-                }
-            }
+            if (cb + k < cend - 1 && cnt[k] <= dense) m = max(m, cnt[k]);
         }
         m = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(m, 0));
         if (lane == 0 && m > 0) atomicMax(&s_max, m);  // ordered by the scan's barriers
@@ -1584,7 +1629,9 @@ __global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
         const int c = c0 + threadIdx.x * CELL_ITEMS + k;
         if (c >= c1) break;
         const int st = A.new_start[c], e = A.new_start[c + 1];
-        if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1 || e - st > dense_threshold(A.tile_cap));
+        const bool dns = c != cend - 1 && e - st > dense_threshold(A.tile_cap);
+        if (dns) list_dense(A, c, cloud);
+        if (e > st) cell_tile_starts(A, cloud, st, e, c == cend - 1 || dns);
     }
 }
 
@@ -1611,9 +1658,12 @@ __global__ void __launch_bounds__(256) mover_rank(Args<R> A) {
         if (x < hi && r.y >= 0 && r.y < A.capacity) {
             A.src_out[x] = r.y;
             const int k = r.w & (MREC_OVF_CELL - 1);
+            const int st = A.new_start[r.x];
+            const bool ovf = (r.w & MREC_OVF_CELL) != 0;
+            const bool dns = !ovf && hi - st > dense_threshold(A.tile_cap);
+            if (dns && x == st) list_dense(A, r.x, k);
             if (tiles) {
-                const int st = A.new_start[r.x];
-                if ((r.w & MREC_OVF_CELL) || hi - st > dense_threshold(A.tile_cap)) {
+                if (ovf || dns) {
                     split_tile_start(A, k, st, x);
                 } else if (rank == 0) {
                     if (st == lo) cell_tile_starts(A, k, st, hi, false);
