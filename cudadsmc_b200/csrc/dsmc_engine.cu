@@ -64,8 +64,8 @@ constexpr int kMinTile = MIN_TILE;  // smallest tile the autotuner tries (sizes 
 #endif
 
 // the kernels of one step, in launch order
-const char* kKernelNames[] = {"step_pass", "scan_cells", "permute_pass", "mover_rank"};
-constexpr int kNumStepKernels = 4;
+const char* kKernelNames[] = {"dense_collide", "step_pass", "scan_cells", "permute_pass", "mover_rank"};
+constexpr int kNumStepKernels = 5;
 
 }  // namespace
 
@@ -350,15 +350,16 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0:
+        case 0: dense_collide<R><<<DENSE_GRID, DENSE_BLOCK, 0, stream>>>(A); break;
+        case 1:
             if (nclouds == 1)
                 step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 1: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
-        case 2: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
-        case 3: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
+        case 2: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
+        case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
+        case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
     }
 
@@ -708,7 +709,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         sync();
         check_err();
         // the dense-cell lists: the scan lists into one and clears the other, which the coming
-        // step's step_pass still reads, so both are put back afterwards
+        // step's dense_collide still reads, so both are put back afterwards
         int nd[2] = {0, 0};
         CU(cudaMemcpyAsync(nd, ctl.p->ndense, sizeof(nd), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));

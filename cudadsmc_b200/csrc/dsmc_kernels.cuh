@@ -74,8 +74,8 @@ constexpr int ACC_BUCKETS = 16;
 // smallest nominal tile (sizes the tile tables: at most capacity / MIN_TILE + clouds + 2 tiles)
 constexpr int MIN_TILE = 128;
 // A grid cell of more than dense_threshold(CAP) atoms is dense: like the overflow cell it is split
-// across tiles (a tile begins at each nominal start inside it), and step_pass collides it at its
-// head, before any tile, reaching its atoms through the sorted order.  Every other grid cell fits a
+// across tiles (a tile begins at each nominal start inside it), and dense_collide collides it
+// before step_pass, reaching its atoms through the sorted order.  Every other grid cell fits a
 // tile, so a tiling of nominal size T >= MIN_TILE (tiles of at most T - 1 + dense_threshold
 // atoms) always fits the staging capacity.
 __host__ __device__ constexpr int dense_threshold(int cap) { return cap - MIN_TILE + 1; }
@@ -115,10 +115,8 @@ struct Ctl {
     int scan_ticket;  // scan_cells blocks started: a block's ticket is the scan block it processes
     int tiles_built[2];  // 1: scan_cells wrote the tiling of that parity (else the atoms' placement does)
     unsigned scan_epoch;  // scan_cells launches completed: tags the look-back descriptors of a launch
-    int ndense[2];     // dense grid cells listed for the step of each parity (collided at the head of step_pass;
-                       // listed where the atoms are placed, the list of the coming step cleared by the scan)
-    int dense_ticket;  // dense cells taken by step_pass blocks in the current step (cleared by the scan)
-    int dense_done;    // dense cells collided in the current step (cleared by the scan)
+    int ndense[2];  // dense grid cells listed for the step of each parity (collided by dense_collide;
+                    // listed where the atoms are placed, the list of the coming step cleared by the scan)
 };
 
 // keys written by step_pass, one per atom position:
@@ -508,84 +506,60 @@ __device__ __forceinline__ unsigned long long global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// a wait on other blocks that sees no progress for this long gives up with EB_TIMEOUT instead of
-// hanging (the scan's look-back, the dense-cell barrier of step_pass)
+// a look-back that sees no progress for this long gives up with EB_TIMEOUT instead of hanging
 constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
 
 // ---------------------------------------------------------------------------------------------
-// The NTC collisions of the step's dense grid cells (more atoms than a tile stages beside a
-// minimal tile), which the tiles leave out.  Run at the head of step_pass by every block before
-// its first tile: warp 0 takes 32 listed cells at a time from a ticket and each lane runs one
-// cell's serial loop -- the same collide_cell code, Philox words and order as inside a tile, so
-// the same result bit for bit -- on the velocities in global memory, reached through the sorted
-// order's permutation, then counts the cell done; the block then waits until every listed cell is
-// done, so that its tiles gather collided velocities.  Cells are independent, so colliding them
-// here or inside a tile is the same.  A block only waits on cells that blocks which have already
-// started took (tickets are taken at block start), so the wait ends whatever the scheduling; it is
-// also bounded in time (EB_TIMEOUT).  With no dense cell (the usual case) it costs one load.
+// dense_collide: the NTC collisions of the step's dense grid cells (more atoms than a tile stages
+// beside a minimal tile), which step_pass leaves out.  One thread per cell runs the same serial
+// loop as a cell inside a tile -- same collide_cell code, Philox words and order, so the same
+// result bit for bit -- on the velocities in global memory, reached through the sorted order's
+// permutation, and adds its counts to the cloud's totals.  Launched before step_pass, which then
+// gathers the collided velocities; cells are independent, so colliding them here or inside a tile
+// is the same.  With no dense cell (the usual case) its blocks read the count and return.
 // ---------------------------------------------------------------------------------------------
+constexpr int DENSE_BLOCK = 128;
+constexpr int DENSE_GRID = 148;
 template <class R>
-__device__ void collide_dense_cells(const Args<R>& A, int nd, int step) {
+__global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
     typedef typename V4T<R>::type R4;
     const int p = A.parity;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const int n_now = A.ctl->n[p];
-        for (;;) {
-            int i0 = 0;
-            if (lane == 0) i0 = atomicAdd(&A.ctl->dense_ticket, 32);
-            i0 = __shfl_sync(0xffffffffu, i0, 0);
-            if (i0 >= nd) break;
-            const int i = i0 + lane;
-            if (i < nd) {
-                const int2 d = A.dense_list[i];
-                const int c = d.x, k = d.y;
-                if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
-                    atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                } else if (A.clouds[k].flags & F_COLLIDE) {
-                    const CloudPhys<R>& P = A.clouds[k];
-                    const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
-                    if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
-                        atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                    } else {
-                        R svm = A.sigvrmax[c];
-                        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
-                        CollideResult<R> cr;
-                        if (A.clog_ij) {
-                            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n,
-                                                     A.clog_count, A.clog_cap, &A.ctl->err};
-                            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(
-                                g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed, &lg);
-                        } else {
-                            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                               (uint32_t)step, A.seed);
-                        }
-                        A.sigvrmax[c] = svm;
-                        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
-                        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
-                        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
-                        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
-                    }
-                }
-                __threadfence();  // the cell's velocities before its done count
-                atomicAdd(&A.ctl->dense_done, 1);
-            }
+    const int nd = min(A.ctl->ndense[p], A.dense_cap);
+    if (nd == 0) return;
+    const int step = A.ctl->step[p];
+    if (step % A.collide_every != 0) return;
+    const int n_now = A.ctl->n[p];
+    for (int i = blockIdx.x * DENSE_BLOCK + threadIdx.x; i < nd; i += gridDim.x * DENSE_BLOCK) {
+        const int2 d = A.dense_list[i];
+        const int c = d.x, k = d.y;
+        if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            continue;
         }
-        if (lane == 0) {
-            const unsigned long long t0 = global_ns();
-            while (true) {
-                int done;
-                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(done) : "l"(&A.ctl->dense_done) : "memory");
-                if (done >= nd) break;
-                if (global_ns() - t0 > LB_TIMEOUT_NS) {
-                    atomicOr(&A.ctl->err, EB_TIMEOUT);
-                    break;
-                }
-                __nanosleep(256);
-            }
+        const CloudPhys<R>& P = A.clouds[k];
+        if (!(P.flags & F_COLLIDE)) continue;
+        const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
+        if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
+            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            continue;
         }
+        R svm = A.sigvrmax[c];
+        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
+        CollideResult<R> cr;
+        if (A.clog_ij) {
+            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n, A.clog_count,
+                                     A.clog_cap, &A.ctl->err};
+            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
+                                                                     (uint32_t)step, A.seed, &lg);
+        } else {
+            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
+        }
+        A.sigvrmax[c] = svm;
+        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
+        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
+        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
+        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
     }
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -638,8 +612,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         s_lost = z;  // ordered before first use by the barrier after the first load_cloud
     }
 
-    if ((A.ctl->ndense[p] > 0) && collide_now) collide_dense_cells(A, min(A.ctl->ndense[p], A.dense_cap), step);
-
     // this warp's chunk of mover-list slots: the next free one and the chunk's end
     int mv_next = 0, mv_end = 0;
     // tiles in a grid-stride loop: the launch size only sets how many tiles run at once
@@ -648,6 +620,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         const int te = A.tile_begin[b + 1];
         const int L = te - tb;
         const int cloud = A.tile_cloud[b];
+        const int nsplit = b + 1 < ntiles ? A.tile_split[b + 1] : 0;  // with the bounds: one round trip
         if (cloud != cur_cloud) {  // block-uniform: the cloud's parameters and knife cut
             if (!ONE) load_cloud(P_sh, A.clouds + cloud);
             __syncthreads();
@@ -697,7 +670,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 prefetch_l2(A.psi_in + s);  // read in the motion phase: an L2 hit by then
             }
         }
-        if (threadIdx.x == 0) s_nhead = 0;
+        if (threadIdx.x == 0) {
+            s_nhead = 0;
+            s_next_split = nsplit;  // whether the next tile begins inside this tile's last cell
+        }
         // the next tile's storage indices into L2 (its first DRAM round trip), while the
         // gathers of this one are in flight
         {
@@ -708,9 +684,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 if (x < nte) prefetch_l2(A.src_in + x);
             }
         }
-        // whether the next tile begins inside this tile's last cell (kept in shared memory for the
-        // tile's end, where thread 0 reads it; loaded while the gathers are in flight)
-        if (threadIdx.x == 0) s_next_split = b + 1 < ntiles && A.tile_split[b + 1] != 0 ? 1 : 0;
         // each thread's cell pass reads only the positions it staged itself: its own copies
         // suffice, the barrier after the pass publishes the cells and the staged tile
         cp_async_wait_all();
@@ -726,7 +699,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
         StepAcc acc;
         zero_acc(acc);
         // phase 2: NTC collisions, one thread per grid cell that fits a tile (dense cells, which
-        // were collided at the head of the kernel, and the overflow cell are split across tiles).  The cells
+        // dense_collide has collided, and the overflow cell are split across tiles).  The cells
         // holding two or more atoms are listed first, so that every lane takes a cell.
         if ((P.flags & F_COLLIDE) && collide_now) {
             for (int base = 0; base < L; base += BLOCK) {
@@ -753,7 +726,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 const int c_beg = A.old_start[c], c_end = A.old_start[c + 1];
                 R svm = A.sigvrmax[c];
                 const int n = c_end - c_beg;
-                if (n > DENSE) continue;  // a dense cell: collided at the head of the kernel
+                if (n > DENSE) continue;  // a dense cell: collided by dense_collide
                 if (c_beg != tb + t || n > L - t) {  // cell not wholly inside this tile
                     atomicOr(&A.ctl->err, EB_INCONSISTENT);
                     continue;
@@ -952,7 +925,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
 // and init_tiles after a full sort).  The nominal starts S + j*T of cloud k (S its first sorted
 // position, T the coming nominal size) that fall inside a grid cell [st, e) snap to the cell's end,
 // except one exactly at st; a split cell -- the overflow cell, which never collides, or a dense
-// cell, which step_pass collides at its head -- begins a tile at each nominal start inside it.
+// cell, which dense_collide collides -- begins a tile at each nominal start inside it.
 // ---------------------------------------------------------------------------------------------
 // every tile start in the non-empty cell [st, e) of cloud k
 template <class R>
@@ -976,7 +949,7 @@ __device__ void cell_tile_starts(const Args<R>& A, int k, int st, int e, bool ov
     }
 }
 
-// lists grid cell c of cloud k, dense in the coming step, for that step's step_pass (called once per
+// lists grid cell c of cloud k, dense in the coming step, for that step's dense_collide (called once per
 // dense cell: by the atom placed at its first position, or by init_tiles after a full sort)
 template <class R>
 __device__ __forceinline__ void list_dense(const Args<R>& A, int c, int k) {
@@ -1338,8 +1311,6 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
         A.ctl->movers[q] = 0;
         A.ctl->novf[q] = 0;
         A.ctl->ndense[q] = 0;  // the coming step's dense cells are listed where its atoms are placed
-        A.ctl->dense_ticket = 0;
-        A.ctl->dense_done = 0;
         A.ctl->tiles_built[q] = (A.nclouds == 1 && !A.init_mode && T == A.ctl->tile_T[A.parity]) ? 1 : 0;
         A.ctl->tile_T[q] = T;
         A.ctl->max_cell = 0;

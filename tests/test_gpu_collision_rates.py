@@ -7,7 +7,7 @@ tests/golden/reference_collision_rates.json) lists the rate it measured with 1e3
 on 5^3 and 10^3 cells.  The same sweep runs here on the GPU engine: every (test atoms, cells) entry
 must give the analytic rate within four statistical errors and 0.5 %.  The 5^3-cell rows at 5e5 and
 1e6 test atoms hold 4000 and 8000 atoms per cell, more than a tile stages: they run through the
-dense-cell path (cells split across tiles, collided at the head of step_pass).
+dense-cell path (cells split across tiles, collided by dense_collide).
 """
 import json
 import math

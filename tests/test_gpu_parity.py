@@ -181,7 +181,7 @@ def test_profiling_mode_identical():
     orc.step(5)
     assert_same(a, orc)
     t = a.kernel_times()
-    assert len(t) == a.launches_per_step() == 4  # step_pass, scan_cells, permute_pass, mover_rank
+    assert len(t) == a.launches_per_step() == 5  # dense_collide, step_pass, scan_cells, permute_pass, mover_rank
     assert all(v[1] == 5 for v in t.values())
 
 
@@ -276,7 +276,7 @@ DENSE_FP32 = 1280 - 128 + 1  # grid cells above this many atoms are split across
 @pytest.mark.parametrize("precision", [FP32, FP64])
 def test_one_dense_cell_bit_exact(precision):
     # 4000 atoms in one cell, more than a tile stages: the cell is split across tiles, its
-    # collisions run at the head of step_pass through the sorted order, and the result is the oracle's
+    # collisions run in dense_collide through the sorted order, and the result is the oracle's
     run, c = scaled(2, n=4000, cells=1, flags=F_COLLIDE | F_LARMOR, precision=precision, alpha=2e7)
     sim, orc = run_pair(run, c, 12, check_every=[1, 5, 6])
     occ = np.diff(sim.cell_starts())
@@ -301,7 +301,7 @@ def test_dense_cells_split_across_small_tiles():
 @pytest.mark.parametrize("precision,threshold", [(FP32, 1153), (FP64, 897)])
 def test_cells_crossing_the_dense_threshold(precision, threshold):
     # a hot periodic box whose 27 cells hold the dense threshold on average: every step some cells
-    # become dense (split across tiles, collided at the head of step_pass) and others stop being
+    # become dense (split across tiles, collided by dense_collide) and others stop being
     # dense, while their stayers in later tiles still carry their ranks; bit-exact throughout
     run, c = scaled(1, n=27 * threshold, cells=3, flags=F_COLLIDE, precision=precision, temperature=2e-3,
                     alpha=3e5)
