@@ -112,7 +112,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     int max_tiles = 0;
     int tile_nominal = 0;
     int nscan_blocks = 0;
-    int cell_block = 256;  // threads of a scan_cells block (cell_block_for)
+    int cell_items = 16;  // cells per thread of a scan_cells block (cell_items_for)
     std::vector<int> cloud_atoms_init;  // initial atoms per cloud
     std::vector<int> cloud_cell_base;
     // device memory
@@ -282,9 +282,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemset(cdyn.p, 0, nclouds * sizeof(CloudDyn)));
         CU(cudaMemset(cdiag.p, 0, nclouds * sizeof(CloudDiagDev)));
         CU(cudaMemset(ctl.p, 0, sizeof(Ctl)));
-        // scan blocks: each covers up to cell_block * CELL_ITEMS cells of a single cloud
-        cell_block = cell_block_for(total_cells);
-        const int chunk = cell_block * CELL_ITEMS;
+        // scan blocks: each covers up to CELL_BLOCK * cell_items cells of a single cloud
+        cell_items = cell_items_for(total_cells);
+        const int chunk = CELL_BLOCK * cell_items;
         std::vector<int4> hb;
         std::vector<int> first(nclouds + 1);
         // a cloud whose cells start off a 4-cell boundary gets a first block of the 1-3 cells up to
@@ -357,7 +357,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             else
                 step_pass<R, BLOCK, CAP, MINB, false><<<step_grid(), BLOCK, smem_tile, stream>>>(A);
             break;
-        case 2: launch_scan(A, scan_extra_blocks(nclouds, cell_block)); break;
+        case 2: launch_scan(A, scan_extra_blocks(nclouds, CELL_BLOCK)); break;
         case 3: permute_pass<R><<<resident_permute, 256, 0, stream>>>(A); break;
         case 4: mover_rank<R><<<MOVER_GRID, 256, 0, stream>>>(A); break;
         }
@@ -365,8 +365,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 
     // the cell scan with `extra` leading blocks (overflow carries and step totals) before the scan blocks
     void launch_scan(const Args<R>& A, int extra) {
-        if (cell_block == 512) scan_cells<R, 512><<<extra + nscan_blocks, 512, 0, stream>>>(A);
-        else scan_cells<R, 256><<<extra + nscan_blocks, 256, 0, stream>>>(A);
+        if (cell_items == 16) scan_cells<R, CELL_BLOCK, 16><<<extra + nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
+        else scan_cells<R, CELL_BLOCK, 8><<<extra + nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
     }
 
     void enqueue_step(int p) {
@@ -495,8 +495,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         const int ab = (n + 255) / 256;
         if (n > 0) fs_cells<R><<<ab, 256, 0, stream>>>(S, A);
         launch_scan(A, 0);
-        if (cell_block == 512) init_tiles<R, 512><<<nscan_blocks, 512, 0, stream>>>(A);
-        else init_tiles<R, 256><<<nscan_blocks, 256, 0, stream>>>(A);
+        if (cell_items == 16) init_tiles<R, CELL_BLOCK, 16><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
+        else init_tiles<R, CELL_BLOCK, 8><<<nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
         if (n > 0) {
             // stable by (cell, source index): LSD passes over the digits of the cell ids
             const int nch = radix_chunks(n), passes = radix_passes(total_cells);

@@ -1082,12 +1082,11 @@ constexpr int SCAN_CHUNK = SCAN_BLOCK * SCAN_ITEMS;
 #ifndef DSMC_LB_STRIDE
 #define DSMC_LB_STRIDE 32
 #endif
-// scan_cells block (CB threads, CELL_ITEMS cells each): 512 threads on grids of more than
-// CELL_LARGE_GRID cells (fewer tickets and descriptors), 256 below (a shorter block scan on the
-// critical path of a small grid's step)
-constexpr int CELL_ITEMS = 16;
-constexpr int CELL_LARGE_GRID = 1 << 20;
-inline int cell_block_for(int total_cells) { return total_cells > CELL_LARGE_GRID ? 512 : 256; }
+// scan_cells block: CELL_BLOCK threads (four blocks per SM at 64 registers, so that one block's
+// loads overlap another's look-back and barriers), ITEMS cells each: 16 on grids that give every SM
+// two blocks or more at that size, else 8 (more, shorter blocks for a small grid's short step)
+constexpr int CELL_BLOCK = 256;
+inline int cell_items_for(int total_cells) { return total_cells >= 2 * 148 * CELL_BLOCK * 16 ? 16 : 8; }
 // descriptors lie LB_STRIDE words apart (one per 256 bytes), so that the look-back reads of all
 // blocks spread over the L2 slices instead of queueing on the few that hold a dense array
 constexpr int LB_STRIDE = DSMC_LB_STRIDE;
@@ -1409,7 +1408,7 @@ __device__ void ovf_carries(const Args<R>& A) {
 // the largest grid-cell count, and (last block) the top level.  In a physics step the launch puts
 // scan_extra_blocks(nclouds, CB) blocks ahead of the scan blocks: the overflow-cell carries, then the
 // clouds' step totals, one warp per cloud; after a full sort it carries the scan blocks alone.
-template <class R, int CB>
+template <class R, int CB, int CELL_ITEMS>
 __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
     constexpr int CELL_CHUNK = CB * CELL_ITEMS;
     __shared__ uint32_t wsum[32];
@@ -1591,7 +1590,7 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
 
 // Tile starts of the tiling the scan built after a full sort (no atoms are placed by
 // permute_pass then): the same rule, per cell.
-template <class R, int CB>
+template <class R, int CB, int CELL_ITEMS>
 __global__ void __launch_bounds__(CB) init_tiles(Args<R> A) {
     const int blk = blockIdx.x;
     const int4 hb = A.scan_blk[blk];
