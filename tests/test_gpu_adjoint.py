@@ -55,6 +55,27 @@ def test_gpu_smoothed_run_matches_oracle(recorded):
     np.testing.assert_allclose(grad_g, ge_o + gn_o, rtol=1e-9, atol=1e-12 * np.max(np.abs(ge_o + gn_o)))
 
 
+def test_recorded_collisions_of_dense_cells():
+    # a 2^3 grid: the central cells hold thousands of atoms and are collided by dense_collide, which
+    # records its collisions (atom ids through the permutation) like the tiles do; the smoothed
+    # model on the GPU equals the oracle's on that record
+    run, c = adjoint_cloud(n=20000, steps=100)
+    c.cells[0] = c.cells[1] = c.cells[2] = 2
+    sim = Simulation(run, c)
+    sim.init_cloud(97)
+    assert np.diff(sim.cell_starts())[:-1].max() > 1153
+    g = sim.adjoint_run(100, checkpoint_every=32, precision=FP64, sigmoid_width_kT=0.2)
+    rec = sim.adjoint_export()
+    ij = rec["ij"]
+    assert ij.shape[0] == g["collisions"] > 0
+    assert np.all(ij >= 0) and np.all(ij < c.n_atoms) and np.all(ij[:, 0] != ij[:, 1])
+    loss_o, parts_o, ge_o, gn_o = oracle.smooth_loss(run, c, theta_of(c), 0.2, rec["x0"], rec["v0"], rec["psi0"],
+                                                     rec["steps"], rec["off"], rec["ij"], rec["n"], grad=True,
+                                                     fp64=True, majorana_width=0.05)
+    assert g["mean_energy_kT"] == parts_o[0] and g["retained_fraction"] == parts_o[1]
+    np.testing.assert_allclose(np.array(g["dE_dtheta"]), ge_o, rtol=1e-9, atol=1e-12 * np.max(np.abs(ge_o)))
+
+
 def check_terms_against_differences(sim, th, g, min_checked):
     """Every term's gradient against central differences of that term, 1e-3 relative."""
     grads = (np.array(g["dE_dtheta"]), np.array(g["dN_dtheta"]))

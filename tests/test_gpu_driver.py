@@ -94,14 +94,17 @@ def test_driver_snapshot_records_match_the_oracle(tmp_path):
     assert np.count_nonzero(ev["step"] >= 0) > 0  # atoms were lost
 
 
-def test_step_records_match_the_oracle_with_collisions():
+@pytest.mark.parametrize("cells", [24, 3])
+def test_step_records_match_the_oracle_with_collisions(cells):
     """The records through the Python binding with enough collisions to count (alpha 2e4): lost
-    atoms by id and per-cell collision counts after every step, bit for bit with the oracle."""
+    atoms by id and per-cell collision counts after every step, bit for bit with the oracle.  On
+    3^3 cells the central cells are dense (more atoms than a tile stages): their counts come from
+    dense_collide."""
     import oracle
     from cudadsmc_b200 import F_COLLIDE, F_KNIFE, F_LARMOR, F_MAJORANA, F_NORMALISE
     run, c = preset(2)
     c.n_atoms = c.capacity = 30000
-    c.cells[0] = c.cells[1] = c.cells[2] = 24
+    c.cells[0] = c.cells[1] = c.cells[2] = cells
     c.alpha = 2e4
     c.flags |= F_COLLIDE | F_LARMOR | F_NORMALISE | F_MAJORANA | F_KNIFE
     sim = Simulation(run, c)
@@ -121,3 +124,5 @@ def test_step_records_match_the_oracle_with_collisions():
         for k in ("pos", "vel", "step", "fate"):
             np.testing.assert_array_equal(eg[k], eo[k])
     assert total > 0 and np.count_nonzero(eg["step"] >= 0) > 0
+    if cells == 3:
+        assert np.diff(sim.cell_starts())[:-1].max() > 1153
