@@ -15,6 +15,8 @@ Datasets (reference names, including its spelling of simuatedTime):
   per frame: atomNumber, simuatedTime (1, 1)
 Frames whose atom count fell (atoms were lost) are padded at the end of the atom axis: NaN for
 floating-point datasets, -1 for atomID and cellID, 0 for atomIsSpinUp.
+save_npz() packs the stacked (N, k, t) datasets of a directory into one .npz archive under the
+same names (the file the reference's single HDF5 output stands for), and load_npz() reads it back.
 """
 from __future__ import annotations
 
@@ -110,3 +112,16 @@ def read_snapshots(directory: str) -> dict:
         rows = max(a.shape[0] for a in arrs)
         out[name] = np.stack([_pad(a, rows) for a in arrs], axis=-1)
     return out
+
+
+def save_npz(directory: str, path: str) -> dict:
+    """Every dataset of the frames in `directory`, stacked as (N, k, t), into the archive `path`."""
+    data = read_snapshots(directory)
+    np.savez(path, **data)
+    return data
+
+
+def load_npz(path: str) -> dict:
+    """The (N, k, t) datasets of an archive written by save_npz."""
+    with np.load(path) as z:
+        return {name: z[name] for name in z.files}

@@ -11,7 +11,7 @@ import numpy as np
 
 import oracle
 from cudadsmc_b200 import F_COLLIDE, F_KNIFE, F_LARMOR, F_MAJORANA, F_NORMALISE
-from cudadsmc_b200.snapshots import enable_records, read_snapshots, write_snapshot
+from cudadsmc_b200.snapshots import enable_records, load_npz, read_snapshots, save_npz, write_snapshot
 
 
 def small_cloud():
@@ -72,3 +72,21 @@ def test_snapshot_round_trip_on_the_oracle(tmp_path):
     before = orc2.diagnostics()["collisions"]
     orc2.step(1)
     assert cc.sum() == orc2.diagnostics()["collisions"] - before
+
+
+def test_npz_archive_holds_the_stacked_frames(tmp_path):
+    run, c = small_cloud()
+    orc = oracle.Oracle(run, c)
+    orc.init_cloud(5)
+    enable_records(orc)
+    for frame in range(2):
+        if frame:
+            orc.step(3)
+        write_snapshot(orc, str(tmp_path / "frames"), frame)
+    data = save_npz(str(tmp_path / "frames"), str(tmp_path / "atomData.npz"))
+    back = load_npz(str(tmp_path / "atomData.npz"))
+    assert sorted(back) == sorted(data)
+    for name, arr in data.items():
+        assert back[name].shape == arr.shape and back[name].dtype == arr.dtype, name
+        np.testing.assert_array_equal(back[name], arr)
+    assert back["positions"].shape[-1] == 2
