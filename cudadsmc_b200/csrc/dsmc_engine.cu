@@ -76,6 +76,10 @@ struct dsmc_handle {
     virtual void step(int n) = 0;
     virtual void sync() = 0;
     virtual void diag(int cloud, dsmc_diag* out) = 0;
+    virtual void diag_reserve(int nslots) = 0;
+    virtual void diag_enqueue(int slot) = 0;
+    virtual void diag_collect(int slot, int cloud, dsmc_diag* out) = 0;
+    virtual int64_t diag_copy_bytes() const = 0;
     virtual void get_state(dsmc_state_buffers* out) = 0;
     virtual void set_state(const dsmc_state_buffers* in) = 0;
     virtual void get_cell_starts(int32_t* start, int64_t cap, int64_t* total) = 0;
@@ -213,6 +217,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 
     ~Engine() override {
         drop_graphs();
+        free_diag_slots();
         for (int i = 0; i <= kNumStepKernels; ++i)
             if (ev[i]) cudaEventDestroy(ev[i]);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -581,8 +586,65 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (cloud < -1 || cloud >= nclouds) throw Fail{DSMC_ERR_INVALID, "cloud index out of range"};
         std::vector<CloudDiagDev> g(nclouds);
         CU(cudaMemcpyAsync(g.data(), cdiag.p, nclouds * sizeof(CloudDiagDev), cudaMemcpyDeviceToHost, stream));
+        int err = 0;
+        CU(cudaMemcpyAsync(&err, &ctl.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
         CU(cudaGetLastError());
+        diag_from(g.data(), err, cloud, out);
+    }
+
+    // Diagnostics read back without waiting: each slot of a pinned host ring holds one copy of
+    // every cloud's step totals and the error bits, taken on the stream when it is enqueued; a
+    // collect waits for that copy only (so K steps with a read-back each need not stop the stream).
+    // A slot is the clouds' totals (at the slot's 64-byte aligned start: they hold 128-bit sums),
+    // then this trailer.
+    struct DiagSlotTrailer { int err; int used; };
+    unsigned char* diag_host = nullptr;
+    std::vector<cudaEvent_t> diag_ev;
+    size_t diag_slot_bytes() const {
+        return ((nclouds * sizeof(CloudDiagDev) + sizeof(DiagSlotTrailer) + 63) / 64) * 64;
+    }
+    void free_diag_slots() {
+        for (cudaEvent_t e : diag_ev) cudaEventDestroy(e);
+        diag_ev.clear();
+        if (diag_host) cudaFreeHost(diag_host);
+        diag_host = nullptr;
+    }
+    void diag_reserve(int nslots) override {
+        if (nslots < 1 || nslots > (1 << 16)) throw Fail{DSMC_ERR_INVALID, "diagnostics slots must be in [1, 65536]"};
+        if ((int)diag_ev.size() >= nslots) return;
+        sync();
+        free_diag_slots();
+        CU(cudaHostAlloc((void**)&diag_host, (size_t)nslots * diag_slot_bytes(), cudaHostAllocDefault));
+        memset(diag_host, 0, (size_t)nslots * diag_slot_bytes());
+        diag_ev.resize(nslots);
+        for (auto& e : diag_ev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    int64_t diag_copy_bytes() const override { return (int64_t)(nclouds * sizeof(CloudDiagDev) + sizeof(int)); }
+    CloudDiagDev* diag_slot(int slot) {
+        return reinterpret_cast<CloudDiagDev*>(diag_host + (size_t)slot * diag_slot_bytes());
+    }
+    DiagSlotTrailer* diag_trailer(int slot) { return reinterpret_cast<DiagSlotTrailer*>(diag_slot(slot) + nclouds); }
+    void diag_enqueue(int slot) override {
+        if (!initialised) throw Fail{DSMC_ERR_STATE, "diagnostics before init"};
+        if (slot < 0 || slot >= (int)diag_ev.size()) throw Fail{DSMC_ERR_INVALID, "diagnostics slot not reserved"};
+        DiagSlotTrailer* tr = diag_trailer(slot);
+        CU(cudaMemcpyAsync(diag_slot(slot), cdiag.p, nclouds * sizeof(CloudDiagDev), cudaMemcpyDeviceToHost, stream));
+        CU(cudaMemcpyAsync(&tr->err, &ctl.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CU(cudaEventRecord(diag_ev[slot], stream));
+        tr->used = 1;
+    }
+    void diag_collect(int slot, int cloud, dsmc_diag* out) override {
+        if (slot < 0 || slot >= (int)diag_ev.size()) throw Fail{DSMC_ERR_INVALID, "diagnostics slot not reserved"};
+        if (cloud < -1 || cloud >= nclouds) throw Fail{DSMC_ERR_INVALID, "cloud index out of range"};
+        const DiagSlotTrailer* tr = diag_trailer(slot);
+        if (!tr->used) throw Fail{DSMC_ERR_STATE, "diagnostics slot collected before it was enqueued"};
+        CU(cudaEventSynchronize(diag_ev[slot]));
+        diag_from(diag_slot(slot), tr->err, cloud, out);
+    }
+
+    // the diagnostics of `cloud` (-1: all) from a copy of the clouds' step totals
+    void diag_from(const CloudDiagDev* g, int ctl_err, int cloud, dsmc_diag* out) {
         int k0 = cloud < 0 ? 0 : cloud, k1 = cloud < 0 ? nclouds : cloud + 1;
         CloudDiagDev s;
         memset(&s, 0, sizeof(s));
@@ -621,9 +683,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         out->collisions = s.cum_coll;
         out->candidates = s.cum_cand;
         out->atom_steps = s.cum_atom_steps;
-        Ctl h;
-        CU(cudaMemcpy(&h, ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
-        out->error = h.err | err;
+        out->error = ctl_err | err;
     }
 
     void get_state(dsmc_state_buffers* o) override {
@@ -1229,6 +1289,20 @@ DSMC_API dsmc_status dsmc_diagnostics(dsmc_handle* h, int32_t cloud, dsmc_diag* 
     NEED_H;
     if (!out) return DSMC_ERR_INVALID;
     return guard(h, [&] { h->diag(cloud, out); });
+}
+DSMC_API dsmc_status dsmc_diagnostics_reserve(dsmc_handle* h, int32_t nslots) {
+    NEED_H;
+    return guard(h, [&] { h->diag_reserve(nslots); });
+}
+DSMC_API int64_t dsmc_diagnostics_copy_bytes(dsmc_handle* h) { return h ? h->diag_copy_bytes() : 0; }
+DSMC_API dsmc_status dsmc_diagnostics_enqueue(dsmc_handle* h, int32_t slot) {
+    NEED_H;
+    return guard(h, [&] { h->diag_enqueue(slot); });
+}
+DSMC_API dsmc_status dsmc_diagnostics_collect(dsmc_handle* h, int32_t slot, int32_t cloud, dsmc_diag* out) {
+    NEED_H;
+    if (!out) return DSMC_ERR_INVALID;
+    return guard(h, [&] { h->diag_collect(slot, cloud, out); });
 }
 DSMC_API dsmc_status dsmc_get_state(dsmc_handle* h, dsmc_state_buffers* out) {
     NEED_H;

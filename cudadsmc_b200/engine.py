@@ -25,7 +25,9 @@ EXPORTED_SYMBOLS = (
     "dsmc_abi_version", "dsmc_status_string", "dsmc_last_error", "dsmc_preset", "dsmc_create",
     "dsmc_destroy", "dsmc_set_stream", "dsmc_init_cloud", "dsmc_step", "dsmc_synchronize",
     "dsmc_batch_create", "dsmc_batch_step",
-    "dsmc_diagnostics", "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
+    "dsmc_diagnostics", "dsmc_diagnostics_reserve", "dsmc_diagnostics_enqueue", "dsmc_diagnostics_collect",
+    "dsmc_diagnostics_copy_bytes",
+    "dsmc_get_state", "dsmc_set_state", "dsmc_get_cell_starts",
     "dsmc_get_sigvrmax", "dsmc_set_sigvrmax", "dsmc_set_profiling", "dsmc_kernel_times",
     "dsmc_launches_per_step", "dsmc_autotune", "dsmc_autotune_table", "dsmc_set_recording", "dsmc_get_evaporated", "dsmc_get_cell_collisions",
     "dsmc_adjoint_run", "dsmc_adjoint_loss", "dsmc_adjoint_loss_parts",
@@ -64,6 +66,10 @@ def load_library(path: str | None = None) -> C.CDLL:
         "dsmc_batch_step": (i32, [vp, i32]),
         "dsmc_synchronize": (i32, [vp]),
         "dsmc_diagnostics": (i32, [vp, i32, C.POINTER(Diag)]),
+        "dsmc_diagnostics_reserve": (i32, [vp, i32]),
+        "dsmc_diagnostics_enqueue": (i32, [vp, i32]),
+        "dsmc_diagnostics_collect": (i32, [vp, i32, i32, C.POINTER(Diag)]),
+        "dsmc_diagnostics_copy_bytes": (C.c_int64, [vp]),
         "dsmc_get_state": (i32, [vp, C.POINTER(StateBuffers)]),
         "dsmc_set_state": (i32, [vp, C.POINTER(StateBuffers)]),
         "dsmc_get_cell_starts": (i32, [vp, C.POINTER(C.c_int32), i64, C.POINTER(i64)]),
@@ -169,6 +175,24 @@ class Simulation:
     def diagnostics(self, cloud: int = -1) -> dict:
         d = Diag()
         self._check(self.lib.dsmc_diagnostics(self._h, int(cloud), C.byref(d)))
+        return d.as_dict()
+
+    def reserve_diagnostics(self, nslots: int) -> None:
+        """Pinned host slots for diagnostics_enqueue / diagnostics_collect."""
+        self._check(self.lib.dsmc_diagnostics_reserve(self._h, int(nslots)))
+
+    def diagnostics_enqueue(self, slot: int) -> None:
+        """Copies the current step totals into `slot` on the stream, without waiting."""
+        self._check(self.lib.dsmc_diagnostics_enqueue(self._h, int(slot)))
+
+    def diagnostics_copy_bytes(self) -> int:
+        """Bytes one diagnostics_enqueue copies from the device."""
+        return int(self.lib.dsmc_diagnostics_copy_bytes(self._h))
+
+    def diagnostics_collect(self, slot: int, cloud: int = -1) -> dict:
+        """The diagnostics as they were when `slot` was enqueued (waits for that copy only)."""
+        d = Diag()
+        self._check(self.lib.dsmc_diagnostics_collect(self._h, int(slot), int(cloud), C.byref(d)))
         return d.as_dict()
 
     # -- state -------------------------------------------------------------------------------------

@@ -191,6 +191,20 @@ DSMC_API dsmc_status dsmc_synchronize(dsmc_handle* h);
 /* cloud >= 0: that cloud; cloud == -1: sums over all clouds (temperature from the sums). */
 DSMC_API dsmc_status dsmc_diagnostics(dsmc_handle* h, int32_t cloud, dsmc_diag* out);
 
+/* Diagnostics read back without stopping the stream (a loop that reads every step's totals, as
+ * the reference's main loop prints them, then keeps the GPU busy).  dsmc_diagnostics_reserve
+ * allocates nslots slots of pinned host memory (once; a larger count reallocates, after a
+ * synchronize).  dsmc_diagnostics_enqueue(h, slot) copies every cloud's step totals and the error
+ * bits into that slot on the handle's stream and returns at once; dsmc_diagnostics_collect(h, slot,
+ * cloud, out) waits for that copy and fills *out exactly as dsmc_diagnostics would have at the
+ * enqueue (DSMC_ERR_STATE for a slot never enqueued, DSMC_ERR_INVALID outside the reserve).  A slot
+ * enqueued again before it is collected holds the later copy. */
+DSMC_API dsmc_status dsmc_diagnostics_reserve(dsmc_handle* h, int32_t nslots);
+DSMC_API dsmc_status dsmc_diagnostics_enqueue(dsmc_handle* h, int32_t slot);
+DSMC_API dsmc_status dsmc_diagnostics_collect(dsmc_handle* h, int32_t slot, int32_t cloud, dsmc_diag* out);
+/* bytes one dsmc_diagnostics_enqueue copies from the device (0 for a null handle) */
+DSMC_API int64_t dsmc_diagnostics_copy_bytes(dsmc_handle* h);
+
 DSMC_API dsmc_status dsmc_get_state(dsmc_handle* h, dsmc_state_buffers* out);
 DSMC_API dsmc_status dsmc_set_state(dsmc_handle* h, const dsmc_state_buffers* in);
 

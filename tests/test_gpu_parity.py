@@ -407,3 +407,27 @@ def test_reinit_with_another_seed_matches_a_fresh_handle():
     sa, sb = a.get_state(), b.get_state()
     for k in ("pos", "vel", "psi"):
         np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_diagnostics_enqueued_each_step_equal_the_synchronous_ones():
+    # dsmc_diagnostics_enqueue copies a step's totals without waiting; collecting them afterwards
+    # gives, slot by slot, exactly what dsmc_diagnostics returned after the same step of a twin run
+    run, c = scaled(2, n=30000, cells=24, flags=ALL, alpha=4000.0)
+    a, b = Simulation(run, c), Simulation(run, c)
+    a.init_cloud(21)
+    b.init_cloud(21)
+    a.reserve_diagnostics(6)
+    sync = []
+    for k in range(6):
+        a.step(1)
+        a.diagnostics_enqueue(k)
+        b.step(1)
+        sync.append(b.diagnostics())
+    for k in range(6):
+        assert a.diagnostics_collect(k) == sync[k], k
+    with pytest.raises(DSMCError):
+        a.diagnostics_collect(6)  # outside the reserve
+    a.reserve_diagnostics(8)  # grows: the new slots were never enqueued
+    with pytest.raises(DSMCError):
+        a.diagnostics_collect(7)
+    assert a.diagnostics_copy_bytes() > 0
