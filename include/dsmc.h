@@ -118,7 +118,11 @@ typedef struct dsmc_params {
     double hbar;           /* 0 -> 1.05457148e-34 (CUDADSMC/include/deviceSystemParameters.cuh:18) */
     double kB;             /* 0 -> 1.3806503e-23 */
     uint64_t seed;         /* Philox key for init (overridden by dsmc_init_cloud) and collisions */
-    int32_t tile_atoms;    /* nominal atoms per tile (0 -> engine default) */
+    int32_t tile_atoms;    /* nominal atoms per tile (0 -> engine default; 128 .. tile capacity - 128).
+                              Any cell occupancy is accepted: a grid cell of more atoms than a
+                              tile stages beside a minimal tile (1153 in FP32, 897 in FP64) is
+                              split across tiles and collided by its own kernel, bit for bit as
+                              inside a tile. */
     int32_t use_graphs;    /* 1 -> replay captured CUDA graphs in dsmc_step (default), 0 -> plain launches */
     int32_t step_blocks_per_sm; /* blocks of the step kernel per SM (0 -> as many as fit) */
     int32_t reserved0;
