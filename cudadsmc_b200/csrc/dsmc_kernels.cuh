@@ -62,7 +62,7 @@ constexpr int MV_CHUNK = 64;  // grid-stride kernels over the mover list
 
 struct __align__(16) TilePartial {
     i128 sum_v2, sum_B, evap_v2, evap_B;
-    long long n_alive, n_maj, n_knife, coll, cand, ovf_stayers, pad1, pad2;
+    long long n_alive, n_maj, n_knife, coll, cand, pad0, pad1, pad2;
 };
 
 // Per-cloud totals of one step, gathered in ACC_BUCKETS buckets per cloud (tile b adds into bucket
@@ -108,7 +108,6 @@ struct Ctl {
     int err;
     int movers[2];  // movers listed by the step of each parity (the other parity's is cleared by the scan)
     int novf[2];    // tiles listed in ovf_list by the step of each parity
-    int ovf_lo[2];  // lowest listed tile: tile_ovf_carry holds the carries from there on
     int scan_done;    // scan_cells blocks finished (the last one runs the top level and clears it)
     int max_cell;     // largest coming grid-cell count, gathered by scan_cells (cleared by its top level)
     int tile_T[2];    // nominal tile size of the tiling built for each parity
@@ -308,7 +307,7 @@ __device__ __forceinline__ void block_reduce_acc(StepAcc& a, StepAcc* sm, TilePa
         if (lane == 0) {
             out.sum_v2 = w.sum_v2; out.sum_B = w.sum_B; out.evap_v2 = 0; out.evap_B = 0;
             out.n_alive = w.n_alive; out.n_maj = 0; out.n_knife = 0;
-            out.coll = w.coll; out.cand = w.cand; out.ovf_stayers = 0;
+            out.coll = w.coll; out.cand = w.cand; out.pad0 = 0;
             out.pad1 = 0; out.pad2 = 0;
         }
     }
@@ -328,7 +327,6 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
     t.n_knife = warp_sum_ll(t.n_knife);
     t.coll = warp_sum_ll(t.coll);
     t.cand = warp_sum_ll(t.cand);
-    t.ovf_stayers = warp_sum_ll(t.ovf_stayers);
     if (lane == 0) sm[warp] = t;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -342,7 +340,6 @@ __device__ __forceinline__ void block_reduce_partial(TilePartial& t, TilePartial
             t.n_knife += sm[w].n_knife;
             t.coll += sm[w].coll;
             t.cand += sm[w].cand;
-            t.ovf_stayers += sm[w].ovf_stayers;
         }
     }
     __syncthreads();
@@ -388,7 +385,7 @@ __device__ __forceinline__ i128 from_limbs(const unsigned long long* l) {
 __device__ __forceinline__ void zero_partial(TilePartial& t) {
     t.sum_v2 = 0; t.sum_B = 0; t.evap_v2 = 0; t.evap_B = 0;
     t.n_alive = 0; t.n_maj = 0; t.n_knife = 0; t.coll = 0; t.cand = 0;
-    t.ovf_stayers = 0; t.pad1 = 0; t.pad2 = 0;
+    t.pad0 = 0; t.pad1 = 0; t.pad2 = 0;
 }
 
 template <class R>
@@ -1347,7 +1344,6 @@ __device__ void ovf_carries(const Args<R>& A) {
     }
     __syncthreads();
     const int lo = s_lo, hi = s_hi;
-    if (threadIdx.x == 0) A.ctl->ovf_lo[p] = lo;
     constexpr int IT = 16;
     for (int base = lo; base <= hi; base += BLOCK * IT) {
         const int i0 = base + threadIdx.x * IT;
