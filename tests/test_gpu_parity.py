@@ -431,3 +431,26 @@ def test_diagnostics_enqueued_each_step_equal_the_synchronous_ones():
     with pytest.raises(DSMCError):
         a.diagnostics_collect(7)
     assert a.diagnostics_copy_bytes() > 0
+
+
+def test_every_atom_lost_then_empty_steps():
+    # a knife at 0.02 kT removes the whole cloud in the first step; the empty cloud keeps
+    # stepping (no tiles, no cells occupied) beside a second cloud that keeps its atoms, the
+    # evaporated energy and counts equal the oracle's, and a state of zero atoms can be set
+    run, c = scaled(2, n=5000, cells=16, flags=ALL, alpha=2e4)
+    c.knife_nknots = 1
+    c.knife_step[0] = 0.0
+    c.knife_eta[0] = 0.02
+    run2, c1 = scaled(2, n=3000, cells=12, flags=F_COLLIDE | F_LARMOR, alpha=2e4)
+    c1.stream_id = 1
+    sim, orc = run_pair(run, [c, c1], 6, check_every=[1, 1, 4])
+    assert sim.diagnostics(0)["n_alive"] == 0 and sim.diagnostics(0)["n_evaporated"] == 5000
+    assert sim.diagnostics(1)["n_alive"] == 3000
+    # set_state with no atoms at all, then steps
+    z = np.zeros((0, 4), dtype=np.float32)
+    for s in (sim, orc):
+        s.set_state(z, z, z, [0, 0])
+    sim.step(2)
+    orc.step(2)
+    assert_same(sim, orc)
+    assert sim.diagnostics()["n_alive"] == 0
