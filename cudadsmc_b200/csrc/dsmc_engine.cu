@@ -180,6 +180,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaGetDevice(&dev));
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         smem_tile = (size_t)CAP * (2 * sizeof(R4) + 2 * sizeof(int) + sizeof(uint16_t));
+        CU(cudaFuncSetAttribute(dense_collide<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, DENSE_SMEM_BYTES));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_tile));
         CU(cudaFuncSetAttribute(step_pass<R, BLOCK, CAP, MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -355,7 +356,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     // ------------------------------------------------------------------ launches
     void launch_step_kernel(int which, const Args<R>& A) {
         switch (which) {
-        case 0: dense_collide<R><<<DENSE_GRID, DENSE_BLOCK, 0, stream>>>(A); break;
+        case 0: dense_collide<R><<<DENSE_GRID, DENSE_BLOCK, DENSE_SMEM_BYTES, stream>>>(A); break;
         case 1:
             if (nclouds == 1)
                 step_pass<R, BLOCK, CAP, MINB, true><<<step_grid(), BLOCK, smem_tile, stream>>>(A);

@@ -508,54 +508,97 @@ constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
 
 // ---------------------------------------------------------------------------------------------
 // dense_collide: the NTC collisions of the step's dense grid cells (more atoms than a tile stages
-// beside a minimal tile), which step_pass leaves out.  One thread per cell runs the same serial
-// loop as a cell inside a tile -- same collide_cell code, Philox words and order, so the same
-// result bit for bit -- on the velocities in global memory, reached through the sorted order's
-// permutation, and adds its counts to the cloud's totals.  Launched before step_pass, which then
-// gathers the collided velocities; cells are independent, so colliding them here or inside a tile
-// is the same.  With no dense cell (the usual case) its blocks read the count and return.
+// beside a minimal tile), which step_pass leaves out.  One block per listed cell (a grid-stride
+// loop over the list): the block gathers the cell's velocities through the sorted order's
+// permutation into shared memory, one thread runs the same serial loop as a cell inside a tile --
+// same collide_cell code, Philox words and order, so the same result bit for bit -- and the block
+// writes them back.  A cell larger than the block's shared memory (dense_smem_atoms) is collided by
+// that thread on the velocities in global memory.  Launched before step_pass, which then gathers
+// the collided velocities; cells are independent, so colliding them here or inside a tile is the
+// same.  With no dense cell (the usual case) its blocks read the count and return.
 // ---------------------------------------------------------------------------------------------
-constexpr int DENSE_BLOCK = 128;
+constexpr int DENSE_BLOCK = 512;
 constexpr int DENSE_GRID = 148;
+constexpr int DENSE_SMEM_BYTES = 200 * 1024;  // dynamic shared memory of a dense_collide block
 template <class R>
 __global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
     typedef typename V4T<R>::type R4;
+    extern __shared__ __align__(16) unsigned char dense_smem[];
+    R4* s_v = reinterpret_cast<R4*>(dense_smem);
     const int p = A.parity;
     const int nd = min(A.ctl->ndense[p], A.dense_cap);
     if (nd == 0) return;
     const int step = A.ctl->step[p];
     if (step % A.collide_every != 0) return;
     const int n_now = A.ctl->n[p];
-    for (int i = blockIdx.x * DENSE_BLOCK + threadIdx.x; i < nd; i += gridDim.x * DENSE_BLOCK) {
+    const int cap = (int)(DENSE_SMEM_BYTES / sizeof(R4));
+    R4* const vel = const_cast<R4*>(A.vel_in);
+    for (int i = blockIdx.x; i < nd; i += gridDim.x) {  // block-uniform: every value below is
         const int2 d = A.dense_list[i];
         const int c = d.x, k = d.y;
         if (c < 0 || c >= A.total_cells || k < 0 || k >= A.nclouds) {
-            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_INCONSISTENT);
             continue;
         }
         const CloudPhys<R>& P = A.clouds[k];
         if (!(P.flags & F_COLLIDE)) continue;
         const int c_beg = A.old_start[c], n = A.old_start[c + 1] - c_beg;
         if (c_beg < 0 || n < 0 || c_beg + n > n_now) {
-            atomicOr(&A.ctl->err, EB_INCONSISTENT);
+            if (threadIdx.x == 0) atomicOr(&A.ctl->err, EB_INCONSISTENT);
             continue;
         }
-        R svm = A.sigvrmax[c];
-        GatherVel<R> g{const_cast<R4*>(A.vel_in), A.src_in + c_beg, A.capacity, &A.ctl->err};
-        CollideResult<R> cr;
-        if (A.clog_ij) {
-            GatherCollisionLog<R> lg{A.pos_in, A.src_in + c_beg, A.capacity, A.clog_ij, A.clog_n, A.clog_count,
-                                     A.clog_cap, &A.ctl->err};
-            cr = collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base),
-                                                                     (uint32_t)step, A.seed, &lg);
-        } else {
-            cr = collide_cell<R, GatherVel<R>>(g, n, svm, P, (uint32_t)(c - P.cell_base), (uint32_t)step, A.seed);
+        const int* src = A.src_in + c_beg;
+        const bool staged = n <= cap;
+        constexpr int U = 4;  // gathers in flight per thread: the indices of four atoms, then their velocities
+        if (staged) {
+            for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
+                int s[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : 0;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int t = t0 + u * DENSE_BLOCK;
+                    if (t >= n) continue;
+                    if (s[u] >= 0 && s[u] < A.capacity) s_v[t] = vel[s[u]];
+                    else atomicOr(&A.ctl->err, EB_INCONSISTENT);
+                }
+            }
+            __syncthreads();
         }
-        A.sigvrmax[c] = svm;
-        CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
-        if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
-        if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
-        if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
+        if (threadIdx.x == 0) {
+            R svm = A.sigvrmax[c];
+            GatherCollisionLog<R> lg{A.pos_in, src, A.capacity, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap,
+                                     &A.ctl->err};
+            CollideResult<R> cr;
+            const uint32_t lc = (uint32_t)(c - P.cell_base);
+            if (staged) {
+                cr = A.clog_ij ? collide_cell<R, R4*, GatherCollisionLog<R>>(s_v, n, svm, P, lc, (uint32_t)step,
+                                                                            A.seed, &lg)
+                               : collide_cell<R>(s_v, n, svm, P, lc, (uint32_t)step, A.seed);
+            } else {
+                GatherVel<R> g{vel, src, A.capacity, &A.ctl->err};
+                cr = A.clog_ij ? collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, lc,
+                                                                                     (uint32_t)step, A.seed, &lg)
+                               : collide_cell<R, GatherVel<R>>(g, n, svm, P, lc, (uint32_t)step, A.seed);
+            }
+            A.sigvrmax[c] = svm;
+            CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
+            if (cr.accepted) atomicAdd(&bucket->coll, (unsigned long long)cr.accepted);
+            if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
+            if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
+        }
+        if (staged) {
+            __syncthreads();
+            for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
+                int s[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : -1;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (s[u] >= 0 && s[u] < A.capacity) vel[s[u]] = s_v[t0 + u * DENSE_BLOCK];
+            }
+            __syncthreads();  // the staging area is reused by the block's next cell
+        }
     }
 }
 
