@@ -75,10 +75,12 @@ constexpr int ACC_BUCKETS = 16;
 constexpr int MIN_TILE = 128;
 // A grid cell of more than dense_threshold(CAP) atoms is dense: like the overflow cell it is split
 // across tiles (a tile begins at each nominal start inside it), and dense_collide collides it
-// before step_pass, reaching its atoms through the sorted order.  Every other grid cell fits a
-// tile, so a tiling of nominal size T >= MIN_TILE (tiles of at most T - 1 + dense_threshold
-// atoms) always fits the staging capacity.
-__host__ __device__ constexpr int dense_threshold(int cap) { return cap - MIN_TILE + 1; }
+// before step_pass, reaching its atoms through the sorted order.  A tiling of nominal size T holds
+// tiles of at most T - 1 + (largest other grid cell) atoms, so the scan's T = CAP + 1 - that
+// count never falls below DENSE_MIN_TILE (cells fuller than that go to dense_collide, which
+// stages a cell in shared memory, rather than shrinking every tile of the step).
+constexpr int DENSE_MIN_TILE = 512;
+__host__ __device__ constexpr int dense_threshold(int cap) { return cap + 1 - DENSE_MIN_TILE; }
 // tile_ovf word of a tile: the stayers of its last cell when that cell continues into the next
 // tile, and TILE_WHOLE when the tile lies inside that cell (it also began inside it)
 constexpr int TILE_WHOLE = 1 << 30;

@@ -63,7 +63,7 @@ def test_recorded_collisions_of_dense_cells():
     c.cells[0] = c.cells[1] = c.cells[2] = 2
     sim = Simulation(run, c)
     sim.init_cloud(97)
-    assert np.diff(sim.cell_starts())[:-1].max() > 1153
+    assert np.diff(sim.cell_starts())[:-1].max() > 769
     g = sim.adjoint_run(100, checkpoint_every=32, precision=FP64, sigmoid_width_kT=0.2)
     rec = sim.adjoint_export()
     ij = rec["ij"]

@@ -125,4 +125,4 @@ def test_step_records_match_the_oracle_with_collisions(cells):
             np.testing.assert_array_equal(eg[k], eo[k])
     assert total > 0 and np.count_nonzero(eg["step"] >= 0) > 0
     if cells == 3:
-        assert np.diff(sim.cell_starts())[:-1].max() > 1153
+        assert np.diff(sim.cell_starts())[:-1].max() > 769

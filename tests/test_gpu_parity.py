@@ -270,7 +270,7 @@ def test_dense_cells_and_tiny_clouds():
     assert occ[:-1].max() > 300
 
 
-DENSE_FP32 = 1280 - 128 + 1  # grid cells above this many atoms are split across tiles (FP32)
+DENSE_FP32 = 1280 + 1 - 512  # grid cells above this many atoms are split across tiles (FP32)
 
 
 @pytest.mark.parametrize("precision", [FP32, FP64])
@@ -298,7 +298,7 @@ def test_dense_cells_split_across_small_tiles():
     assert sim.diagnostics(0)["collisions"] > 0 and sim.diagnostics(1)["collisions"] > 0
 
 
-@pytest.mark.parametrize("precision,threshold", [(FP32, 1153), (FP64, 897)])
+@pytest.mark.parametrize("precision,threshold", [(FP32, 769), (FP64, 513)])
 def test_cells_crossing_the_dense_threshold(precision, threshold):
     # a hot periodic box whose 27 cells hold the dense threshold on average: every step some cells
     # become dense (split across tiles, collided by dense_collide) and others stop being
