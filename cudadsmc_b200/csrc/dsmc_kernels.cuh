@@ -429,34 +429,6 @@ template <class R> struct TileCollisionLog {
     }
 };
 
-// The velocities of a dense cell in global memory: element i of the cell is the atom at sorted
-// position first + i, stored at src[first + i] (an index outside the state flags the step
-// inconsistent and reads atom 0 without writing it)
-template <class R> struct GatherVel {
-    typedef typename V4T<R>::type R4;
-    R4* vel;
-    const int* src;  // the cell's entries of the gather permutation
-    int capacity;
-    int* err;
-    __device__ __forceinline__ int at(uint32_t i) const {
-        const int s = src[i];
-        if (s < 0 || s >= capacity) {
-            atomicOr(err, EB_INCONSISTENT);
-            return -1;
-        }
-        return s;
-    }
-};
-template <class R> __device__ __forceinline__ typename V4T<R>::type vload(const GatherVel<R>& g, uint32_t i) {
-    const int s = g.at(i);
-    return g.vel[s < 0 ? 0 : s];
-}
-template <class R>
-__device__ __forceinline__ void vstore(const GatherVel<R>& g, uint32_t i, const typename V4T<R>::type& v) {
-    const int s = g.at(i);
-    if (s >= 0) g.vel[s] = v;
-}
-
 // the collision record of a dense cell: atom ids read through the same permutation
 template <class R> struct GatherCollisionLog {
     typedef typename V4T<R>::type R4;
@@ -510,12 +482,12 @@ constexpr unsigned long long LB_TIMEOUT_NS = 1000000000ull;
 
 // ---------------------------------------------------------------------------------------------
 // dense_collide: the NTC collisions of the step's dense grid cells (more atoms than a tile stages
-// beside a minimal tile), which step_pass leaves out.  One block per listed cell (a grid-stride
+// beside a 512-atom tile), which step_pass leaves out.  One block per listed cell (a grid-stride
 // loop over the list): the block gathers the cell's velocities through the sorted order's
 // permutation into shared memory, one thread runs the same serial loop as a cell inside a tile --
 // same collide_cell code, Philox words and order, so the same result bit for bit -- and the block
-// writes them back.  A cell larger than the block's shared memory (dense_smem_atoms) is collided by
-// that thread on the velocities in global memory.  Launched before step_pass, which then gathers
+// writes them back.  A cell larger than the block's shared memory is gathered the same way into
+// its own slots of the step's output velocity buffer instead (contiguous, in L2).  Launched before step_pass, which then gathers
 // the collided velocities; cells are independent, so colliding them here or inside a tile is the
 // same.  With no dense cell (the usual case) its blocks read the count and return.
 // ---------------------------------------------------------------------------------------------
@@ -550,38 +522,33 @@ __global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
             continue;
         }
         const int* src = A.src_in + c_beg;
-        const bool staged = n <= cap;
+        // the cell's velocities, contiguous: in shared memory when they fit, else in the cell's
+        // slots of the buffer this step's step_pass writes later (free until then)
+        R4* const stage_v = n <= cap ? s_v : A.vel_out + c_beg;
         constexpr int U = 4;  // gathers in flight per thread: the indices of four atoms, then their velocities
-        if (staged) {
-            for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
-                int s[U];
+        for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
+            int s[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : 0;
+            for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : 0;
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int t = t0 + u * DENSE_BLOCK;
-                    if (t >= n) continue;
-                    if (s[u] >= 0 && s[u] < A.capacity) s_v[t] = vel[s[u]];
-                    else atomicOr(&A.ctl->err, EB_INCONSISTENT);
-                }
+            for (int u = 0; u < U; ++u) {
+                const int t = t0 + u * DENSE_BLOCK;
+                if (t >= n) continue;
+                if (s[u] >= 0 && s[u] < A.capacity) stage_v[t] = vel[s[u]];
+                else atomicOr(&A.ctl->err, EB_INCONSISTENT);
             }
-            __syncthreads();
         }
+        __syncthreads();
         if (threadIdx.x == 0) {
             R svm = A.sigvrmax[c];
-            GatherCollisionLog<R> lg{A.pos_in, src, A.capacity, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap,
-                                     &A.ctl->err};
-            CollideResult<R> cr;
             const uint32_t lc = (uint32_t)(c - P.cell_base);
-            if (staged) {
-                cr = A.clog_ij ? collide_cell<R, R4*, GatherCollisionLog<R>>(s_v, n, svm, P, lc, (uint32_t)step,
-                                                                            A.seed, &lg)
-                               : collide_cell<R>(s_v, n, svm, P, lc, (uint32_t)step, A.seed);
+            CollideResult<R> cr;
+            if (A.clog_ij) {
+                GatherCollisionLog<R> lg{A.pos_in, src, A.capacity, A.clog_ij, A.clog_n, A.clog_count, A.clog_cap,
+                                         &A.ctl->err};
+                cr = collide_cell<R, R4*, GatherCollisionLog<R>>(stage_v, n, svm, P, lc, (uint32_t)step, A.seed, &lg);
             } else {
-                GatherVel<R> g{vel, src, A.capacity, &A.ctl->err};
-                cr = A.clog_ij ? collide_cell<R, GatherVel<R>, GatherCollisionLog<R>>(g, n, svm, P, lc,
-                                                                                     (uint32_t)step, A.seed, &lg)
-                               : collide_cell<R, GatherVel<R>>(g, n, svm, P, lc, (uint32_t)step, A.seed);
+                cr = collide_cell<R>(stage_v, n, svm, P, lc, (uint32_t)step, A.seed);
             }
             A.sigvrmax[c] = svm;
             CloudAccum* bucket = A.accum + k * ACC_BUCKETS + (i & (ACC_BUCKETS - 1));
@@ -589,18 +556,16 @@ __global__ void __launch_bounds__(DENSE_BLOCK) dense_collide(Args<R> A) {
             if (cr.candidates) atomicAdd(&bucket->cand, (unsigned long long)cr.candidates);
             if (A.rec_cell_coll) A.rec_cell_coll[c] = make_int2(step, cr.accepted);
         }
-        if (staged) {
-            __syncthreads();
-            for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
-                int s[U];
+        __syncthreads();
+        for (int t0 = threadIdx.x; t0 < n; t0 += DENSE_BLOCK * U) {
+            int s[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : -1;
+            for (int u = 0; u < U; ++u) s[u] = t0 + u * DENSE_BLOCK < n ? src[t0 + u * DENSE_BLOCK] : -1;
 #pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (s[u] >= 0 && s[u] < A.capacity) vel[s[u]] = s_v[t0 + u * DENSE_BLOCK];
-            }
-            __syncthreads();  // the staging area is reused by the block's next cell
+            for (int u = 0; u < U; ++u)
+                if (s[u] >= 0 && s[u] < A.capacity) vel[s[u]] = stage_v[t0 + u * DENSE_BLOCK];
         }
+        __syncthreads();  // the staging area is reused by the block's next cell
     }
 }
 
