@@ -125,6 +125,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
     DevBuf<int> src[2];
     DevBuf<int> Lc, Ic, mover_base, in_list, tile_ovf, tile_ovf_carry, ovf_list, tile_cell;
     DevBuf<int2> dense_list;
+    DevBuf<int> cloud_lost;  // per cloud: atoms removed by the current step (read and cleared by its scan)
     int dense_cap = 0;  // dense cells a step can hold: each has more than dense_threshold(CAP) atoms
     DevBuf<int4> mrec;
     DevBuf<int2> keys;
@@ -279,6 +280,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         tile_cell.alloc(max_tiles);
         dense_cap = capacity / (dense_threshold(CAP) + 1) + 1;
         dense_list.alloc(dense_cap);
+        cloud_lost.alloc(nclouds);
+        CU(cudaMemset(cloud_lost.p, 0, nclouds * sizeof(int)));
         sigvrmax.alloc(total_cells);
         accum.alloc((size_t)nclouds * ACC_BUCKETS);
         CU(cudaMemset(accum.p, 0, (size_t)nclouds * ACC_BUCKETS * sizeof(CloudAccum)));
@@ -337,6 +340,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             A.tile_split_next = tile_split[q].p;
             A.tile_ovf = tile_ovf.p; A.tile_ovf_carry = tile_ovf_carry.p; A.ovf_list = ovf_list.p;
             A.tile_cell = tile_cell.p; A.dense_list = dense_list.p; A.dense_cap = dense_cap;
+            A.cloud_lost = cloud_lost.p;
             A.accum = accum.p;
             A.clouds = d_phys.p; A.cdyn = cdyn.p; A.cdiag = cdiag.p; A.ctl = ctl.p;
             A.one = phys[0];
@@ -371,8 +375,14 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
 
     // the cell scan with `extra` leading blocks (overflow carries and step totals) before the scan blocks
     void launch_scan(const Args<R>& A, int extra) {
-        if (cell_items == 16) scan_cells<R, CELL_BLOCK, 16><<<extra + nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
-        else scan_cells<R, CELL_BLOCK, 8><<<extra + nscan_blocks, CELL_BLOCK, 0, stream>>>(A);
+        const int g = extra + nscan_blocks;
+        if (nclouds == 1) {
+            if (cell_items == 16) scan_cells<R, CELL_BLOCK, 16, false><<<g, CELL_BLOCK, 0, stream>>>(A);
+            else scan_cells<R, CELL_BLOCK, 8, false><<<g, CELL_BLOCK, 0, stream>>>(A);
+        } else {
+            if (cell_items == 16) scan_cells<R, CELL_BLOCK, 16, true><<<g, CELL_BLOCK, 0, stream>>>(A);
+            else scan_cells<R, CELL_BLOCK, 8, true><<<g, CELL_BLOCK, 0, stream>>>(A);
+        }
     }
 
     void enqueue_step(int p) {
@@ -488,6 +498,7 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         CU(cudaMemsetAsync(start[1].p, 0, (total_cells + 1) * sizeof(int), stream));
         CU(cudaMemsetAsync(Lc.p, 0, total_cells * sizeof(int), stream));
         CU(cudaMemsetAsync(Ic.p, 0, total_cells * sizeof(int), stream));
+        CU(cudaMemsetAsync(cloud_lost.p, 0, nclouds * sizeof(int), stream));
         // the scan's epoch restarts at 0 with the cleared control block: clear its descriptors too
         CU(cudaMemsetAsync(scan_desc.p, 0, (size_t)nscan_blocks * LB_STRIDE * sizeof(unsigned long long), stream));
         Args<R> A = args[1];

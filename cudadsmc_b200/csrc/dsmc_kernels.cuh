@@ -177,6 +177,10 @@ template <class R> struct Args {
     int* tile_cell;  // per split tile: the cell it begins inside (written by step_pass)
     int2* dense_list;  // (cell, cloud) of each dense grid cell of the coming step (ctl->ndense)
     int dense_cap;
+    // per cloud: atoms the step removed (Majorana, knife, or an unstageable tile), counted per tile
+    // by step_pass; the cell scan starts each cloud's look-back chain from the earlier clouds' old
+    // totals less these (atoms never change clouds), and its top level clears them
+    int* cloud_lost;
     CloudAccum* accum;  // nclouds x ACC_BUCKETS
     const CloudPhys<R>* clouds;
     CloudPhys<R> one;   // the parameters of cloud 0, read from the kernel parameters by one-cloud runs
@@ -648,7 +652,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 atomicAdd(&A.Lc[cell_of(P, q.x, q.y, q.z, box)], 1);
                 A.keys[tb + t] = make_int2(-1, KIND_LOST);
             }
-            if (threadIdx.x == 0) A.tile_ovf[b] = 0;
+            if (threadIdx.x == 0) {
+                A.tile_ovf[b] = 0;
+                const int dropped = min(L, nprev - tb);
+                if (!ONE && dropped > 0) atomicAdd(&A.cloud_lost[cloud], dropped);
+            }
             continue;
         }
         const R cut = s_cut;
@@ -907,6 +915,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 if (i < A.max_tiles) A.ovf_list[i] = b;
             }
             accum_tile(bucket, tot);
+            const unsigned long long nlost = s_lost.n_maj + s_lost.n_knife;
+            if (!ONE && nlost) atomicAdd(&A.cloud_lost[cloud], (int)nlost);  // one cloud: its scan needs none
             accum_lost(bucket, s_lost);
         }
         // stayers whose cell run began in an earlier chunk: add the stayers of that run there
@@ -1323,6 +1333,7 @@ __device__ void scan_top_block(const Args<R>& A, unsigned epoch) {
         A.ctl->scan_ticket = 0;
         A.ctl->scan_epoch = epoch + 1;
     }
+    for (int k = threadIdx.x; k < A.nclouds; k += BLOCK) A.cloud_lost[k] = 0;  // read by this scan's cloud heads
 }
 
 // Stayers of split cells (overflow and dense cells), run by one block of a physics-step scan_cells
@@ -1414,7 +1425,8 @@ __device__ void ovf_carries(const Args<R>& A) {
 // the largest grid-cell count, and (last block) the top level.  In a physics step the launch puts
 // scan_extra_blocks(nclouds, CB) blocks ahead of the scan blocks: the overflow-cell carries, then the
 // clouds' step totals, one warp per cloud; after a full sort it carries the scan blocks alone.
-template <class R, int CB, int CELL_ITEMS>
+// MULTI: the handle holds more than one cloud (each cloud's look-back chain starts at its first block)
+template <class R, int CB, int CELL_ITEMS, bool MULTI>
 __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
     constexpr int CELL_CHUNK = CB * CELL_ITEMS;
     __shared__ uint32_t wsum[32];
@@ -1445,6 +1457,7 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
     const int blk = s_blk;
     if (blk < A.nscan_blocks) {
         const int4 hb = A.scan_blk[blk];
+        const int head_blk = MULTI ? A.cloud_first_blk[hb.x] : 0;  // used at the look-back: loaded with the cells
         const int c0 = hb.y, cend = hb.z, c1 = hb.w;  // this block's cells [c0, c1) of a cloud ending at cend
         const int cb = c0 + threadIdx.x * CELL_ITEMS;
         // a block of CELL_CHUNK cells from a 16-byte boundary: vector loads and stores
@@ -1505,6 +1518,14 @@ __global__ void __launch_bounds__(CB, 1024 / CB) scan_cells(Args<R> A) {
             unsigned excl = 0;
             if (blk == 0) {
                 if (lane == 0) lb_store(A.scan_desc, 0, lb_word(epoch, LB_INC, tot));
+            } else if (MULTI && !A.init_mode && blk == head_blk) {
+                // a cloud's first scan block in a physics step: its offset is the earlier clouds' new
+                // totals, each its old total less the step's losses (atoms never change clouds), so
+                // the chain restarts here and no block waits on the blocks of earlier clouds
+                long long part = 0;
+                for (int k2 = lane; k2 < hb.x; k2 += 32) part += A.cdyn[k2].n[A.parity] - A.cloud_lost[k2];
+                excl = (unsigned)warp_sum_ll(part);
+                if (lane == 0) lb_store(A.scan_desc, blk, lb_word(epoch, LB_INC, excl + tot));
             } else {
                 if (lane == 0) lb_store(A.scan_desc, blk, lb_word(epoch, LB_AGG, tot));
                 excl = lb_exclusive(A.scan_desc, blk, epoch, &A.ctl->err);
