@@ -273,14 +273,17 @@ def test_dense_cells_and_tiny_clouds():
 DENSE_FP32 = 1280 + 1 - 512  # grid cells above this many atoms are split across tiles (FP32)
 
 
-@pytest.mark.parametrize("precision", [FP32, FP64])
-def test_one_dense_cell_bit_exact(precision):
-    # 4000 atoms in one cell, more than a tile stages: the cell is split across tiles, its
-    # collisions run in dense_collide through the sorted order, and the result is the oracle's
-    run, c = scaled(2, n=4000, cells=1, flags=F_COLLIDE | F_LARMOR, precision=precision, alpha=2e7)
+@pytest.mark.parametrize("precision,n,alpha", [(FP32, 4000, 2e7), (FP64, 4000, 2e7), (FP32, 16000, 2e6),
+                                             (FP64, 8000, 5e6)])
+def test_one_dense_cell_bit_exact(precision, n, alpha):
+    # one cell holding most of the atoms, more than a tile stages: the cell is split across tiles,
+    # its collisions run in dense_collide -- its velocities gathered into shared memory, or (16000
+    # atoms in FP32, 8000 in FP64: more than the 12800 / 6400 that fit) into its slots of the step's
+    # output buffer -- and the result is the oracle's
+    run, c = scaled(2, n=n, cells=1, flags=F_COLLIDE | F_LARMOR, precision=precision, alpha=alpha)
     sim, orc = run_pair(run, c, 12, check_every=[1, 5, 6])
     occ = np.diff(sim.cell_starts())
-    assert occ[0] > 3000
+    assert occ[0] > 0.75 * n
     assert sim.diagnostics()["collisions"] > 50
 
 
