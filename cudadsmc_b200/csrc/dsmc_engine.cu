@@ -1253,7 +1253,7 @@ DSMC_API dsmc_status dsmc_create(const dsmc_params* run, const dsmc_cloud_params
         if (run->precision == DSMC_FP32)
             *out = new Engine<float, DSMC_FP32_BLOCK, DSMC_FP32_CAP, DSMC_FP32_MINB>(*run, clouds, nclouds);
         else if (run->precision == DSMC_FP64)
-            *out = new Engine<double, 256, 1024, 2>(*run, clouds, nclouds);
+            *out = new Engine<double, 256, 1536, 2>(*run, clouds, nclouds);
         else {
             g_create_error = "precision must be DSMC_FP32 or DSMC_FP64";
             return DSMC_ERR_INVALID;

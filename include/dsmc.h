@@ -120,7 +120,7 @@ typedef struct dsmc_params {
     uint64_t seed;         /* Philox key for init (overridden by dsmc_init_cloud) and collisions */
     int32_t tile_atoms;    /* nominal atoms per tile (0 -> engine default; 128 .. tile capacity - 128).
                               Any cell occupancy is accepted: a grid cell of more atoms than a
-                              tile stages beside a 512-atom tile (769 in FP32, 513 in FP64) is
+                              tile stages beside a 512-atom tile (769 in FP32, 1025 in FP64) is
                               split across tiles and collided by its own kernel, bit for bit as
                               inside a tile. */
     int32_t use_graphs;    /* 1 -> replay captured CUDA graphs in dsmc_step (default), 0 -> plain launches */

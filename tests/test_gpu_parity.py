@@ -301,7 +301,7 @@ def test_dense_cells_split_across_small_tiles():
     assert sim.diagnostics(0)["collisions"] > 0 and sim.diagnostics(1)["collisions"] > 0
 
 
-@pytest.mark.parametrize("precision,threshold", [(FP32, 769), (FP64, 513)])
+@pytest.mark.parametrize("precision,threshold", [(FP32, 769), (FP64, 1025)])
 def test_cells_crossing_the_dense_threshold(precision, threshold):
     # a hot periodic box whose 27 cells hold the dense threshold on average: every step some cells
     # become dense (split across tiles, collided by dense_collide) and others stop being
