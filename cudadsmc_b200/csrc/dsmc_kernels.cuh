@@ -657,6 +657,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) step_pass(const __grid_constant__
                 const int dropped = min(L, nprev - tb);
                 if (!ONE && dropped > 0) atomicAdd(&A.cloud_lost[cloud], dropped);
             }
+            if (!ONE) __syncthreads();  // the shared cloud parameters were read above; the next tile may replace them
             continue;
         }
         const R cut = s_cut;
