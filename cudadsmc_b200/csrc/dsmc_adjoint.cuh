@@ -2,11 +2,16 @@
 //
 // State of the smoothed model: one atom per id (0..n-1), x and v as R4 (fourth lane unused), the
 // spinor psi as R4 (Re u, Im u, Re d, Im d), the survival weight w.  The adjoint state holds
-// ADJ_SEEDS copies (the two loss terms), seed q of atom i at index q n + i.  A step is two launches: the recorded collisions of the step, applied by one
-// thread in recorded order (collisions of different cells touch different atoms; within a cell
-// the recording order is the collision order), then the per-atom move + weight update.  The
-// backward pass walks segments of K steps from the end: it restores the segment's checkpoint,
-// recomputes the segment storing each step's start state, then runs the adjoint steps backwards.
+// ADJ_SEEDS copies (the two loss terms), seed q of atom i at index q n + i.  A step is the recorded
+// collisions of the step, applied by one warp with every atom's collisions in recorded order
+// (collisions of different cells touch different atoms; within a cell the recording order is the
+// collision order), then the per-atom move + weight update; the collisions of the next step run in
+// the move kernel's last block to finish, so a step is one launch.  The backward pass walks
+// segments of K steps from the end: it restores the segment's checkpoint into the first slot of
+// the segment store and recomputes the segment from slot to slot (each slot holds a step's start
+// state), then runs the adjoint steps backwards, each with the adjoint of its collisions in the
+// last block.  The parameter adjoints are summed per block of the adjoint kernels (one slot each,
+// no atomics) and reduced in a fixed order at the end, so gradients repeat bit for bit.
 #ifndef DSMC_ADJOINT_CUH
 #define DSMC_ADJOINT_CUH
 
@@ -34,60 +39,131 @@ template <class S> struct SmoothArgs {
     S4* vb;
     S4* pb;
     S* wb;
-    double* theta_b;   // ADJ_SEEDS x ADJ_NPARAM accumulators
+    double* theta_b;   // ADJ_SEEDS x ADJ_NPARAM results
+    double* theta_part;  // per block of adj_seed / adj_move: ADJ_SEEDS x ADJ_NPARAM partial sums
+    int* done;         // blocks of the running move / adjoint kernel finished (its last block resets it)
     TilePartial* partials;
     SmoothConsts<S> C;
     int n;
 };
 
-// applies the recorded collisions of step t (one thread, recorded order)
-template <class S>
-__global__ void sm_collide(SmoothArgs<S> A, int t, int store_pre) {
+// The recorded collisions of step t, applied by one warp to the velocities v (n atoms): up to 32
+// collisions at a time, one per lane; a collision waits while an earlier one of its batch that shares
+// an atom is still pending, so every atom meets its collisions in recorded order (collisions without
+// a shared atom commute: they touch different velocities).  REVERSE: the adjoint, which walks the
+// step's collisions from the last and pulls the velocity adjoints of both seeds back through each.
+template <class S, bool REVERSE>
+__device__ void warp_collisions(const SmoothArgs<S>& A, typename V4T<S>::type* v, int t, int store_pre) {
     typedef typename V4T<S>::type S4;
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int k = A.off[t]; k < A.off[t + 1]; ++k) {
-        const int i = A.ij[k].x, j = A.ij[k].y;
-        if (i < 0 || i >= A.n || j < 0 || j >= A.n) continue;
-        S4 a = A.v[i], b = A.v[j];
-        if (store_pre) {
-            A.vpre[2 * k] = a;
-            A.vpre[2 * k + 1] = b;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int k0 = A.off[t], k1 = A.off[t + 1];
+    for (int base = 0; base < k1 - k0; base += 32) {
+        const int pos = base + lane;  // position in the order the collisions are applied
+        const int k = REVERSE ? k1 - 1 - pos : k0 + pos;
+        int i = -1, j = -1;
+        if (pos < k1 - k0) {
+            const int2 pr = A.ij[k];
+            i = pr.x;
+            j = pr.y;
         }
-        S vi[3] = {a.x, a.y, a.z}, vj[3] = {b.x, b.y, b.z};
-        const S nn[3] = {(S)A.nv[3 * k], (S)A.nv[3 * k + 1], (S)A.nv[3 * k + 2]};
-        collide_fixed(vi, vj, nn);
-        a.x = vi[0]; a.y = vi[1]; a.z = vi[2];
-        b.x = vj[0]; b.y = vj[1]; b.z = vj[2];
-        A.v[i] = a;
-        A.v[j] = b;
+        int pending = (pos < k1 - k0 && i >= 0 && i < A.n && j >= 0 && j < A.n) ? 1 : 0;
+        while (__any_sync(FULL, pending)) {
+            bool blocked = false;
+            for (int l = 0; l < 31; ++l) {
+                const int pi = __shfl_sync(FULL, i, l), pj = __shfl_sync(FULL, j, l);
+                const int pp = __shfl_sync(FULL, pending, l);
+                if (l < lane && pp && (pi == i || pi == j || pj == i || pj == j)) blocked = true;
+            }
+            if (pending && !blocked) {
+                const S nn[3] = {(S)A.nv[3 * k], (S)A.nv[3 * k + 1], (S)A.nv[3 * k + 2]};
+                if (!REVERSE) {
+                    S4 a = v[i], b = v[j];
+                    if (store_pre) {
+                        A.vpre[2 * k] = a;
+                        A.vpre[2 * k + 1] = b;
+                    }
+                    S vi[3] = {a.x, a.y, a.z}, vj[3] = {b.x, b.y, b.z};
+                    collide_fixed(vi, vj, nn);
+                    a.x = vi[0]; a.y = vi[1]; a.z = vi[2];
+                    b.x = vj[0]; b.y = vj[1]; b.z = vj[2];
+                    v[i] = a;
+                    v[j] = b;
+                } else {
+                    const S4 a = A.vpre[2 * k], b = A.vpre[2 * k + 1];
+                    const S vi[3] = {a.x, a.y, a.z}, vj[3] = {b.x, b.y, b.z};
+                    for (int q = 0; q < ADJ_SEEDS; ++q) {
+                        S4 bi = A.vb[q * A.n + i], bj = A.vb[q * A.n + j];
+                        S vib[3] = {bi.x, bi.y, bi.z}, vjb[3] = {bj.x, bj.y, bj.z};
+                        collide_fixed_adjoint(vi, vj, nn, vib, vjb);
+                        bi.x = vib[0]; bi.y = vib[1]; bi.z = vib[2];
+                        bj.x = vjb[0]; bj.y = vjb[1]; bj.z = vjb[2];
+                        A.vb[q * A.n + i] = bi;
+                        A.vb[q * A.n + j] = bj;
+                    }
+                }
+                pending = 0;
+            }
+            __syncwarp();  // this round's velocities are visible to the lanes that wait for them
+        }
     }
 }
 
-// per-atom move + weight of step t; stores the start state at slot `seg` when seg >= 0
-template <class S>
-__global__ void __launch_bounds__(256) sm_move(SmoothArgs<S> A, S cut, int seg, int last) {
-    typedef typename V4T<S>::type S4;
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= A.n) return;
-    S4 xv = A.x[i], vv = A.v[i], pv = A.psi[i];
-    S w = A.w[i];
-    if (seg >= 0) {
-        const size_t o = (size_t)seg * A.n + i;
-        A.seg_x[o] = xv;
-        A.seg_v[o] = vv;
-        A.seg_psi[o] = pv;
-        A.seg_w[o] = w;
+// Run by every thread of a block at its end: the last block of the grid to get here applies the
+// collisions of step t (REVERSE: their adjoint) once every block's writes are visible.
+template <class S, bool REVERSE>
+__device__ void collisions_in_last_block(const SmoothArgs<S>& A, typename V4T<S>::type* v, int t, int store_pre) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(A.done, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x < 32) {
+        warp_collisions<S, REVERSE>(A, v, t, store_pre);
+        if (threadIdx.x == 0) *A.done = 0;
     }
-    S x[3] = {xv.x, xv.y, xv.z}, v[3] = {vv.x, vv.y, vv.z}, p[4] = {pv.x, pv.y, pv.z, pv.w};
-    const S e = smooth_step(A.C, cut, x, v, p, w);
-    xv.x = x[0]; xv.y = x[1]; xv.z = x[2];
-    vv.x = v[0]; vv.y = v[1]; vv.z = v[2];
-    pv.x = p[0]; pv.y = p[1]; pv.z = p[2]; pv.w = p[3];
-    A.x[i] = xv;
-    A.v[i] = vv;
-    A.psi[i] = pv;
-    A.w[i] = w;
-    if (last) A.e[i] = e;
+}
+
+// the recorded collisions of step t on their own (one warp); slot < 0: the state arrays, else the
+// segment slot
+template <class S>
+__global__ void sm_collide(SmoothArgs<S> A, int t, int store_pre, int slot) {
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    warp_collisions<S, false>(A, slot < 0 ? A.v : A.seg_v + (size_t)slot * A.n, t, store_pre);
+}
+
+// per-atom move + weight of a step.  slot < 0: the state arrays in place; else the start state in
+// segment slot `slot`, the end state into slot + 1.  coll_t >= 0: the last block then applies the
+// collisions of step coll_t to the end state (store_pre: keeping their pre-collision velocities).
+template <class S>
+__global__ void __launch_bounds__(256) sm_move(SmoothArgs<S> A, S cut, int slot, int last, int coll_t, int store_pre) {
+    typedef typename V4T<S>::type S4;
+    const size_t oi = slot < 0 ? 0 : (size_t)slot * A.n, oo = slot < 0 ? 0 : (size_t)(slot + 1) * A.n;
+    S4* xi = slot < 0 ? A.x : A.seg_x + oi;
+    S4* vi = slot < 0 ? A.v : A.seg_v + oi;
+    S4* pi = slot < 0 ? A.psi : A.seg_psi + oi;
+    S* wi = slot < 0 ? A.w : A.seg_w + oi;
+    S4* xo = slot < 0 ? A.x : A.seg_x + oo;
+    S4* vo = slot < 0 ? A.v : A.seg_v + oo;
+    S4* po = slot < 0 ? A.psi : A.seg_psi + oo;
+    S* wo = slot < 0 ? A.w : A.seg_w + oo;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
+        S4 xv = xi[i], vv = vi[i], pv = pi[i];
+        S w = wi[i];
+        S x[3] = {xv.x, xv.y, xv.z}, v[3] = {vv.x, vv.y, vv.z}, p[4] = {pv.x, pv.y, pv.z, pv.w};
+        const S e = smooth_step(A.C, cut, x, v, p, w);
+        xv.x = x[0]; xv.y = x[1]; xv.z = x[2];
+        vv.x = v[0]; vv.y = v[1]; vv.z = v[2];
+        pv.x = p[0]; pv.y = p[1]; pv.z = p[2]; pv.w = p[3];
+        xo[i] = xv;
+        vo[i] = vv;
+        po[i] = pv;
+        wo[i] = w;
+        if (last) A.e[i] = e;
+    }
+    if (coll_t >= 0) collisions_in_last_block<S, false>(A, vo, coll_t, store_pre);
 }
 
 // exact sums of w and w e per block (sum_v2 <- w, sum_B <- w e)
@@ -142,9 +218,8 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c) {
 template <class S>
 __global__ void __launch_bounds__(256) adj_seed(SmoothArgs<S> A, const double* sums, double half_m_over_kT) {
     typedef typename V4T<S>::type S4;
-    const int i = blockIdx.x * 256 + threadIdx.x;
     double tb0 = 0, tb1 = 0;
-    if (i < A.n) {
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
         const double W = sums[0], Sm = sums[1];
         const double e = (double)A.e[i], w = (double)A.w[i];
         const double dEdw = half_m_over_kT * (e / W - Sm / (W * W));
@@ -170,25 +245,28 @@ __global__ void __launch_bounds__(256) adj_seed(SmoothArgs<S> A, const double* s
         A.vb[A.n + i] = z;
         A.pb[A.n + i] = z;
         A.wb[A.n + i] = (S)(1.0 / (double)A.n);
-        tb0 = dEde * (double)A.C.kappa * (double)f.dabs_dBp;
-        tb1 = dEde * (double)A.C.kappa * (double)f.dabs_dB0;
+        tb0 += dEde * (double)A.C.kappa * (double)f.dabs_dBp;
+        tb1 += dEde * (double)A.C.kappa * (double)f.dabs_dB0;
     }
     double unused = 0;
     block_sum3(tb0, tb1, unused);
-    if (threadIdx.x == 0) {
-        atomicAdd(&A.theta_b[0], tb0);
-        atomicAdd(&A.theta_b[1], tb1);
+    if (threadIdx.x == 0) {  // the block's own slot (cleared before): seed 0, B' and B0
+        double* th = A.theta_part + (size_t)blockIdx.x * ADJ_SEEDS * ADJ_NPARAM;
+        th[0] += tb0;
+        th[1] += tb1;
     }
 }
 
 // adjoint of the per-atom part of step t (start state in segment slot seg) for both seeds; the cut
-// of the step depends on the knots k0 (weight 1 - f) and k0 + 1 (weight f)
+// of the step depends on the knots k0 (weight 1 - f) and k0 + 1 (weight f).  Each block adds its
+// parameter adjoints to its own slot; its last block to finish then pulls the velocity adjoints
+// back through the step's collisions (in reverse order).  Atoms in a grid-stride loop over the grid
+// adj_seed had (the same slots).
 template <class S>
-__global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg, int k0, double f) {
+__global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg, int k0, double f, int t) {
     typedef typename V4T<S>::type S4;
-    const int i = blockIdx.x * 256 + threadIdx.x;
     double t0[ADJ_SEEDS] = {0, 0}, t1[ADJ_SEEDS] = {0, 0}, cb[ADJ_SEEDS] = {0, 0};
-    if (i < A.n) {
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
         const size_t o = (size_t)seg * A.n + i;
         const S4 xs = A.seg_x[o], vs = A.seg_v[o], ps = A.seg_psi[o];
         const S ws = A.seg_w[o];
@@ -215,45 +293,33 @@ __global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg,
             A.vb[q * A.n + i] = b;
             A.pb[q * A.n + i] = c;
             A.wb[q * A.n + i] = wb[q];
-            t0[q] = (double)tb[q][0];
-            t1[q] = (double)tb[q][1];
-            cb[q] = (double)cut_b[q] * A.C.cut_scale;
+            t0[q] += (double)tb[q][0];
+            t1[q] += (double)tb[q][1];
+            cb[q] += (double)cut_b[q] * A.C.cut_scale;
         }
     }
 #pragma unroll
     for (int q = 0; q < ADJ_SEEDS; ++q) {
         block_sum3(t0[q], t1[q], cb[q]);
         if (threadIdx.x == 0) {
-            double* th = A.theta_b + q * ADJ_NPARAM;
-            atomicAdd(&th[0], t0[q]);
-            atomicAdd(&th[1], t1[q]);
-            atomicAdd(&th[2 + k0], cb[q] * (1.0 - f));
-            if (f != 0.0 && 2 + k0 + 1 < ADJ_NPARAM) atomicAdd(&th[2 + k0 + 1], cb[q] * f);
+            double* th = A.theta_part + ((size_t)blockIdx.x * ADJ_SEEDS + q) * ADJ_NPARAM;
+            th[0] += t0[q];
+            th[1] += t1[q];
+            th[2 + k0] += cb[q] * (1.0 - f);
+            if (f != 0.0 && 2 + k0 + 1 < ADJ_NPARAM) th[2 + k0 + 1] += cb[q] * f;
         }
     }
+    collisions_in_last_block<S, true>(A, A.v, t, 0);
 }
 
-// adjoint of the recorded collisions of step t, in reverse order
-template <class S>
-__global__ void sm_collide_adjoint(SmoothArgs<S> A, int t) {
-    typedef typename V4T<S>::type S4;
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int k = A.off[t + 1] - 1; k >= A.off[t]; --k) {
-        const int i = A.ij[k].x, j = A.ij[k].y;
-        if (i < 0 || i >= A.n || j < 0 || j >= A.n) continue;
-        const S4 a = A.vpre[2 * k], b = A.vpre[2 * k + 1];
-        const S vi[3] = {a.x, a.y, a.z}, vj[3] = {b.x, b.y, b.z};
-        const S nn[3] = {(S)A.nv[3 * k], (S)A.nv[3 * k + 1], (S)A.nv[3 * k + 2]};
-        for (int q = 0; q < ADJ_SEEDS; ++q) {
-            S4 bi = A.vb[q * A.n + i], bj = A.vb[q * A.n + j];
-            S vib[3] = {bi.x, bi.y, bi.z}, vjb[3] = {bj.x, bj.y, bj.z};
-            collide_fixed_adjoint(vi, vj, nn, vib, vjb);
-            bi.x = vib[0]; bi.y = vib[1]; bi.z = vib[2];
-            bj.x = vjb[0]; bj.y = vjb[1]; bj.z = vjb[2];
-            A.vb[q * A.n + i] = bi;
-            A.vb[q * A.n + j] = bj;
-        }
-    }
+// theta_b[o] = sum over the nb blocks' slots of output o (one warp per output, a fixed order)
+__global__ void adj_theta_reduce(const double* part, int nb, double* theta_b) {
+    const int o = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (o >= ADJ_SEEDS * ADJ_NPARAM) return;
+    double acc = 0;
+    for (int b = lane; b < nb; b += 32) acc += part[(size_t)b * ADJ_SEEDS * ADJ_NPARAM + o];
+    acc = warp_sum_d(acc);
+    if (lane == 0) theta_b[o] = acc;
 }
 
 // initial state of the recorded run by atom id, in double: out_x[3 id + a], out_v[3 id + a]

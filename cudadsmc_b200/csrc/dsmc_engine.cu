@@ -987,10 +987,20 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         const int nseg = (steps + K - 1) / K;
         const int ab = (nn + 255) / 256;
         const int sum_blocks = std::min(ab, 1184);
+        int occ = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sm_move<S>, 256, 0));
+        const int move_blocks = std::min(ab, num_sms * std::max(occ, 1));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_move<S>, 256, 0));
+        const int adj_blocks = std::min(ab, num_sms * std::max(occ, 1));
         partials_buf.alloc(sum_blocks);
         adj_sums.alloc(2);
+        DevBuf<int> done;
+        done.alloc(1);
+        CU(cudaMemsetAsync(done.p, 0, sizeof(int), stream));
         A.x = x.p; A.v = v.p; A.psi = ps.p; A.w = w.p; A.e = e.p;
         A.ij = adj_ij.p; A.nv = adj_n.p; A.off = adj_off.p; A.partials = partials_buf.p;
+        A.done = done.p;
+        DevBuf<double> theta_part;
         if (grad) {
             vpre.alloc(2 * (size_t)std::max(adj_nlog, 1));
             seg_x.alloc((size_t)K * nn); seg_v.alloc((size_t)K * nn); seg_p.alloc((size_t)K * nn);
@@ -1001,6 +1011,9 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             wb.alloc(ADJ_SEEDS * (size_t)nn);
             adj_theta_b.alloc(ADJ_SEEDS * ADJ_NPARAM);
             CU(cudaMemsetAsync(adj_theta_b.p, 0, ADJ_SEEDS * ADJ_NPARAM * sizeof(double), stream));
+            theta_part.alloc((size_t)adj_blocks * ADJ_SEEDS * ADJ_NPARAM);
+            CU(cudaMemsetAsync(theta_part.p, 0, (size_t)adj_blocks * ADJ_SEEDS * ADJ_NPARAM * sizeof(double), stream));
+            A.theta_part = theta_part.p;
             A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_psi = seg_p.p; A.seg_w = seg_w.p;
             A.xb = xb.p; A.vb = vb.p; A.pb = pb.p; A.wb = wb.p; A.theta_b = adj_theta_b.p;
         }
@@ -1009,16 +1022,20 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             cuts[t] = (S)(A.C.cut_scale * knife_eta(c.knife_nknots, c.knife_step, theta + 2, (double)t));
         CU(cudaEventRecord(ev[0], stream));
         if (n > 0) sm_load<S><<<ab, 256, 0, stream>>>(A, adj_x0.p, adj_v0.p, adj_p0.p);
-        for (int t = 0; t < steps; ++t) {
-            if (grad && t % K == 0) {
+        // a step is one launch: the move, then the next step's collisions in its last block -- except
+        // before a checkpoint, which keeps the state the next step starts from before its collisions
+        for (int t = 0; n > 0 && t < steps; ++t) {
+            const bool ck = grad && t % K == 0;
+            if (ck) {
                 const size_t o = (size_t)(t / K) * nn;
                 CU(cudaMemcpyAsync(ck_x.p + o, x.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_v.p + o, v.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_p.p + o, ps.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_w.p + o, w.p, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
             }
-            sm_collide<S><<<1, 32, 0, stream>>>(A, t, 0);
-            if (n > 0) sm_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], -1, t == steps - 1 ? 1 : 0);
+            if (t == 0 || ck) sm_collide<S><<<1, 32, 0, stream>>>(A, t, 0, -1);
+            const bool fuse = t + 1 < steps && !(grad && (t + 1) % K == 0);
+            sm_move<S><<<move_blocks, 256, 0, stream>>>(A, cuts[t], -1, t == steps - 1 ? 1 : 0, fuse ? t + 1 : -1, 0);
         }
         if (n > 0) sm_sums<S><<<sum_blocks, 256, 0, stream>>>(A);
         sm_sums_final<<<1, 32, 0, stream>>>(partials_buf.p, n > 0 ? sum_blocks : 0, adj_sums.p);
@@ -1037,26 +1054,27 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         if (!grad) return;
         CU(cudaEventRecord(ev[2], stream));
         const double half_m_over_kT = 0.5 * c.mass / kT;
-        if (n > 0) adj_seed<S><<<ab, 256, 0, stream>>>(A, adj_sums.p, half_m_over_kT);
-        for (int s = nseg - 1; s >= 0; --s) {
+        if (n > 0) adj_seed<S><<<adj_blocks, 256, 0, stream>>>(A, adj_sums.p, half_m_over_kT);
+        for (int s = nseg - 1; n > 0 && s >= 0; --s) {
             const int t0 = s * K, t1 = std::min(steps, t0 + K);
             const size_t o = (size_t)s * nn;
-            CU(cudaMemcpyAsync(x.p, ck_x.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
-            CU(cudaMemcpyAsync(v.p, ck_v.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
-            CU(cudaMemcpyAsync(ps.p, ck_p.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
-            CU(cudaMemcpyAsync(w.p, ck_w.p + o, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
-            for (int t = t0; t < t1; ++t) {
-                sm_collide<S><<<1, 32, 0, stream>>>(A, t, 1);
-                if (n > 0) sm_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], t - t0, 0);
-            }
+            // the segment from its checkpoint, slot to slot: slot t - t0 holds the state step t starts
+            // from (after its collisions), which is all the adjoint steps read
+            CU(cudaMemcpyAsync(seg_x.p, ck_x.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(seg_v.p, ck_v.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(seg_p.p, ck_p.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
+            CU(cudaMemcpyAsync(seg_w.p, ck_w.p + o, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
+            sm_collide<S><<<1, 32, 0, stream>>>(A, t0, 1, 0);
+            for (int t = t0; t + 1 < t1; ++t)
+                sm_move<S><<<move_blocks, 256, 0, stream>>>(A, cuts[t], t - t0, 0, t + 1, 1);
             for (int t = t1 - 1; t >= t0; --t) {
                 int k0 = 0;
                 double f = 0;
                 knot_weights(c.knife_nknots, c.knife_step, (double)t, &k0, &f);
-                if (n > 0) adj_move<S><<<ab, 256, 0, stream>>>(A, cuts[t], t - t0, k0, f);
-                sm_collide_adjoint<S><<<1, 32, 0, stream>>>(A, t);
+                adj_move<S><<<adj_blocks, 256, 0, stream>>>(A, cuts[t], t - t0, k0, f, t);
             }
         }
+        adj_theta_reduce<<<1, 32 * ADJ_SEEDS * ADJ_NPARAM, 0, stream>>>(theta_part.p, adj_blocks, adj_theta_b.p);
         CU(cudaEventRecord(ev[3], stream));
         CU(cudaMemcpyAsync(tb, adj_theta_b.p, ADJ_SEEDS * ADJ_NPARAM * sizeof(double), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
