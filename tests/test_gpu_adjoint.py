@@ -55,6 +55,30 @@ def test_gpu_smoothed_run_matches_oracle(recorded):
     np.testing.assert_allclose(grad_g, ge_o + gn_o, rtol=1e-9, atol=1e-12 * np.max(np.abs(ge_o + gn_o)))
 
 
+def test_gradients_repeat_bit_for_bit(recorded):
+    # the parameter adjoints are summed per block and reduced in a fixed order, and each step's
+    # collisions are applied with every atom's collisions in recorded order: evaluating the
+    # gradient again on the same recorded run gives the same bits, in FP64 and in FP32
+    run, c, sim, g = recorded
+    th = theta_of(c)
+    first = sim.adjoint_loss_parts(th, grad=True)
+    again = sim.adjoint_loss_parts(th, grad=True)
+    for a, b in zip(first, again):
+        assert np.array_equal(a, b)
+    np.testing.assert_array_equal(first[1], np.array(g["dE_dtheta"]))
+    np.testing.assert_array_equal(first[2], np.array(g["dN_dtheta"]))
+    s32 = Simulation(run, c)
+    s32.init_cloud(2468)
+    g32 = s32.adjoint_run(300, checkpoint_every=64, precision=FP32, sigmoid_width_kT=0.2)
+    assert g32["collisions"] > 0
+    for _ in range(2):  # the smoothed model again in the run's precision, on its record
+        parts, ge, gn = s32.adjoint_loss_parts(th, grad=True)
+        assert parts[0] == g32["mean_energy_kT"] and parts[1] == g32["retained_fraction"]
+        np.testing.assert_array_equal(ge, np.array(g32["dE_dtheta"]))
+        np.testing.assert_array_equal(gn, np.array(g32["dN_dtheta"]))
+    s32.close()
+
+
 def test_recorded_collisions_of_dense_cells():
     # a 2^3 grid: the central cells hold thousands of atoms and are collided by dense_collide, which
     # records its collisions (atom ids through the permutation) like the tiles do; the smoothed
