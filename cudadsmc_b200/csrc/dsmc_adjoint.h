@@ -51,14 +51,16 @@ template <class R> struct SmoothConsts {
     double cut_scale;                   // d cut / d eta = 2 kB T0 / m
 };
 
-// field of the linear trap with its derivatives
+// field of the linear trap: B = (h x, h y, B0 - B' z), h = B'/2, written B = J x + B0 e_z with
+// J = diag(h, h, -B'); its unit vector, |B|, grad |B| = J b^ and (derivs) d|B|/dB', d|B|/dB0.  The
+// second derivatives are never formed: the adjoints apply them through P = (I - b^ b^T) / |B|
+// (field_grad_adjoint).
 template <class R> struct QuadField {
     R b[3];      // unit field
     R absB;
+    R inv;       // 1 / |B| (0 where the field vanishes)
     R g[3];      // grad |B|
-    R H[3][3];   // Hessian of |B|
     R dabs_dBp, dabs_dB0;
-    R dg_dBp[3], dg_dB0[3];
 };
 
 template <class R>
@@ -75,25 +77,32 @@ DSMC_HD void quad_field(R Bp, R B0, R x, R y, R z, bool derivs, QuadField<R>& f)
         f.absB = R(0);
         f.b[0] = R(0); f.b[1] = R(0); f.b[2] = R(1);
     }
+    f.inv = inv;
     const R J[3] = {h, h, -Bp};
     for (int i = 0; i < 3; ++i) f.g[i] = J[i] * f.b[i];
     if (!derivs) return;
-    // (I - b b^T) / |B|, zero where the field vanishes
-    R P[3][3];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) P[i][j] = ((i == j ? R(1) : R(0)) - f.b[i] * f.b[j]) * inv;
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) f.H[i][j] = J[i] * P[i][j] * J[j];
     const R q[3] = {R(0.5) * x, R(0.5) * y, -z};  // dB/dB'
     f.dabs_dBp = f.b[0] * q[0] + f.b[1] * q[1] + f.b[2] * q[2];
     f.dabs_dB0 = f.b[2];
-    const R dJ[3] = {R(0.5), R(0.5), R(-1)};
-    for (int i = 0; i < 3; ++i) {
-        const R dbBp = P[i][0] * q[0] + P[i][1] * q[1] + P[i][2] * q[2];
-        const R dbB0 = P[i][2];
-        f.dg_dBp[i] = dJ[i] * f.b[i] + J[i] * dbBp;
-        f.dg_dB0[i] = J[i] * dbB0;
-    }
+}
+
+// adjoint of g = grad |B| = J b^ at x: with an adjoint gb of g, accumulates into xb (3) and tb
+// (B', B0).  dg/dx = J P J (the Hessian of |B|); dg_i/dB' = dJ_i b_i + J_i (P q)_i with q = dB/dB' =
+// (x/2, y/2, -z) and dJ = (1/2, 1/2, -1); dg_i/dB0 = J_i P_i2.  With u = J gb and r = P u (P is
+// symmetric): xb += J r, tb[0] += sum dJ_i b_i gb_i + q . r, tb[1] += r_2.
+template <class R>
+DSMC_HD void field_grad_adjoint(R Bp, const R* x, const QuadField<R>& f, const R* gb, R* xb, R* tb) {
+    const R h = R(0.5) * Bp;
+    const R u[3] = {h * gb[0], h * gb[1], -Bp * gb[2]};
+    const R d = f.b[0] * u[0] + f.b[1] * u[1] + f.b[2] * u[2];
+    R r[3];
+    for (int i = 0; i < 3; ++i) r[i] = (u[i] - f.b[i] * d) * f.inv;
+    xb[0] += h * r[0];
+    xb[1] += h * r[1];
+    xb[2] += -Bp * r[2];
+    tb[0] += R(0.5) * (f.b[0] * gb[0] + f.b[1] * gb[1]) - f.b[2] * gb[2]
+             + (R(0.5) * x[0] * r[0] + R(0.5) * x[1] * r[1] - x[2] * r[2]);
+    tb[1] += r[2];
 }
 
 template <class R> DSMC_HD R sigmoid(R z) { return R(1) / (R(1) + xexp(-z)); }
@@ -141,10 +150,9 @@ DSMC_HD R smooth_step(const SmoothConsts<R>& C, R cut, R* x, R* v, R* psi, R& w)
 // adjoint of (b, |B|) at x through the field vector: accumulates into xb (3) and tb (B', B0)
 template <class R>
 DSMC_HD void field_vec_adjoint(R Bp, const R* x, const QuadField<R>& f, const R* bb, R absBb, R* xb, R* tb) {
-    const R inv = f.absB > R(0) ? R(1) / f.absB : R(0);
     const R d = f.b[0] * bb[0] + f.b[1] * bb[1] + f.b[2] * bb[2];
     R Bb[3];
-    for (int i = 0; i < 3; ++i) Bb[i] = (bb[i] - f.b[i] * d) * inv + f.b[i] * absBb;
+    for (int i = 0; i < 3; ++i) Bb[i] = (bb[i] - f.b[i] * d) * f.inv + f.b[i] * absBb;
     const R h = R(0.5) * Bp;
     xb[0] += h * Bb[0];
     xb[1] += h * Bb[1];
@@ -215,20 +223,17 @@ DSMC_HD void smooth_step_adjoint(const SmoothConsts<R>& C, R cut, const R* x0, c
         // v2 = v1 + hdt as g(x1)
         R g1b[3];
         for (int i = 0; i < 3; ++i) g1b[i] = C.half_dt * as * v2b[i];
-        for (int i = 0; i < 3; ++i) x1b[i] += f1.H[i][0] * g1b[0] + f1.H[i][1] * g1b[1] + f1.H[i][2] * g1b[2];
-        theta_b[q][0] += f1.dg_dBp[0] * g1b[0] + f1.dg_dBp[1] * g1b[1] + f1.dg_dBp[2] * g1b[2];
-        theta_b[q][1] += f1.dg_dB0[0] * g1b[0] + f1.dg_dB0[1] * g1b[1] + f1.dg_dB0[2] * g1b[2];
+        field_grad_adjoint(C.Bp, x1, f1, g1b, x1b, theta_b[q]);
         // x1 = x0 + dt v1 ; v1 = v0 + hdt as g(x0)
         R v1b[3];
         for (int i = 0; i < 3; ++i) v1b[i] = v2b[i] + C.dt * x1b[i];
         R g0b[3];
         for (int i = 0; i < 3; ++i) g0b[i] = C.half_dt * as * v1b[i];
         for (int i = 0; i < 3; ++i) {
-            xb[q][i] = x1b[i] + f0.H[i][0] * g0b[0] + f0.H[i][1] * g0b[1] + f0.H[i][2] * g0b[2];
+            xb[q][i] = x1b[i];
             vb[q][i] = v1b[i];
         }
-        theta_b[q][0] += f0.dg_dBp[0] * g0b[0] + f0.dg_dBp[1] * g0b[1] + f0.dg_dBp[2] * g0b[2];
-        theta_b[q][1] += f0.dg_dB0[0] * g0b[0] + f0.dg_dB0[1] * g0b[1] + f0.dg_dB0[2] * g0b[2];
+        field_grad_adjoint(C.Bp, x0, f0, g0b, xb[q], theta_b[q]);
         // psi1 = c psi0 + s T(b0) psi0, angle t = theta_per_B |B(x0)|
         if (larmor) {
             R tp[4];  // T(b0)^T psi1_bar
