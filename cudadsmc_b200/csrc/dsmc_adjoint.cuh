@@ -1,8 +1,9 @@
 // dsmc_adjoint.cuh -- kernels of the smoothed model and its adjoint (see dsmc_adjoint.h).
 //
-// State of the smoothed model: one atom per id (0..n-1), x and v as R4 (fourth lane unused), the
-// spinor psi as R4 (Re u, Im u, Re d, Im d), the survival weight w.  The adjoint state holds
-// ADJ_SEEDS copies (the two loss terms), seed q of atom i at index q n + i.  A step is the recorded
+// State of the smoothed model: one atom per id (0..n-1), x as R4 with the survival weight w in its
+// fourth lane, v as R4 (fourth lane unused), the spinor psi as R4 (Re u, Im u, Re d, Im d).  The
+// adjoint state holds ADJ_SEEDS copies (the two loss terms), seed q of atom i at index q n + i, the
+// weight's adjoint in the fourth lane of the position's.  A step is the recorded
 // collisions of the step, applied by one warp with every atom's collisions in recorded order
 // (collisions of different cells touch different atoms; within a cell the recording order is the
 // collision order), then the per-atom move + weight update; the collisions of the next step run in
@@ -22,10 +23,9 @@ namespace dsmc {
 
 template <class S> struct SmoothArgs {
     typedef typename V4T<S>::type S4;
-    S4* x;
+    S4* x;             // position, survival weight in .w
     S4* v;
     S4* psi;
-    S* w;
     S* e;              // knife energy after the last step
     const int2* ij;    // recorded pairs (atom ids)
     const double* nv;  // recorded directions, 3 per pair
@@ -34,11 +34,9 @@ template <class S> struct SmoothArgs {
     S4* seg_x;         // stored start states of the current segment [K][n]
     S4* seg_v;
     S4* seg_psi;
-    S* seg_w;
     S4* xb;            // adjoints, ADJ_SEEDS x n each
     S4* vb;
     S4* pb;
-    S* wb;
     double* theta_b;   // ADJ_SEEDS x ADJ_NPARAM results
     double* theta_part;  // per block of adj_seed / adj_move: ADJ_SEEDS x ADJ_NPARAM partial sums
     int* done;         // blocks of the running move / adjoint kernel finished (its last block resets it)
@@ -144,23 +142,20 @@ __global__ void __launch_bounds__(256) sm_move(SmoothArgs<S> A, S cut, int slot,
     S4* xi = slot < 0 ? A.x : A.seg_x + oi;
     S4* vi = slot < 0 ? A.v : A.seg_v + oi;
     S4* pi = slot < 0 ? A.psi : A.seg_psi + oi;
-    S* wi = slot < 0 ? A.w : A.seg_w + oi;
     S4* xo = slot < 0 ? A.x : A.seg_x + oo;
     S4* vo = slot < 0 ? A.v : A.seg_v + oo;
     S4* po = slot < 0 ? A.psi : A.seg_psi + oo;
-    S* wo = slot < 0 ? A.w : A.seg_w + oo;
     for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
         S4 xv = xi[i], vv = vi[i], pv = pi[i];
-        S w = wi[i];
+        S w = xv.w;
         S x[3] = {xv.x, xv.y, xv.z}, v[3] = {vv.x, vv.y, vv.z}, p[4] = {pv.x, pv.y, pv.z, pv.w};
         const S e = smooth_step(A.C, cut, x, v, p, w);
-        xv.x = x[0]; xv.y = x[1]; xv.z = x[2];
+        xv.x = x[0]; xv.y = x[1]; xv.z = x[2]; xv.w = w;
         vv.x = v[0]; vv.y = v[1]; vv.z = v[2];
         pv.x = p[0]; pv.y = p[1]; pv.z = p[2]; pv.w = p[3];
         xo[i] = xv;
         vo[i] = vv;
         po[i] = pv;
-        wo[i] = w;
         if (last) A.e[i] = e;
     }
     if (coll_t >= 0) collisions_in_last_block<S, false>(A, vo, coll_t, store_pre);
@@ -173,8 +168,9 @@ __global__ void __launch_bounds__(256) sm_sums(SmoothArgs<S> A) {
     TilePartial acc;
     zero_partial(acc);
     for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
-        acc.sum_v2 += fx_from((double)A.w[i]);
-        acc.sum_B += fx_from((double)A.w[i] * (double)A.e[i]);
+        const double w = (double)A.x[i].w;
+        acc.sum_v2 += fx_from(w);
+        acc.sum_B += fx_from(w * (double)A.e[i]);
     }
     block_reduce_partial<256>(acc, red);
     if (threadIdx.x == 0) A.partials[blockIdx.x] = acc;
@@ -221,17 +217,17 @@ __global__ void __launch_bounds__(256) adj_seed(SmoothArgs<S> A, const double* s
     double tb0 = 0, tb1 = 0;
     for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
         const double W = sums[0], Sm = sums[1];
-        const double e = (double)A.e[i], w = (double)A.w[i];
+        const S4 xv = A.x[i], vv = A.v[i];
+        const double e = (double)A.e[i], w = (double)xv.w;
         const double dEdw = half_m_over_kT * (e / W - Sm / (W * W));
         const double dEde = half_m_over_kT * w / W;
-        const S4 xv = A.x[i], vv = A.v[i];
         QuadField<S> f;
         quad_field(A.C.Bp, A.C.B0, xv.x, xv.y, xv.z, true, f);
         S4 xb, vb, z;
         xb.x = (S)(dEde * (double)A.C.kappa * (double)f.g[0]);
         xb.y = (S)(dEde * (double)A.C.kappa * (double)f.g[1]);
         xb.z = (S)(dEde * (double)A.C.kappa * (double)f.g[2]);
-        xb.w = (S)0;
+        xb.w = (S)dEdw;
         vb.x = (S)(dEde * 2.0 * (double)vv.x);
         vb.y = (S)(dEde * 2.0 * (double)vv.y);
         vb.z = (S)(dEde * 2.0 * (double)vv.z);
@@ -240,11 +236,11 @@ __global__ void __launch_bounds__(256) adj_seed(SmoothArgs<S> A, const double* s
         A.xb[i] = xb;
         A.vb[i] = vb;
         A.pb[i] = z;
-        A.wb[i] = (S)dEdw;
+        z.w = (S)(1.0 / (double)A.n);
         A.xb[A.n + i] = z;
+        z.w = (S)0;
         A.vb[A.n + i] = z;
         A.pb[A.n + i] = z;
-        A.wb[A.n + i] = (S)(1.0 / (double)A.n);
         tb0 += dEde * (double)A.C.kappa * (double)f.dabs_dBp;
         tb1 += dEde * (double)A.C.kappa * (double)f.dabs_dB0;
     }
@@ -269,7 +265,7 @@ __global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg,
     for (int i = blockIdx.x * 256 + threadIdx.x; i < A.n; i += gridDim.x * 256) {
         const size_t o = (size_t)seg * A.n + i;
         const S4 xs = A.seg_x[o], vs = A.seg_v[o], ps = A.seg_psi[o];
-        const S ws = A.seg_w[o];
+        const S ws = xs.w;
         const S x0[3] = {xs.x, xs.y, xs.z}, v0[3] = {vs.x, vs.y, vs.z}, p0[4] = {ps.x, ps.y, ps.z, ps.w};
         S xb[ADJ_SEEDS][3], vb[ADJ_SEEDS][3], pb[ADJ_SEEDS][4], wb[ADJ_SEEDS], tb[ADJ_SEEDS][2], cut_b[ADJ_SEEDS];
 #pragma unroll
@@ -278,7 +274,7 @@ __global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg,
             xb[q][0] = a.x; xb[q][1] = a.y; xb[q][2] = a.z;
             vb[q][0] = b.x; vb[q][1] = b.y; vb[q][2] = b.z;
             pb[q][0] = c.x; pb[q][1] = c.y; pb[q][2] = c.z; pb[q][3] = c.w;
-            wb[q] = A.wb[q * A.n + i];
+            wb[q] = a.w;
             tb[q][0] = S(0); tb[q][1] = S(0);
             cut_b[q] = S(0);
         }
@@ -286,13 +282,12 @@ __global__ void __launch_bounds__(256) adj_move(SmoothArgs<S> A, S cut, int seg,
 #pragma unroll
         for (int q = 0; q < ADJ_SEEDS; ++q) {
             S4 a, b, c;
-            a.x = xb[q][0]; a.y = xb[q][1]; a.z = xb[q][2]; a.w = S(0);
+            a.x = xb[q][0]; a.y = xb[q][1]; a.z = xb[q][2]; a.w = wb[q];
             b.x = vb[q][0]; b.y = vb[q][1]; b.z = vb[q][2]; b.w = S(0);
             c.x = pb[q][0]; c.y = pb[q][1]; c.z = pb[q][2]; c.w = pb[q][3];
             A.xb[q * A.n + i] = a;
             A.vb[q * A.n + i] = b;
             A.pb[q * A.n + i] = c;
-            A.wb[q * A.n + i] = wb[q];
             t0[q] += (double)tb[q][0];
             t1[q] += (double)tb[q][1];
             cb[q] += (double)cut_b[q] * A.C.cut_scale;
@@ -349,13 +344,12 @@ __global__ void __launch_bounds__(256) sm_load(SmoothArgs<S> A, const double* x0
     const int i = blockIdx.x * 256 + threadIdx.x;
     if (i >= A.n) return;
     S4 x, v, p;
-    x.x = (S)x0[3 * i]; x.y = (S)x0[3 * i + 1]; x.z = (S)x0[3 * i + 2]; x.w = (S)0;
+    x.x = (S)x0[3 * i]; x.y = (S)x0[3 * i + 1]; x.z = (S)x0[3 * i + 2]; x.w = (S)1;
     v.x = (S)v0[3 * i]; v.y = (S)v0[3 * i + 1]; v.z = (S)v0[3 * i + 2]; v.w = (S)0;
     p.x = (S)p0[4 * i]; p.y = (S)p0[4 * i + 1]; p.z = (S)p0[4 * i + 2]; p.w = (S)p0[4 * i + 3];
     A.x[i] = x;
     A.v[i] = v;
     A.psi[i] = p;
-    A.w[i] = (S)1;
 }
 
 }  // namespace dsmc

@@ -982,8 +982,8 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         A.n = n;
         const int nn = std::max(n, 1);
         DevBuf<S4> x, v, ps, xb, vb, pb, vpre, seg_x, seg_v, seg_p, ck_x, ck_v, ck_p;
-        DevBuf<S> w, e, wb, seg_w, ck_w;
-        x.alloc(nn); v.alloc(nn); ps.alloc(nn); w.alloc(nn); e.alloc(nn);
+        DevBuf<S> e;  // the survival weight rides in x's fourth lane, its adjoints in xb's
+        x.alloc(nn); v.alloc(nn); ps.alloc(nn); e.alloc(nn);
         const int nseg = (steps + K - 1) / K;
         const int ab = (nn + 255) / 256;
         const int sum_blocks = std::min(ab, 1184);
@@ -997,25 +997,22 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
         DevBuf<int> done;
         done.alloc(1);
         CU(cudaMemsetAsync(done.p, 0, sizeof(int), stream));
-        A.x = x.p; A.v = v.p; A.psi = ps.p; A.w = w.p; A.e = e.p;
+        A.x = x.p; A.v = v.p; A.psi = ps.p; A.e = e.p;
         A.ij = adj_ij.p; A.nv = adj_n.p; A.off = adj_off.p; A.partials = partials_buf.p;
         A.done = done.p;
         DevBuf<double> theta_part;
         if (grad) {
             vpre.alloc(2 * (size_t)std::max(adj_nlog, 1));
             seg_x.alloc((size_t)K * nn); seg_v.alloc((size_t)K * nn); seg_p.alloc((size_t)K * nn);
-            seg_w.alloc((size_t)K * nn);
             ck_x.alloc((size_t)nseg * nn); ck_v.alloc((size_t)nseg * nn); ck_p.alloc((size_t)nseg * nn);
-            ck_w.alloc((size_t)nseg * nn);
             xb.alloc(ADJ_SEEDS * (size_t)nn); vb.alloc(ADJ_SEEDS * (size_t)nn); pb.alloc(ADJ_SEEDS * (size_t)nn);
-            wb.alloc(ADJ_SEEDS * (size_t)nn);
             adj_theta_b.alloc(ADJ_SEEDS * ADJ_NPARAM);
             CU(cudaMemsetAsync(adj_theta_b.p, 0, ADJ_SEEDS * ADJ_NPARAM * sizeof(double), stream));
             theta_part.alloc((size_t)adj_blocks * ADJ_SEEDS * ADJ_NPARAM);
             CU(cudaMemsetAsync(theta_part.p, 0, (size_t)adj_blocks * ADJ_SEEDS * ADJ_NPARAM * sizeof(double), stream));
             A.theta_part = theta_part.p;
-            A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_psi = seg_p.p; A.seg_w = seg_w.p;
-            A.xb = xb.p; A.vb = vb.p; A.pb = pb.p; A.wb = wb.p; A.theta_b = adj_theta_b.p;
+            A.vpre = vpre.p; A.seg_x = seg_x.p; A.seg_v = seg_v.p; A.seg_psi = seg_p.p;
+            A.xb = xb.p; A.vb = vb.p; A.pb = pb.p; A.theta_b = adj_theta_b.p;
         }
         std::vector<S> cuts(steps);
         for (int t = 0; t < steps; ++t)
@@ -1031,7 +1028,6 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
                 CU(cudaMemcpyAsync(ck_x.p + o, x.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_v.p + o, v.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
                 CU(cudaMemcpyAsync(ck_p.p + o, ps.p, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
-                CU(cudaMemcpyAsync(ck_w.p + o, w.p, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
             }
             if (t == 0 || ck) sm_collide<S><<<1, 32, 0, stream>>>(A, t, 0, -1);
             const bool fuse = t + 1 < steps && !(grad && (t + 1) % K == 0);
@@ -1063,7 +1059,6 @@ template <class R, int BLOCK, int CAP, int MINB> struct Engine final : dsmc_hand
             CU(cudaMemcpyAsync(seg_x.p, ck_x.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
             CU(cudaMemcpyAsync(seg_v.p, ck_v.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
             CU(cudaMemcpyAsync(seg_p.p, ck_p.p + o, n * sizeof(S4), cudaMemcpyDeviceToDevice, stream));
-            CU(cudaMemcpyAsync(seg_w.p, ck_w.p + o, n * sizeof(S), cudaMemcpyDeviceToDevice, stream));
             sm_collide<S><<<1, 32, 0, stream>>>(A, t0, 1, 0);
             for (int t = t0; t + 1 < t1; ++t)
                 sm_move<S><<<move_blocks, 256, 0, stream>>>(A, cuts[t], t - t0, 0, t + 1, 1);
