@@ -185,11 +185,13 @@ def test_profiling_mode_identical():
     assert all(v[1] == 5 for v in t.values())
 
 
-def test_batched_clouds_match_oracle_and_single_runs():
+@pytest.mark.parametrize("precision", [FP32, FP64])
+def test_batched_clouds_match_oracle_and_single_runs(precision):
     rng = np.random.default_rng(7)
     clouds = []
     for k in range(5):
-        run, c = scaled(2, n=int(rng.integers(500, 20000)), cells=int(rng.integers(8, 24)), flags=ALL, alpha=2000.0)
+        run, c = scaled(2, n=int(rng.integers(500, 20000)), cells=int(rng.integers(8, 24)), flags=ALL, alpha=2000.0,
+                        precision=precision)
         c.dBdz = float(rng.uniform(1.5, 4.0))
         c.temperature = float(rng.uniform(5e-6, 50e-6))
         from cudadsmc_b200.engine import load_library  # noqa
